@@ -1,0 +1,186 @@
+/* SANKHYA restarted-PDHG LP engine on one NVIDIA B200 (sm_100a) -- C ABI.
+ *
+ * This is the drop-in for the reference solver's CPU PDHG call
+ *     Solution sankhya::pdhg::solve_pdhg(const Model&, const Options&, Logger&)
+ *     (include/sankhya/pdhg.hpp:15, src/pdhg/pdhg.cpp:267-726)
+ * at its one call site, run_lp_engine in src/core/solve.cpp:385-395. The adapter a maintainer
+ * adds on the reference side turns the Model and Options into the structs below and the
+ * result back into a Solution; it is shown in INTEGRATION.md.
+ *
+ * Conventions follow the reference's C API (include/sankhya/sankhya.h:16-28):
+ *   ERRORS are returned, never thrown; sankhya_pdhg_gpu_last_error() gives the reason for the
+ *     most recent failing call on the calling thread.
+ *   OWNERSHIP: the caller owns every input array and every output buffer; the library owns
+ *     device memory and handles, released by the matching *_free.
+ *   THREADING: a handle is not internally synchronised; distinct handles on distinct threads
+ *     are fine. The error string is thread-local.
+ *   NO CPU FALLBACK: when the GPU path cannot run, the call fails with a status; nothing is
+ *     silently computed on the host.
+ *
+ * Storage matches the reference's SparseMatrix (include/sankhya/sparse.hpp:109-112): CSC,
+ * int32 column starts [n+1] and row indices [nnz] ascending within each column, FP64 values.
+ * An absent bound is +-inf or any |v| >= 1e30 (include/sankhya/types.hpp:32-39).
+ */
+#ifndef SANKHYA_PDHG_GPU_H
+#define SANKHYA_PDHG_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- Status of a call. The values mirror sankhya::gpu::GpuStatus
+ *      (include/sankhya/gpu_runtime.hpp:19-30); 10 and 11 are additions. ------------------ */
+typedef enum sankhya_pdhg_gpu_status {
+  SANKHYA_GPU_SUCCESS = 0,
+  SANKHYA_GPU_CUDA_UNAVAILABLE = 1,
+  SANKHYA_GPU_NO_COMPATIBLE_DEVICE = 2,
+  SANKHYA_GPU_INIT_FAILED = 3,
+  SANKHYA_GPU_OUT_OF_MEMORY = 4,
+  SANKHYA_GPU_KERNEL_LAUNCH_FAILED = 5,
+  SANKHYA_GPU_COPY_FAILED = 6,
+  SANKHYA_GPU_SYNC_FAILED = 7,
+  SANKHYA_GPU_INVALID_DEVICE_STATE = 8,
+  SANKHYA_GPU_NON_FINITE_OUTPUT = 9,
+  SANKHYA_GPU_INVALID_ARGUMENT = 10, /* malformed problem or parameters; see last_error */
+  SANKHYA_GPU_DEVICE_TIMEOUT = 11    /* a bounded device-side wait gave up; context intact */
+} sankhya_pdhg_gpu_status;
+
+/* ---- Solve status of a result: the values of sankhya_solve_status
+ *      (include/sankhya/sankhya.h:53-66). ---------------------------------------------- */
+enum {
+  SANKHYA_PDHG_NOT_SOLVED = 0,
+  SANKHYA_PDHG_OPTIMAL = 1,
+  SANKHYA_PDHG_FEASIBLE = 2,
+  SANKHYA_PDHG_INFEASIBLE = 3,
+  SANKHYA_PDHG_UNBOUNDED = 4,
+  SANKHYA_PDHG_ITERATION_LIMIT = 5,
+  SANKHYA_PDHG_TIME_LIMIT = 6,
+  SANKHYA_PDHG_NUMERICAL_ERROR = 8,
+  SANKHYA_PDHG_MODEL_ERROR = 9
+};
+
+/* Arithmetic of the iteration. */
+enum {
+  SANKHYA_PDHG_FP64 = 0,  /* FP64 matrix, iterates and reductions throughout */
+  SANKHYA_PDHG_MIXED = 1  /* FP32 matrix and iterates with FP64 reductions and FP64 KKT,
+                             restart and step-size logic; then an FP64 polish phase
+                             warm-started from the FP32 iterate when the request is below
+                             what FP32 reaches */
+};
+
+/* Stopping rule. */
+enum {
+  /* src/pdhg/pdhg.cpp:585-586: meets_request(tol) AND (stop_at_request OR the project's
+   * absolute standard: primal 1e-7, dual 1e-7, verified gap 1e-9, complementarity 1e-6). */
+  SANKHYA_PDHG_STOP_REFERENCE = 0,
+  /* Relative KKT only: max(relative primal, relative dual, relative gap) <= tolerance, the
+   * PDLP-literature criterion (time-to-relative-KKT). Status is still assigned by the
+   * reference's rules (optimal only when the absolute standard holds). */
+  SANKHYA_PDHG_STOP_RELATIVE_KKT = 1
+};
+
+/* One LP as the reference's Model holds it (include/sankhya/model.hpp:131-225). */
+typedef struct sankhya_pdhg_problem {
+  int32_t num_rows;
+  int32_t num_cols;
+  int32_t num_nonzeros;
+  const int32_t* col_starts;  /* [n+1] */
+  const int32_t* row_indices; /* [nnz] */
+  const double* values;       /* [nnz] */
+  const double* cost;         /* [n], in the model's own sense */
+  const double* col_lower;    /* [n] */
+  const double* col_upper;    /* [n] */
+  const double* row_lower;    /* [m] */
+  const double* row_upper;    /* [m] */
+  int32_t maximize;           /* model.sense == kMaximize */
+  double objective_offset;
+} sankhya_pdhg_problem;
+
+/* Options. Fill with sankhya_pdhg_gpu_default_params(); the first six mirror the reference's
+ * option registry rows of the same name (src/util/options.cpp:83-418). */
+typedef struct sankhya_pdhg_params {
+  double tolerance;         /* pdhg_tolerance, default 1e-4 */
+  int64_t iteration_limit;  /* iteration_limit, -1 = 1,000,000 (src/pdhg/pdhg.cpp:311-313) */
+  double time_limit;        /* time_limit in seconds, default +inf */
+  int32_t restart;          /* pdhg_restart, default 1 */
+  int32_t stop_at_request;  /* pdhg_stop_at_request, default 0 */
+  int64_t random_seed;      /* random_seed, default 0 (the norm estimate uses seed + 1) */
+  /* GPU knobs (new rows) */
+  int32_t precision;        /* SANKHYA_PDHG_FP64 (default) or SANKHYA_PDHG_MIXED */
+  int32_t stop_rule;        /* SANKHYA_PDHG_STOP_REFERENCE (default) or _RELATIVE_KKT */
+  int32_t device;           /* CUDA device ordinal, default 0 */
+  int32_t verbose;          /* 1 prints the iteration table at each evaluation */
+  int32_t detect_infeasibility; /* 1 (default): certify primal infeasibility / dual
+                                   unboundedness from iterate differences */
+  double mixed_switch_tolerance; /* MIXED: relative KKT at which the FP32 phase hands over
+                                    to FP64 when the stop rule needs more; default 1e-5 */
+  int32_t group_size_rows;  /* lanes per row for A x (0 = autotune) */
+  int32_t group_size_cols;  /* lanes per row for A'y (0 = autotune) */
+  int32_t reserved[8];
+} sankhya_pdhg_params;
+
+/* Unscaled residual block of the reported point (src/pdhg/pdhg.cpp:81-110). */
+typedef struct sankhya_pdhg_residuals {
+  double relative_primal;
+  double relative_dual;
+  double relative_gap;
+  double primal_objective; /* minimise space, offset excluded */
+  double dual_objective;
+  double absolute_primal;
+  double absolute_dual;
+  double gap_as_verified;
+  double complementarity;
+} sankhya_pdhg_residuals;
+
+/* Result. The caller allocates the arrays (any may be NULL); the library fills the rest.
+ * Sign conventions follow src/pdhg/pdhg.cpp:647-661: row_dual = sense * (-y),
+ * col_dual = sense * (c_min + A'y), with y the PDHG multiplier. */
+typedef struct sankhya_pdhg_result {
+  double* col_value;   /* [n] */
+  double* row_dual;    /* [m] */
+  double* col_dual;    /* [n] */
+  double* farkas_dual; /* [m] filled when status is INFEASIBLE (row_dual sign) */
+  double* primal_ray;  /* [n] filled when status is UNBOUNDED */
+  int32_t status;      /* SANKHYA_PDHG_* solve status */
+  int32_t converged;
+  int64_t iterations;  /* accepted iterations, all phases */
+  int64_t attempts;    /* accepted + rejected steps */
+  int64_t restarts;
+  int64_t evaluations;
+  int64_t fp32_iterations; /* MIXED: accepted iterations in the FP32 phase */
+  double objective;    /* original sense, offset included */
+  double dual_bound;   /* finite only when the point meets the project standard */
+  double spectral_norm;
+  double setup_seconds;  /* validation, scaling, upload, norm estimate */
+  double solve_seconds;  /* the iteration loop, device-timed */
+  double total_seconds;  /* the whole call, host wall clock */
+  sankhya_pdhg_residuals residuals;
+  char message[512];
+} sankhya_pdhg_result;
+
+/* Defaults equal to the reference's option defaults. */
+void sankhya_pdhg_gpu_default_params(sankhya_pdhg_params* params);
+
+/* Solve one LP on the GPU. Replaces pdhg::solve_pdhg (src/pdhg/pdhg.cpp:267) for the
+ * adapter at src/core/solve.cpp:392. A model the reference would reject (Model::validate,
+ * src/core/model.cpp:125-210) returns SUCCESS with status MODEL_ERROR and the reason in
+ * result->message, as solve_pdhg does (src/pdhg/pdhg.cpp:273-278). */
+int sankhya_pdhg_gpu_solve(const sankhya_pdhg_problem* problem,
+                           const sankhya_pdhg_params* params, sankhya_pdhg_result* result);
+
+/* Reason for the most recent failing call on this thread (never NULL). */
+const char* sankhya_pdhg_gpu_last_error(void);
+
+/* Device queries, the successors of is_cuda_available / get_gpu_device_count
+ * (include/sankhya/gpu_runtime.hpp:71-77). */
+int sankhya_pdhg_gpu_device_count(void);
+int sankhya_pdhg_gpu_device_name(int device, char* name, int capacity);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SANKHYA_PDHG_GPU_H */

@@ -1,0 +1,334 @@
+// Host-side preparation of one LP (see pdhg_host.cuh).
+#include "pdhg_host.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <queue>
+#include <string>
+
+namespace sih26 {
+
+bool host_finite_bound(double v) { return !(std::isinf(v) || std::fabs(v) >= 1e30); }
+
+static std::string fmtd(const char* f, long long a, long long b = 0) {
+  char buf[256];
+  std::snprintf(buf, sizeof buf, f, a, b);
+  return buf;
+}
+
+void check_structure(const sankhya_pdhg_problem& p) {
+  const auto bad = [](const std::string& why) {
+    throw Failure{SANKHYA_GPU_INVALID_ARGUMENT, why};
+  };
+  if (p.num_rows < 0 || p.num_cols < 0 || p.num_nonzeros < 0) bad("negative problem size");
+  const int m = p.num_rows, n = p.num_cols;
+  if (!p.col_starts) bad("col_starts is NULL");
+  if (n > 0 && (!p.cost || !p.col_lower || !p.col_upper)) bad("a column array is NULL");
+  if (m > 0 && (!p.row_lower || !p.row_upper)) bad("a row array is NULL");
+  if (p.num_nonzeros > 0 && (!p.row_indices || !p.values)) bad("matrix arrays are NULL");
+  if (p.col_starts[0] != 0) bad("col_starts[0] != 0");
+  if (p.col_starts[n] != p.num_nonzeros)
+    bad(fmtd("col_starts[n] = %lld but num_nonzeros = %lld", p.col_starts[n], p.num_nonzeros));
+  for (int j = 0; j < n; ++j) {
+    const int b = p.col_starts[j], e = p.col_starts[j + 1];
+    if (e < b) bad(fmtd("col_starts decreases at column %lld", j));
+    for (int k = b; k < e; ++k) {
+      const int i = p.row_indices[k];
+      if (i < 0 || i >= m) bad(fmtd("row index %lld out of range in column %lld", i, j));
+      if (k > b && i <= p.row_indices[k - 1])
+        bad(fmtd("row indices of column %lld are not strictly ascending (entry %lld)", j, k));
+    }
+  }
+}
+
+std::string validate_model(const sankhya_pdhg_problem& p) {
+  char buf[256];
+  const int m = p.num_rows, n = p.num_cols;
+  for (int j = 0; j < n; ++j) {
+    for (int k = p.col_starts[j]; k < p.col_starts[j + 1]; ++k) {
+      if (!std::isfinite(p.values[k])) {
+        std::snprintf(buf, sizeof buf,
+                      "matrix entry (%d, %d) is %g, which is not a usable coefficient",
+                      p.row_indices[k], j, p.values[k]);
+        return buf;
+      }
+    }
+  }
+  for (int j = 0; j < n; ++j) {
+    const double lo = p.col_lower[j], hi = p.col_upper[j];
+    if (std::isnan(lo) || std::isnan(hi)) {
+      std::snprintf(buf, sizeof buf, "column %d has a NaN bound", j);
+      return buf;
+    }
+    if (lo > hi) {
+      std::snprintf(buf, sizeof buf, "column %d has lower bound %g above upper bound %g", j, lo, hi);
+      return buf;
+    }
+    if (std::isnan(p.cost[j])) {
+      std::snprintf(buf, sizeof buf, "column %d has a NaN objective coefficient", j);
+      return buf;
+    }
+  }
+  for (int i = 0; i < m; ++i) {
+    const double lo = p.row_lower[i], hi = p.row_upper[i];
+    if (std::isnan(lo) || std::isnan(hi)) {
+      std::snprintf(buf, sizeof buf, "row %d has a NaN bound", i);
+      return buf;
+    }
+    if (lo > hi) {
+      std::snprintf(buf, sizeof buf, "row %d has lower bound %g above upper bound %g", i, lo, hi);
+      return buf;
+    }
+  }
+  if (std::isnan(p.objective_offset)) return "objective offset is NaN";
+  return "";
+}
+
+// apply_pass (src/la/scaling.cpp:14-40): the reference rebuilds the matrix through
+// add_entry + finalize(0.0), which keeps pattern and order, i.e. value * row_pass * col_pass.
+static void apply_pass(const sankhya_pdhg_problem& p, Scaling& s, const std::vector<double>& rp,
+                       const std::vector<double>& cp) {
+  for (int j = 0; j < p.num_cols; ++j) {
+    const double cj = cp[j];
+    for (int k = p.col_starts[j]; k < p.col_starts[j + 1]; ++k) {
+      s.values[k] = s.values[k] * rp[p.row_indices[k]] * cj;
+    }
+  }
+  for (int i = 0; i < p.num_rows; ++i) s.dr[i] *= rp[i];
+  for (int j = 0; j < p.num_cols; ++j) s.dc[j] *= cp[j];
+}
+
+Scaling build_scaling(const sankhya_pdhg_problem& p, const std::vector<double>& min_cost,
+                      int ruiz_rounds) {
+  const int m = p.num_rows, n = p.num_cols;
+  Scaling s;
+  s.dr.assign(m, 1.0);
+  s.dc.assign(n, 1.0);
+  s.values.assign(p.values, p.values + p.num_nonzeros);
+  std::vector<double> ra(m), ca(n), rp(m), cp(n);
+  // ruiz_round (scaling.cpp:44-72): 1/sqrt(max |a|) per row and column
+  for (int round = 0; round < ruiz_rounds; ++round) {
+    std::fill(ra.begin(), ra.end(), 0.0);
+    std::fill(ca.begin(), ca.end(), 0.0);
+    for (int j = 0; j < n; ++j) {
+      for (int k = p.col_starts[j]; k < p.col_starts[j + 1]; ++k) {
+        const double mag = std::fabs(s.values[k]);
+        double& r = ra[p.row_indices[k]];
+        r = std::max(r, mag);
+        ca[j] = std::max(ca[j], mag);
+      }
+    }
+    for (int i = 0; i < m; ++i) rp[i] = ra[i] > 0.0 ? 1.0 / std::sqrt(ra[i]) : 1.0;
+    for (int j = 0; j < n; ++j) cp[j] = ca[j] > 0.0 ? 1.0 / std::sqrt(ca[j]) : 1.0;
+    apply_pass(p, s, rp, cp);
+  }
+  // pock_chambolle_round (scaling.cpp:76-100), alpha = 1: 1/sqrt(sum |a|)
+  std::fill(ra.begin(), ra.end(), 0.0);
+  std::fill(ca.begin(), ca.end(), 0.0);
+  for (int j = 0; j < n; ++j) {
+    for (int k = p.col_starts[j]; k < p.col_starts[j + 1]; ++k) {
+      const double mag = std::fabs(s.values[k]);
+      ra[p.row_indices[k]] += mag;
+      ca[j] += mag;
+    }
+  }
+  for (int i = 0; i < m; ++i) rp[i] = ra[i] > 0.0 ? 1.0 / std::sqrt(ra[i]) : 1.0;
+  for (int j = 0; j < n; ++j) cp[j] = ca[j] > 0.0 ? 1.0 / std::sqrt(ca[j]) : 1.0;
+  apply_pass(p, s, rp, cp);
+  // vectors (scaling.cpp:124-145); scale_bound multiplies by 1/dc, it does not divide
+  s.cost.resize(n);
+  s.cl.resize(n);
+  s.cu.resize(n);
+  for (int j = 0; j < n; ++j) {
+    const double dc = s.dc[j];
+    s.cost[j] = min_cost[j] * dc;
+    s.cl[j] = host_finite_bound(p.col_lower[j]) ? p.col_lower[j] * (1.0 / dc) : p.col_lower[j];
+    s.cu[j] = host_finite_bound(p.col_upper[j]) ? p.col_upper[j] * (1.0 / dc) : p.col_upper[j];
+  }
+  s.rl.resize(m);
+  s.ru.resize(m);
+  for (int i = 0; i < m; ++i) {
+    const double dr = s.dr[i];
+    s.rl[i] = host_finite_bound(p.row_lower[i]) ? p.row_lower[i] * dr : p.row_lower[i];
+    s.ru[i] = host_finite_bound(p.row_upper[i]) ? p.row_upper[i] * dr : p.row_upper[i];
+  }
+  return s;
+}
+
+static std::vector<int> order_by_count_desc(const std::vector<int>& count) {
+  std::vector<int> order(count.size());
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return count[a] > count[b]; });
+  return order;
+}
+
+PermutedLp permute(const sankhya_pdhg_problem& p, const std::vector<double>& v) {
+  PermutedLp q;
+  const int m = p.num_rows, n = p.num_cols;
+  q.m = m;
+  q.n = n;
+  q.nnz = p.num_nonzeros;
+  std::vector<int> rc(m, 0), cc(n, 0);
+  for (int j = 0; j < n; ++j) cc[j] = p.col_starts[j + 1] - p.col_starts[j];
+  for (long long k = 0; k < q.nnz; ++k) ++rc[p.row_indices[k]];
+  q.row_perm = order_by_count_desc(rc);
+  q.col_perm = order_by_count_desc(cc);
+  std::vector<int> row_pos(m), col_pos(n);
+  for (int t = 0; t < m; ++t) row_pos[q.row_perm[t]] = t;
+  for (int t = 0; t < n; ++t) col_pos[q.col_perm[t]] = t;
+  // A: rows in permuted order; walking permuted columns in order keeps each row ascending
+  q.a_ptr.assign(m + 1, 0);
+  for (int t = 0; t < m; ++t) q.a_ptr[t + 1] = q.a_ptr[t] + rc[q.row_perm[t]];
+  q.a_idx.resize(q.nnz);
+  q.a_val.resize(q.nnz);
+  std::vector<int> next(q.a_ptr.begin(), q.a_ptr.end() - 1);
+  for (int t = 0; t < n; ++t) {
+    const int j = q.col_perm[t];
+    for (int k = p.col_starts[j]; k < p.col_starts[j + 1]; ++k) {
+      const int slot = next[row_pos[p.row_indices[k]]]++;
+      q.a_idx[slot] = t;
+      q.a_val[slot] = v[k];
+    }
+  }
+  // A': rows are permuted columns; walking permuted rows in order keeps each ascending
+  q.at_ptr.assign(n + 1, 0);
+  for (int t = 0; t < n; ++t) q.at_ptr[t + 1] = q.at_ptr[t] + cc[q.col_perm[t]];
+  q.at_idx.resize(q.nnz);
+  q.at_val.resize(q.nnz);
+  next.assign(q.at_ptr.begin(), q.at_ptr.end() - 1);
+  for (int t = 0; t < m; ++t) {
+    for (int k = q.a_ptr[t]; k < q.a_ptr[t + 1]; ++k) {
+      const int slot = next[q.a_idx[k]]++;
+      q.at_idx[slot] = t;
+      q.at_val[slot] = q.a_val[k];
+    }
+  }
+  return q;
+}
+
+static int lanes_for(int len) {
+  // smallest power of two with at most four nonzeros per lane, capped at a warp
+  int lanes = 1;
+  while (lanes < 32 && lanes * 4 < len) lanes *= 2;
+  return lanes;
+}
+
+HostPart partition(const std::vector<int>& ptr, int G, int warps_per_block, int lanes_override) {
+  constexpr int kSeg = 256;  // == kSegment in pdhg_kernels.cuh
+  const int rows = static_cast<int>(ptr.size()) - 1;
+  const auto len = [&](int r) { return ptr[r + 1] - ptr[r]; };
+  const auto cost = [&](int r) { return static_cast<double>(len(r)) + 2.0; };
+  double total = 0.0;
+  for (int r = 0; r < rows; ++r) total += cost(r);
+  const double target = total / G;
+  // long rows: the prefix longer than one segment (rows are sorted longest first)
+  int L = 0;
+  while (L < rows && len(L) > kSeg) ++L;
+  // LPT assignment of long rows to blocks
+  std::vector<double> load(G, 0.0);
+  std::vector<std::vector<int>> blk_long(G);
+  using Entry = std::pair<double, int>;
+  std::priority_queue<Entry, std::vector<Entry>, std::greater<Entry>> heap;
+  for (int b = 0; b < G; ++b) heap.push({0.0, b});
+  for (int r = 0; r < L; ++r) {
+    auto [l, b] = heap.top();
+    heap.pop();
+    blk_long[b].push_back(r);
+    load[b] = l + cost(r);
+    heap.push({load[b], b});
+  }
+  HostPart hp;
+  hp.blk_seg_begin.assign(G + 1, 0);
+  hp.blk_long_begin.assign(G + 1, 0);
+  for (int b = 0; b < G; ++b) {
+    for (int r : blk_long[b]) {
+      const int first = static_cast<int>(hp.segs.size());
+      int count = 0;
+      for (int k = ptr[r]; k < ptr[r + 1]; k += kSeg) {
+        hp.segs.push_back(make_int4(r, k, std::min(k + kSeg, ptr[r + 1]), 0));
+        ++count;
+      }
+      hp.longs.push_back(make_int4(r, first, count, 0));
+    }
+    hp.blk_seg_begin[b + 1] = static_cast<int>(hp.segs.size());
+    hp.blk_long_begin[b + 1] = static_cast<int>(hp.longs.size());
+  }
+  // items of short rows, a few per warp
+  const double budget = std::max(64.0, target / (2.0 * warps_per_block));
+  std::vector<int4> items;
+  std::vector<double> item_cost;
+  for (int r = L; r < rows;) {
+    const int lanes = lanes_override > 0 ? lanes_override : lanes_for(len(r));
+    const int begin = r;
+    double c = 0.0;
+    while (r < rows && (r == begin || (c + cost(r) <= budget &&
+                                       (lanes_override > 0 || lanes_for(len(r)) == lanes)))) {
+      c += cost(r);
+      ++r;
+    }
+    items.push_back(make_int4(begin, r, lanes, 0));
+    item_cost.push_back(c);
+  }
+  // contiguous runs of items: block b's capacity is what its long rows leave of the common
+  // target; capacities are scaled to the short-row total and filled cumulatively
+  double short_total = 0.0, capsum = 0.0;
+  for (double c : item_cost) short_total += c;
+  std::vector<double> cap(G);
+  for (int b = 0; b < G; ++b) {
+    cap[b] = std::max(0.0, target - load[b]);
+    capsum += cap[b];
+  }
+  const double f = capsum > 0.0 ? short_total / capsum : 0.0;
+  hp.blk_item_begin.assign(G + 1, 0);
+  size_t it = 0;
+  double bound = 0.0, acc = 0.0;
+  for (int b = 0; b < G; ++b) {
+    bound += cap[b] * f;
+    while (it < items.size() && (b == G - 1 || acc + item_cost[it] * 0.5 <= bound)) {
+      acc += item_cost[it];
+      ++it;
+    }
+    hp.blk_item_begin[b + 1] = static_cast<int>(it);
+  }
+  hp.items = std::move(items);
+  return hp;
+}
+
+// mt19937 (Matsumoto & Nishimura) and libstdc++'s generate_canonical<double, 53> for a
+// 32-bit engine: (g0 + g1 * 2^32) / 2^64, clamped below 1.
+void uniform_draws(uint32_t seed, double lo, double hi, size_t count, double* out) {
+  uint32_t st[624];
+  st[0] = seed;
+  for (int k = 1; k < 624; ++k) st[k] = 1812433253u * (st[k - 1] ^ (st[k - 1] >> 30)) + k;
+  int index = 624;
+  const auto next = [&]() {
+    if (index >= 624) {
+      for (int k = 0; k < 624; ++k) {
+        const uint32_t y = (st[k] & 0x80000000u) | (st[(k + 1) % 624] & 0x7fffffffu);
+        st[k] = st[(k + 397) % 624] ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
+      }
+      index = 0;
+    }
+    uint32_t y = st[index++];
+    y ^= y >> 11;
+    y ^= (y << 7) & 0x9d2c5680u;
+    y ^= (y << 15) & 0xefc60000u;
+    y ^= y >> 18;
+    return y;
+  };
+  for (size_t t = 0; t < count; ++t) {
+    double sum = 0.0, tmp = 1.0;
+    for (int k = 0; k < 2; ++k) {
+      sum += static_cast<double>(next()) * tmp;
+      tmp *= 4294967296.0;
+    }
+    double r = sum / tmp;
+    if (r >= 1.0) r = std::nextafter(1.0, 0.0);
+    out[t] = (r * (hi - lo)) + lo;
+  }
+}
+
+}  // namespace sih26

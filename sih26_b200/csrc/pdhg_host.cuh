@@ -1,0 +1,61 @@
+// Host-side preparation of one LP for the PDHG kernels: validation, diagonal scaling,
+// permuted CSR copies of A and A', and the SpMV work partition.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "sankhya_pdhg_gpu.h"
+
+namespace sih26 {
+
+// An error that ends a call: `code` is a sankhya_pdhg_gpu_status.
+struct Failure {
+  int code;
+  std::string message;
+};
+
+bool host_finite_bound(double v);
+
+// Structural checks of the C-ABI input (sizes, pointers, CSC well-formedness). Throws Failure
+// with SANKHYA_GPU_INVALID_ARGUMENT; these are inputs the reference's frozen SparseMatrix can
+// never hold.
+void check_structure(const sankhya_pdhg_problem& p);
+
+// Model::validate for an LP (src/core/model.cpp:125-210): returns "" or the first problem.
+std::string validate_model(const sankhya_pdhg_problem& p);
+
+// build_scaling (src/la/scaling.cpp:111-158): 10 Ruiz rounds then one Pock-Chambolle round,
+// in the reference's order of operations, so Dr and Dc are bit-identical to it.
+struct Scaling {
+  std::vector<double> dr, dc, values, cost, cl, cu, rl, ru;
+};
+Scaling build_scaling(const sankhya_pdhg_problem& p, const std::vector<double>& min_cost,
+                      int ruiz_rounds);
+
+// Rows of A and of A' each sorted by nonzero count, longest first (stable), with CSR copies
+// in that order whose column indices point into the other permuted space.
+struct PermutedLp {
+  int m = 0, n = 0;
+  long long nnz = 0;
+  std::vector<int> row_perm, col_perm;  // position -> original index
+  std::vector<int> a_ptr, a_idx, at_ptr, at_idx;
+  std::vector<double> a_val, at_val;
+};
+PermutedLp permute(const sankhya_pdhg_problem& p, const std::vector<double>& scaled_values);
+
+// Work partition of one CSR matrix over G blocks (see Part in pdhg_kernels.cuh).
+struct HostPart {
+  std::vector<int> blk_seg_begin, blk_long_begin, blk_item_begin;
+  std::vector<int4> segs, longs, items;
+};
+HostPart partition(const std::vector<int>& ptr, int G, int warps_per_block, int lanes_override);
+
+// mt19937 + uniform_real_distribution<double>(lo, hi) as libstdc++ draws it: the random start
+// of estimate_spectral_norm (src/la/scaling.cpp:168-171).
+void uniform_draws(uint32_t seed, double lo, double hi, size_t count, double* out);
+
+}  // namespace sih26

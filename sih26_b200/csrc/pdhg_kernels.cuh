@@ -1,0 +1,774 @@
+// Restarted-PDHG kernels for sm_100a.
+//
+// Iteration = src/pdhg/pdhg.cpp:383-644 restructured for one GPU:
+//
+//   iterate_kernel (cooperative, persistent over a chunk of attempts)
+//     phase P  (rows of A' = columns of A, resident CSR of A'):
+//              g_j = (A' y)_j, x'_j = proj(x_j - tau (c_j + g_j)), partial sum of (x'-x)^2,
+//              and the running sum x_sum += x for the iterate accepted last attempt
+//     barrier
+//     phase D  (rows of A, resident CSR of A):
+//              a'_i = (A x')_i, abar = 2 a' - a, adx = a' - a   (a = A x kept from the
+//              accepted iterate: one SpMV gives both A xbar and A dx, pdhg.cpp:403,432),
+//              y'_i = v - sigma proj(v / sigma, [rl, ru]), v = y + sigma abar,
+//              partial sums of (y'-y)^2 and (y'-y) adx, and y_sum += y
+//     barrier
+//     control  every block reduces the same partials in the same order, so every block
+//              takes the same accept / step-size decision (pdhg.cpp:413-496) without
+//              another barrier
+//   evaluate_kernel (cooperative), after every 40th accepted iteration or a step without
+//     information (pdhg.cpp:502-503): unscaled FP64 residuals of the current iterate and of
+//     the running average (pdhg.cpp:143-263), candidate choice, best point, stopping test
+//     and restart with the primal-weight update (pdhg.cpp:505-643).
+//
+// Internal index spaces are permuted: rows of A sorted by nonzero count (descending) and
+// columns likewise, so a work item holds rows of similar length; the host un-permutes
+// outputs. Reductions use fixed trees over a fixed work partition, so a run is bit-for-bit
+// repeatable.
+#pragma once
+
+#include <cstdint>
+
+#include "device_common.cuh"
+
+namespace sih26 {
+
+// Solver states (Ctrl::state).
+enum : int {
+  kRunning = 0,
+  kNeedEval = 1,
+  kConverged = 2,
+  kIterationLimit = 3,
+  kTimeLimit = 4,
+  kDeviceError = 5
+};
+
+// Host <-> device control block; one per LP. Written only by block 0 at kernel exit; every
+// block reads it at kernel entry.
+struct Residuals {
+  double primal, dual, gap, primal_objective, dual_objective, absolute_primal, absolute_dual,
+      gap_as_verified, complementarity;
+};
+
+struct Ctrl {
+  // step state
+  double eta, omega, restart_kkt, best_worst;
+  long long iteration, attempts, averaged, last_restart, restarts, evaluations;
+  int cur, pending, state, converged;
+  int chosen_average, best_is_set, pad0, pad1;
+  Residuals best, current, average;  // best so far; last evaluation's two candidates
+  // constants of the solve
+  double spectral_norm, eta_ceiling, tolerance, bound_norm, cost_norm;
+  long long iteration_limit;
+  int use_restarts, stop_at_request, stop_rule, pad2;
+  int time_up, pad3;
+};
+
+// SpMV work partition of one CSR matrix in permuted row order (rows sorted by length,
+// longest first). Per block b:
+//   segments  [blk_seg_begin[b], blk_seg_begin[b+1]): {row, nz_begin, nz_end, 0} pieces of at
+//             most kSegment nonzeros of this block's long rows, one warp each;
+//   long rows [blk_long_begin[b], blk_long_begin[b+1]): {row, first segment, segments, 0};
+//             after the block's segments are done, one warp sums a long row's segment
+//             partials in segment order and runs the row's epilogue;
+//   items     [blk_item_begin[b], blk_item_begin[b+1]): {row_begin, row_end, lanes, 0} runs
+//             of short rows, each row reduced by a group of `lanes` lanes.
+// Every long row lives in one block, so no partial crosses blocks and no atomics are needed.
+constexpr int kSegment = 256;
+
+struct Part {
+  const int* blk_seg_begin;
+  const int4* segs;
+  const int* blk_long_begin;
+  const int4* longs;
+  const int* blk_item_begin;
+  const int4* items;
+  double* seg_sum;  // [segments * 2] scratch
+};
+
+template <class T>
+struct Csr {
+  const int* ptr;
+  const int* idx;
+  const T* val;
+  const double* val64;  // FP64 values (== val when T is double)
+};
+
+template <class T>
+struct Prob {
+  int m, n;
+  Csr<T> A, AT;
+  Part pa, pat;
+  // scaled problem, permuted (src/la/scaling.hpp:36-58)
+  const T* c;
+  const T* cl;
+  const T* cu;
+  const T* rl;
+  const T* ru;
+  const double* dr;  // row scaling Dr, permuted
+  const double* dc;  // column scaling Dc, permuted
+  // unscaled problem, permuted; c0 is the min-space cost (pdhg.cpp:287-291)
+  const double* c0;
+  const double* cl0;
+  const double* cu0;
+  const double* rl0;
+  const double* ru0;
+};
+
+template <class T>
+struct State {
+  T* x[2];
+  T* y[2];
+  double* ax[2];
+  double* xsum;
+  double* ysum;
+  T* xr;
+  T* yr;
+  double* xavg;
+  double* yavg;
+  double* best_x;  // scaled, FP64
+  double* best_y;
+  double* partials;  // [2][G][kPartSlots]
+  Ctrl* ctrl;
+  GridBarrier bar;
+};
+
+constexpr int kPartSlots = 20;
+constexpr int kEvalSlots = 16;
+// complementarity slots of the evaluation are max-reductions
+constexpr unsigned kEvalMaxMask = (1u << 6) | (1u << 7) | (1u << 12) | (1u << 13);
+
+template <class T>
+__device__ __forceinline__ double ld(const T* p) {
+  return static_cast<double>(__ldcg(p));
+}
+template <class T>
+__device__ __forceinline__ double ro(const T* p) {
+  return static_cast<double>(__ldg(p));
+}
+
+// ---- generic fused SpMV phase ----------------------------------------------------------
+//
+// For every row r of the matrix owned by this block: s = sum_k val[k] * gather(idx[k])
+// (NV gathered vectors at once, FP64 accumulation), then epi(r, s, acc). Block rows are
+// reduced over the whole block; short rows over a group of `lanes` lanes.
+template <int NV, int NS, class V, class Gather, class Epi>
+__device__ __forceinline__ void run_phase(const int* __restrict__ ptr, const int* __restrict__ idx,
+                                          const V* __restrict__ val, const Part& p,
+                                          const Gather& g, const Epi& epi, double (&acc)[NS]) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int b = blockIdx.x;
+  // 1. segments of long rows: one warp per segment of <= kSegment nonzeros
+  const int sb = __ldg(p.blk_seg_begin + b), se = __ldg(p.blk_seg_begin + b + 1);
+  for (int q = sb + warp; q < se; q += kWarps) {
+    const int4 sg = __ldg(p.segs + q);
+    double s[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) s[v] = 0.0;
+#pragma unroll 8
+    for (int k = sg.y + lane; k < sg.z; k += 32) g.add(s, ro(val + k), __ldg(idx + k));
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) s[v] += __shfl_xor_sync(0xffffffffu, s[v], off);
+    }
+    if (lane == 0) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) p.seg_sum[(size_t)q * NV + v] = s[v];
+    }
+  }
+  // 2. short rows
+  const int ib = __ldg(p.blk_item_begin + b), ie = __ldg(p.blk_item_begin + b + 1);
+  for (int it = ib + warp; it < ie; it += kWarps) {
+    const int4 item = __ldg(p.items + it);
+    const int lanes = item.z;
+    const int groups = 32 / lanes;
+    const int gid = lane / lanes, gl = lane - gid * lanes;
+    for (int base = item.x; base < item.y; base += groups) {
+      const int r = base + gid;
+      const bool valid = r < item.y;
+      double s[NV];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) s[v] = 0.0;
+      if (valid) {
+        const int kb = __ldg(ptr + r), ke = __ldg(ptr + r + 1);
+#pragma unroll 4
+        for (int k = kb + gl; k < ke; k += lanes) g.add(s, ro(val + k), __ldg(idx + k));
+      }
+      for (int off = lanes >> 1; off > 0; off >>= 1) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) s[v] += __shfl_xor_sync(0xffffffffu, s[v], off);
+      }
+      if (valid && gl == 0) epi(r, s, acc);
+    }
+  }
+  // 3. long rows: sum the block's segment partials in segment order, then the epilogue
+  const int lb = __ldg(p.blk_long_begin + b), le = __ldg(p.blk_long_begin + b + 1);
+  if (le > lb) {
+    __syncthreads();
+    for (int q = lb + warp; q < le; q += kWarps) {
+      const int4 lr = __ldg(p.longs + q);
+      double s[NV];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) s[v] = 0.0;
+      for (int k = lane; k < lr.z; k += 32) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) s[v] += p.seg_sum[(size_t)(lr.y + k) * NV + v];
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) s[v] += __shfl_xor_sync(0xffffffffu, s[v], off);
+      }
+      if (lane == 0) epi(lr.x, s, acc);
+    }
+  }
+}
+
+// ---- gathers -------------------------------------------------------------------------
+
+template <class T>
+struct Gather1 {
+  const T* v;
+  __device__ __forceinline__ void add(double (&s)[1], double a, int k) const { s[0] += a * ld(v + k); }
+};
+
+template <class T, class U>
+struct Gather2 {
+  const T* v0;
+  const U* v1;
+  __device__ __forceinline__ void add(double (&s)[2], double a, int k) const {
+    s[0] += a * ld(v0 + k);
+    s[1] += a * ld(v1 + k);
+  }
+};
+
+// ---- epilogues of the iteration ---------------------------------------------------------
+
+// x' = proj_X(x - tau (c + A'y))  (pdhg.cpp:392-400); slot 0 gets (x'-x)^2.
+template <class T>
+struct PrimalStep {
+  const T* x;
+  T* xn;
+  const T* c;
+  const T* cl;
+  const T* cu;
+  double* xsum;
+  double tau;
+  int pending;
+  __device__ __forceinline__ void operator()(int j, const double (&s)[1], double (&acc)[3]) const {
+    const double xo = ld(x + j);
+    if (pending) xsum[j] = __ldcg(xsum + j) + xo;
+    const double xnew = project(xo - tau * (ro(c + j) + s[0]), ro(cl + j), ro(cu + j));
+    const T xs = static_cast<T>(xnew);
+    xn[j] = xs;
+    const double d = static_cast<double>(xs) - xo;
+    acc[0] += d * d;
+  }
+};
+
+// y' = v - sigma proj_C(v / sigma), v = y + sigma A xbar  (pdhg.cpp:402-408);
+// slots 1, 2 get (y'-y)^2 and (y'-y) (A dx)_i.
+template <class T>
+struct DualStep {
+  const T* y;
+  T* yn;
+  const double* ax;
+  double* axn;
+  const T* rl;
+  const T* ru;
+  double* ysum;
+  double sigma;
+  int pending;
+  __device__ __forceinline__ void operator()(int i, const double (&s)[1], double (&acc)[3]) const {
+    const double yo = ld(y + i);
+    if (pending) ysum[i] = __ldcg(ysum + i) + yo;
+    const double anew = s[0];
+    const double aold = __ldcg(ax + i);
+    const double v = yo + sigma * (2.0 * anew - aold);
+    const double ynew = v - sigma * project(v / sigma, ro(rl + i), ro(ru + i));
+    const T ys = static_cast<T>(ynew);
+    yn[i] = ys;
+    axn[i] = anew;
+    const double d = static_cast<double>(ys) - yo;
+    acc[1] += d * d;
+    acc[2] += d * (anew - aold);
+  }
+};
+
+// Sum (or max) of kPartSlots-wide block partials over all blocks, in block order. Every
+// block calls it after a barrier and gets identical totals.
+template <int NS, unsigned MAXMASK>
+__device__ __forceinline__ void reduce_partials(const double* partials, int first_slot,
+                                                double (&tot)[NS], double* sh) {
+  const int G = gridDim.x;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) tot[s] = 0.0;
+  for (int b = threadIdx.x; b < G; b += kThreads) {
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      const double v = __ldcg(partials + (size_t)b * kPartSlots + first_slot + s);
+      tot[s] = ((MAXMASK >> s) & 1u) ? dmax(tot[s], v) : tot[s] + v;
+    }
+  }
+  block_reduce<NS, MAXMASK>(tot, sh);
+}
+
+__device__ __forceinline__ void write_partials(double* partials, int first_slot, const double* v,
+                                               int ns) {
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < ns; ++s) partials[(size_t)blockIdx.x * kPartSlots + first_slot + s] = v[s];
+  }
+}
+
+// ---- the iteration kernel ---------------------------------------------------------------
+
+template <class T>
+__global__ void __launch_bounds__(kThreads) iterate_kernel(Prob<T> P, State<T> S,
+                                                           long long max_attempts) {
+  __shared__ Ctrl c;
+  __shared__ double sh[kWarps * 4];
+  if (threadIdx.x == 0) c = *S.ctrl;
+  __syncthreads();
+  if (c.state != kRunning) return;
+  const int G = gridDim.x;
+  long long a = 0;
+  for (;;) {
+    // loop top (pdhg.cpp:384-385)
+    if (c.iteration >= c.iteration_limit) {
+      if (threadIdx.x == 0) c.state = kIterationLimit;
+      break;
+    }
+    if (c.time_up) {
+      if (threadIdx.x == 0) c.state = kTimeLimit;
+      break;
+    }
+    if (a >= max_attempts) break;
+    ++a;
+    const int cur = c.cur, nxt = cur ^ 1;
+    const double tau = c.eta / c.omega;
+    const double sigma = c.eta * c.omega;
+    double* part = S.partials + (size_t)(c.attempts & 1) * G * kPartSlots;
+    double acc[3] = {0.0, 0.0, 0.0};
+
+    PrimalStep<T> ps{S.x[cur], S.x[nxt], P.c, P.cl, P.cu, S.xsum, tau, c.pending};
+    run_phase<1, 3>(P.AT.ptr, P.AT.idx, P.AT.val, P.pat, Gather1<T>{S.y[cur]}, ps, acc);
+    if (!grid_barrier(S.bar)) goto device_error;
+
+    {
+      DualStep<T> ds{S.y[cur], S.y[nxt], S.ax[cur], S.ax[nxt], P.rl, P.ru, S.ysum, sigma, c.pending};
+      run_phase<1, 3>(P.A.ptr, P.A.idx, P.A.val, P.pa, Gather1<T>{S.x[nxt]}, ds, acc);
+    }
+    block_reduce<3, 0u>(acc, sh);
+    write_partials(part, 0, acc, 3);
+    if (!grid_barrier(S.bar)) goto device_error;
+
+    {
+      double tot[3];
+      reduce_partials<3, 0u>(part, 0, tot, sh);
+      if (threadIdx.x == 0) {
+        // adaptive step size, pdhg.cpp:413-496
+        const double movement = 0.5 * c.omega * tot[0] + 0.5 * tot[1] / c.omega;
+        const double interaction = fabs(tot[2]);
+        const bool no_information = interaction <= 0.0;
+        const double limit = no_information ? INFINITY : movement / interaction;
+        const double exponent = (double)(c.iteration + 1 > 2 ? c.iteration + 1 : 2);
+        const double shrink = 1.0 - pow(exponent, -0.3);
+        const double grow = 1.0 + pow(exponent, -0.6);
+        const double proposed = dmin(shrink * limit, grow * c.eta);
+        const bool accept = c.eta <= limit;
+        if (accept) {
+          c.cur ^= 1;
+          ++c.averaged;
+          ++c.iteration;
+        }
+        c.pending = accept ? 1 : 0;
+        if (!no_information) {
+          c.eta = proposed < 1e-12 ? 1e-12 : (c.eta_ceiling < proposed ? c.eta_ceiling : proposed);
+        }
+        ++c.attempts;
+        c.time_up = *((volatile int*)S.bar.time_up);
+        if (c.iteration != 0 && (c.iteration % 40 == 0 || no_information)) c.state = kNeedEval;
+      }
+      __syncthreads();
+      if (c.state != kRunning) break;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *S.ctrl = c;
+  return;
+device_error:
+  if (blockIdx.x == 0 && threadIdx.x == 0) S.ctrl->state = kDeviceError;
+}
+
+// ---- evaluation ---------------------------------------------------------------------------
+
+// Row terms of evaluate() (pdhg.cpp:152-170, 205-222, 227-238) for NC candidates.
+// slots: 0/1 primal violation^2, 2/3 support, 4/5 row dual violation^2, 6/7 complementarity.
+template <class T, int NC>
+struct RowEval {
+  const double* dr;
+  const double* rl0;
+  const double* ru0;
+  const T* y;          // candidate 0 (scaled)
+  const double* yavg;  // candidate 1 (scaled)
+  const double* ycand; // when non-null: candidate 0 in FP64 (the report)
+  __device__ __forceinline__ void operator()(int i, const double (&s)[NC], double (&acc)[kEvalSlots]) const {
+    const double d_r = __ldg(dr + i);
+    const double lo = __ldg(rl0 + i), hi = __ldg(ru0 + i);
+#pragma unroll
+    for (int q = 0; q < NC; ++q) {
+      const double act = s[q] / d_r;
+      const double ys = q == 0 ? (ycand ? __ldcg(ycand + i) : ld(y + i)) : __ldcg(yavg + i);
+      const double yi = ys * d_r;
+      double viol = 0.0;
+      if (finite_bound(lo)) viol = dmax(viol, lo - act);
+      if (finite_bound(hi)) viol = dmax(viol, act - hi);
+      acc[0 + q] += viol * viol;
+      if (yi > 0.0) {
+        if (finite_bound(hi)) acc[2 + q] += yi * hi; else acc[4 + q] += yi * yi;
+      } else if (yi < 0.0) {
+        if (finite_bound(lo)) acc[2 + q] += yi * lo; else acc[4 + q] += yi * yi;
+      }
+      if (lo != hi) {
+        const double ls = finite_bound(lo) ? act - lo : INFINITY;
+        const double us = finite_bound(hi) ? hi - act : INFINITY;
+        acc[6 + q] = dmax(acc[6 + q], fabs(yi) * dmin(ls, us));
+      }
+    }
+  }
+};
+
+// Column terms (pdhg.cpp:172-199, 239-256). slots: 8/9 dual violation^2, 10/11 bound
+// contribution, 12/13 complementarity, 14/15 primal objective. The report variant also
+// writes the unscaled point and reduced costs.
+template <class T, int NC>
+struct ColEval {
+  const double* dc;
+  const double* cl0;
+  const double* cu0;
+  const double* c0;
+  const T* x;
+  const double* xavg;
+  const double* xcand;  // report: candidate 0 in FP64
+  double* x_out;        // report outputs (unscaled, permuted order)
+  double* reduced_out;
+  __device__ __forceinline__ void operator()(int j, const double (&s)[NC], double (&acc)[kEvalSlots]) const {
+    const double d_c = __ldg(dc + j);
+    const double lo = __ldg(cl0 + j), hi = __ldg(cu0 + j), cj = __ldg(c0 + j);
+#pragma unroll
+    for (int q = 0; q < NC; ++q) {
+      const double d = cj + s[q] / d_c;
+      const double xs = q == 0 ? (xcand ? __ldcg(xcand + j) : ld(x + j)) : __ldcg(xavg + j);
+      const double xj = xs * d_c;
+      if (x_out && q == 0) {
+        x_out[j] = xj;
+        reduced_out[j] = d;
+      }
+      if (d > 0.0) {
+        if (finite_bound(lo)) acc[10 + q] += d * lo; else acc[8 + q] += d * d;
+      } else if (d < 0.0) {
+        if (finite_bound(hi)) acc[10 + q] += d * hi; else acc[8 + q] += d * d;
+      }
+      if (lo != hi) {
+        const double ls = finite_bound(lo) ? xj - lo : INFINITY;
+        const double us = finite_bound(hi) ? hi - xj : INFINITY;
+        acc[12 + q] = dmax(acc[12 + q], fabs(d) * dmin(ls, us));
+      }
+      acc[14 + q] += cj * xj;
+    }
+  }
+};
+
+__device__ __forceinline__ Residuals make_residuals(const double* t, int q, double bound_norm,
+                                                    double cost_norm) {
+  Residuals r;
+  r.absolute_primal = sqrt(t[0 + q]);
+  r.primal = r.absolute_primal / (1.0 + bound_norm);
+  r.absolute_dual = sqrt(t[8 + q] + t[4 + q]);
+  r.dual = r.absolute_dual / (1.0 + cost_norm);
+  r.complementarity = dmax(t[6 + q], t[12 + q]);
+  r.primal_objective = t[14 + q];
+  r.dual_objective = t[10 + q] - t[2 + q];
+  const double absolute_gap = fabs(r.primal_objective - r.dual_objective);
+  r.gap = absolute_gap / (1.0 + fabs(r.primal_objective) + fabs(r.dual_objective));
+  r.gap_as_verified = absolute_gap / dmax(1.0, fabs(r.primal_objective));
+  return r;
+}
+
+__device__ __forceinline__ double worst(const Residuals& r) { return dmax(dmax(r.primal, r.dual), r.gap); }
+
+// pdhg.cpp:119-131
+__device__ __forceinline__ bool meets_request(const Residuals& r, double tol) {
+  return r.primal <= tol && r.dual <= tol && r.gap <= tol && r.absolute_primal <= 1e-7;
+}
+__device__ __forceinline__ bool meets_project_standard(const Residuals& r) {
+  return r.absolute_primal <= 1e-7 && r.absolute_dual <= 1e-7 && r.gap_as_verified <= 1e-9 &&
+         r.complementarity <= 1e-6;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kThreads) evaluate_kernel(Prob<T> P, State<T> S) {
+  __shared__ Ctrl c;
+  __shared__ double sh[kWarps * kEvalSlots];
+  __shared__ int flags[3];  // best updated, restart, chosen average
+  if (threadIdx.x == 0) c = *S.ctrl;
+  __syncthreads();
+  if (c.state != kNeedEval) return;
+  const int G = gridDim.x;
+  const int cur = c.cur;
+  const int stride = G * kThreads;
+  const int gt = blockIdx.x * kThreads + threadIdx.x;
+  const bool has_average = c.averaged > 0;
+  const double count = (double)c.averaged;
+  double* part = S.partials;  // slots 0-1 restart movement, 2-17 residual terms
+
+  // E1: fold the pending running-sum term, form the scaled averages, and measure the
+  // movement since the last restart (pdhg.cpp:519-528, 613-624).
+  double acc1[2] = {0.0, 0.0};
+  for (int j = gt; j < P.n; j += stride) {
+    const double xo = ld(S.x[cur] + j);
+    const double xs = S.xsum[j] + (c.pending ? xo : 0.0);
+    S.xsum[j] = xs;
+    S.xavg[j] = has_average ? xs / count : 0.0;
+    const double d = xo - ld(S.xr + j);
+    acc1[0] += d * d;
+  }
+  for (int i = gt; i < P.m; i += stride) {
+    const double yo = ld(S.y[cur] + i);
+    const double ys = S.ysum[i] + (c.pending ? yo : 0.0);
+    S.ysum[i] = ys;
+    S.yavg[i] = has_average ? ys / count : 0.0;
+    const double d = yo - ld(S.yr + i);
+    acc1[1] += d * d;
+  }
+  block_reduce<2, 0u>(acc1, sh);
+  write_partials(part, 0, acc1, 2);
+  if (!grid_barrier(S.bar)) goto device_error;
+
+  {
+    // E2: both candidates' residual terms in one pass over each matrix (FP64 values).
+    double acc[kEvalSlots];
+#pragma unroll
+    for (int s = 0; s < kEvalSlots; ++s) acc[s] = 0.0;
+    RowEval<T, 2> re{P.dr, P.rl0, P.ru0, S.y[cur], S.yavg, nullptr};
+    run_phase<2, kEvalSlots>(P.A.ptr, P.A.idx, P.A.val64, P.pa,
+                             Gather2<T, double>{S.x[cur], S.xavg}, re, acc);
+    ColEval<T, 2> ce{P.dc, P.cl0, P.cu0, P.c0, S.x[cur], S.xavg, nullptr, nullptr, nullptr};
+    run_phase<2, kEvalSlots>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pat,
+                             Gather2<T, double>{S.y[cur], S.yavg}, ce, acc);
+    block_reduce<kEvalSlots, kEvalMaxMask>(acc, sh);
+    write_partials(part, 2, acc, kEvalSlots);
+  }
+  if (!grid_barrier(S.bar)) goto device_error;
+
+  {
+    double mv[2];
+    reduce_partials<2, 0u>(part, 0, mv, sh);
+    double t[kEvalSlots];
+    reduce_partials<kEvalSlots, kEvalMaxMask>(part, 2, t, sh);
+    if (threadIdx.x == 0) {
+      ++c.evaluations;
+      c.pending = 0;
+      const Residuals current = make_residuals(t, 0, c.bound_norm, c.cost_norm);
+      Residuals better = current;
+      int chosen_average = 0;
+      if (has_average) {
+        const Residuals average = make_residuals(t, 1, c.bound_norm, c.cost_norm);
+        c.average = average;
+        if (worst(average) < worst(current)) {
+          better = average;
+          chosen_average = 1;
+        }
+      }
+      c.current = current;
+      c.chosen_average = chosen_average;
+      int best_updated = 0, restart = 0;
+      if (worst(better) < c.best_worst) {
+        c.best = better;
+        c.best_worst = worst(better);
+        best_updated = 1;
+      }
+      bool stop_here;
+      if (c.stop_rule == 1) {
+        stop_here = worst(better) <= c.tolerance;
+      } else {
+        stop_here = meets_request(better, c.tolerance) &&
+                    (c.stop_at_request || meets_project_standard(better));
+      }
+      if (stop_here) {
+        c.best = better;
+        c.best_worst = worst(better);
+        best_updated = 1;
+        c.converged = 1;
+        c.state = kConverged;
+      } else {
+        c.state = kRunning;
+        if (c.use_restarts) {
+          const double kkt = worst(better);
+          const long long since = c.iteration - c.last_restart;
+          const bool sufficient = kkt <= 0.2 * c.restart_kkt;
+          const long long art = (long long)(0.36 * (double)c.iteration);
+          const bool artificial = since >= (art > 40 ? art : 40);
+          if (sufficient || artificial) {
+            const double dx_norm = sqrt(mv[0]), dy_norm = sqrt(mv[1]);
+            if (dx_norm > 1e-12 && dy_norm > 1e-12) {
+              const double theta = 0.5;
+              double w = exp(theta * log(dy_norm / dx_norm) + (1.0 - theta) * log(c.omega));
+              c.omega = w < 1e-6 ? 1e-6 : (1e6 < w ? 1e6 : w);
+            }
+            c.averaged = 0;
+            c.restart_kkt = kkt;
+            c.last_restart = c.iteration;
+            ++c.restarts;
+            restart = 1;
+          }
+        }
+      }
+      c.best_is_set |= best_updated;
+      flags[0] = best_updated;
+      flags[1] = restart;
+      flags[2] = chosen_average;
+    }
+    __syncthreads();
+  }
+
+  // E3: keep the best point (scaled, FP64) and reset the average at a restart.
+  if (flags[0] || flags[1]) {
+    for (int j = gt; j < P.n; j += stride) {
+      const double xo = ld(S.x[cur] + j);
+      if (flags[0]) S.best_x[j] = flags[2] ? S.xavg[j] : xo;
+      if (flags[1]) {
+        S.xr[j] = S.x[cur][j];
+        S.xsum[j] = 0.0;
+      }
+    }
+    for (int i = gt; i < P.m; i += stride) {
+      const double yo = ld(S.y[cur] + i);
+      if (flags[0]) S.best_y[i] = flags[2] ? S.yavg[i] : yo;
+      if (flags[1]) {
+        S.yr[i] = S.y[cur][i];
+        S.ysum[i] = 0.0;
+      }
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *S.ctrl = c;
+  return;
+device_error:
+  if (blockIdx.x == 0 && threadIdx.x == 0) S.ctrl->state = kDeviceError;
+}
+
+// Final report (pdhg.cpp:647-661): residuals of the best point, its unscaled value and
+// reduced costs. Writes the residual block to ctrl->best.
+template <class T>
+__global__ void __launch_bounds__(kThreads) report_kernel(Prob<T> P, State<T> S, double* x_out,
+                                                          double* reduced_out, double* y_out) {
+  __shared__ double sh[kWarps * kEvalSlots];
+  double acc[kEvalSlots];
+#pragma unroll
+  for (int s = 0; s < kEvalSlots; ++s) acc[s] = 0.0;
+  RowEval<T, 1> re{P.dr, P.rl0, P.ru0, nullptr, nullptr, S.best_y};
+  run_phase<1, kEvalSlots>(P.A.ptr, P.A.idx, P.A.val64, P.pa, Gather1<double>{S.best_x}, re, acc);
+  ColEval<T, 1> ce{P.dc, P.cl0, P.cu0, P.c0, nullptr, nullptr, S.best_x, x_out, reduced_out};
+  run_phase<1, kEvalSlots>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pat, Gather1<double>{S.best_y}, ce, acc);
+  const int stride = gridDim.x * kThreads;
+  for (int i = blockIdx.x * kThreads + threadIdx.x; i < P.m; i += stride) {
+    y_out[i] = __ldcg(S.best_y + i) * __ldg(P.dr + i);
+  }
+  block_reduce<kEvalSlots, kEvalMaxMask>(acc, sh);
+  write_partials(S.partials, 2, acc, kEvalSlots);
+  if (!grid_barrier(S.bar)) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) S.ctrl->state = kDeviceError;
+    return;
+  }
+  double t[kEvalSlots];
+  reduce_partials<kEvalSlots, kEvalMaxMask>(S.partials, 2, t, sh);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    S.ctrl->best = make_residuals(t, 0, S.ctrl->bound_norm, S.ctrl->cost_norm);
+  }
+}
+
+// ---- setup kernels ---------------------------------------------------------------------
+
+// ax = A x for the starting point (FP64 values). One warp per row (setup only).
+template <class T>
+__global__ void spmv_rows_kernel(int rows, const int* __restrict__ ptr, const int* __restrict__ idx,
+                                 const double* __restrict__ val, const T* x, double* out) {
+  const int lane = threadIdx.x & 31;
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int r = w; r < rows; r += nw) {
+    double s = 0.0;
+    for (int k = ptr[r] + lane; k < ptr[r + 1]; k += 32) s += val[k] * static_cast<double>(x[idx[k]]);
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if (lane == 0) out[r] = s;
+  }
+}
+
+// Power iteration on A'A for ||A||_2 (src/la/scaling.cpp:161-194), cooperative: per step
+// normalise v, u = A v, v = A' u, norm = ||v||^(1/2). Writes the estimate (x1.01) to *out.
+struct PowerState {
+  double* v;
+  double* u;
+  double* partials;
+  GridBarrier bar;
+};
+
+template <class T>
+struct PowerGather {
+  const double* v;
+  double inv;
+  __device__ __forceinline__ void add(double (&s)[1], double a, int k) const { s[0] += a * (__ldcg(v + k) * inv); }
+};
+
+struct StoreRow {
+  double* out;
+  __device__ __forceinline__ void operator()(int r, const double (&s)[1], double (&acc)[1]) const { out[r] = s[0]; }
+};
+struct StoreRowNorm {
+  double* out;
+  __device__ __forceinline__ void operator()(int r, const double (&s)[1], double (&acc)[1]) const {
+    out[r] = s[0];
+    acc[0] += s[0] * s[0];
+  }
+};
+
+template <class T>
+__global__ void __launch_bounds__(kThreads) power_kernel(Prob<T> P, PowerState W, int iterations,
+                                                         double* out) {
+  __shared__ double sh[kWarps * 2];
+  const int G = gridDim.x, stride = G * kThreads;
+  const int gt = blockIdx.x * kThreads + threadIdx.x;
+  double norm = 0.0;
+  // ||v||^2 of the random start
+  double a0[1] = {0.0};
+  for (int j = gt; j < P.n; j += stride) { const double t = __ldcg(W.v + j); a0[0] += t * t; }
+  block_reduce<1, 0u>(a0, sh);
+  write_partials(W.partials, 0, a0, 1);
+  if (!grid_barrier(W.bar)) return;
+  for (int step = 0; step < iterations; ++step) {
+    double len2[1];
+    reduce_partials<1, 0u>(W.partials + (size_t)(step & 1) * G * kPartSlots, 0, len2, sh);
+    const double length = sqrt(len2[0]);
+    if (length == 0.0) {
+      if (blockIdx.x == 0 && threadIdx.x == 0) *out = 1.0;
+      return;
+    }
+    double dummy[1] = {0.0};
+    run_phase<1, 1>(P.A.ptr, P.A.idx, P.A.val64, P.pa, PowerGather<T>{W.v, 1.0 / length},
+                    StoreRow{W.u}, dummy);
+    if (!grid_barrier(W.bar)) return;
+    double nx[1] = {0.0};
+    run_phase<1, 1>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pat, PowerGather<T>{W.u, 1.0},
+                    StoreRowNorm{W.v}, nx);
+    block_reduce<1, 0u>(nx, sh);
+    write_partials(W.partials + (size_t)((step + 1) & 1) * G * kPartSlots, 0, nx, 1);
+    if (!grid_barrier(W.bar)) return;
+    norm = 0.0;  // recomputed from the partials at the next step (or below)
+  }
+  double fin[1];
+  reduce_partials<1, 0u>(W.partials + (size_t)(iterations & 1) * G * kPartSlots, 0, fin, sh);
+  norm = sqrt(sqrt(fin[0]));
+  if (blockIdx.x == 0 && threadIdx.x == 0) *out = norm > 0.0 ? norm * 1.01 : 1.0;
+}
+
+}  // namespace sih26

@@ -1,0 +1,599 @@
+// The GPU restarted-PDHG solve behind the C ABI (include/sankhya_pdhg_gpu.h): host
+// orchestration of the kernels in pdhg_kernels.cuh.
+//
+// Replaces sankhya::pdhg::solve_pdhg (src/pdhg/pdhg.cpp:267-726). Setup (validation, scaling,
+// permutation, upload, norm estimate) runs once; the iteration loop then runs on the device
+// in chunks of cooperative launches, the host reading one control block per chunk.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <vector>
+
+#include "pdhg_host.cuh"
+#include "pdhg_kernels.cuh"
+#include "sankhya_pdhg_gpu.h"
+
+namespace sih26 {
+
+thread_local std::string g_last_error;
+
+#define SIH26_CUDA(expr, code)                                                           \
+  do {                                                                                   \
+    const cudaError_t e_ = (expr);                                                       \
+    if (e_ != cudaSuccess)                                                               \
+      throw Failure{code, std::string(#expr) + ": " + cudaGetErrorString(e_)};           \
+  } while (0)
+
+using Clock = std::chrono::steady_clock;
+static double seconds_since(Clock::time_point t0) {
+  return std::chrono::duration<double>(Clock::now() - t0).count();
+}
+
+// Owns every device allocation of one solve.
+class Arena {
+ public:
+  ~Arena() {
+    for (void* p : ptrs_) cudaFree(p);
+  }
+  template <class T>
+  T* alloc(size_t count) {
+    if (count == 0) count = 1;
+    void* p = nullptr;
+    SIH26_CUDA(cudaMalloc(&p, count * sizeof(T)), SANKHYA_GPU_OUT_OF_MEMORY);
+    ptrs_.push_back(p);
+    return static_cast<T*>(p);
+  }
+  template <class T>
+  T* zeros(size_t count) {
+    T* p = alloc<T>(count);
+    SIH26_CUDA(cudaMemset(p, 0, std::max<size_t>(count, 1) * sizeof(T)), SANKHYA_GPU_COPY_FAILED);
+    return p;
+  }
+  template <class T, class U>
+  T* upload(const std::vector<U>& host) {
+    T* p = alloc<T>(host.size());
+    if (!host.empty()) {
+      std::vector<T> conv(host.begin(), host.end());
+      SIH26_CUDA(cudaMemcpy(p, conv.data(), conv.size() * sizeof(T), cudaMemcpyHostToDevice),
+                 SANKHYA_GPU_COPY_FAILED);
+    }
+    return p;
+  }
+  template <class T>
+  T* upload_same(const std::vector<T>& host) {
+    T* p = alloc<T>(host.size());
+    if (!host.empty()) {
+      SIH26_CUDA(cudaMemcpy(p, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice),
+                 SANKHYA_GPU_COPY_FAILED);
+    }
+    return p;
+  }
+
+ private:
+  std::vector<void*> ptrs_;
+};
+
+template <class T>
+static std::vector<T> gather(const std::vector<T>& v, const std::vector<int>& perm) {
+  std::vector<T> out(perm.size());
+  for (size_t t = 0; t < perm.size(); ++t) out[t] = v[perm[t]];
+  return out;
+}
+template <class T>
+static std::vector<T> gather_ptr(const T* v, const std::vector<int>& perm) {
+  std::vector<T> out(perm.size());
+  for (size_t t = 0; t < perm.size(); ++t) out[t] = v[perm[t]];
+  return out;
+}
+
+static Part upload_part(Arena& a, const HostPart& hp) {
+  Part p;
+  p.blk_seg_begin = a.upload_same(hp.blk_seg_begin);
+  p.segs = a.upload_same(hp.segs);
+  p.blk_long_begin = a.upload_same(hp.blk_long_begin);
+  p.longs = a.upload_same(hp.longs);
+  p.blk_item_begin = a.upload_same(hp.blk_item_begin);
+  p.items = a.upload_same(hp.items);
+  p.seg_sum = a.zeros<double>(hp.segs.size() * 2);
+  return p;
+}
+
+static void launch_coop(const void* fn, int grid, void** args, cudaStream_t stream) {
+  SIH26_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kThreads), args, 0, stream),
+             SANKHYA_GPU_KERNEL_LAUNCH_FAILED);
+}
+
+__global__ void read_clock_kernel(unsigned long long* out) { *out = global_ns(); }
+
+// Everything one precision level of the solve needs on the device.
+template <class T>
+struct Level {
+  Prob<T> P;
+  State<T> S;
+};
+
+struct Common {
+  // device copies shared by both precisions
+  const int *a_ptr, *a_idx, *at_ptr, *at_idx;
+  const double *a_val64, *at_val64;
+  const double *dr, *dc, *c0, *cl0, *cu0, *rl0, *ru0;
+  Part pa, pat;
+  double *best_x, *best_y, *partials;
+  Ctrl* ctrl;
+  GridBarrier bar;
+};
+
+template <class T>
+static Level<T> make_level(Arena& a, const Common& cm, const PermutedLp& q, const Scaling& s,
+                           const std::vector<double>& x0) {
+  Level<T> L{};
+  const int m = q.m, n = q.n;
+  Prob<T>& P = L.P;
+  P.m = m;
+  P.n = n;
+  P.A.ptr = cm.a_ptr;
+  P.A.idx = cm.a_idx;
+  P.A.val64 = cm.a_val64;
+  P.AT.ptr = cm.at_ptr;
+  P.AT.idx = cm.at_idx;
+  P.AT.val64 = cm.at_val64;
+  if constexpr (std::is_same<T, double>::value) {
+    P.A.val = cm.a_val64;
+    P.AT.val = cm.at_val64;
+  } else {
+    P.A.val = a.upload<T>(q.a_val);
+    P.AT.val = a.upload<T>(q.at_val);
+  }
+  P.pa = cm.pa;
+  P.pat = cm.pat;
+  P.c = a.upload<T>(gather(s.cost, q.col_perm));
+  P.cl = a.upload<T>(gather(s.cl, q.col_perm));
+  P.cu = a.upload<T>(gather(s.cu, q.col_perm));
+  P.rl = a.upload<T>(gather(s.rl, q.row_perm));
+  P.ru = a.upload<T>(gather(s.ru, q.row_perm));
+  P.dr = cm.dr;
+  P.dc = cm.dc;
+  P.c0 = cm.c0;
+  P.cl0 = cm.cl0;
+  P.cu0 = cm.cu0;
+  P.rl0 = cm.rl0;
+  P.ru0 = cm.ru0;
+  State<T>& S = L.S;
+  for (int k = 0; k < 2; ++k) {
+    S.x[k] = a.zeros<T>(n);
+    S.y[k] = a.zeros<T>(m);
+    S.ax[k] = a.zeros<double>(m);
+  }
+  S.xsum = a.zeros<double>(n);
+  S.ysum = a.zeros<double>(m);
+  S.xr = a.zeros<T>(n);
+  S.yr = a.zeros<T>(m);
+  S.xavg = a.zeros<double>(n);
+  S.yavg = a.zeros<double>(m);
+  S.best_x = cm.best_x;
+  S.best_y = cm.best_y;
+  S.partials = cm.partials;
+  S.ctrl = cm.ctrl;
+  S.bar = cm.bar;
+  if (!x0.empty()) {
+    std::vector<T> xt(x0.begin(), x0.end());
+    SIH26_CUDA(cudaMemcpy(S.x[0], xt.data(), n * sizeof(T), cudaMemcpyHostToDevice),
+               SANKHYA_GPU_COPY_FAILED);
+    SIH26_CUDA(cudaMemcpy(S.xr, xt.data(), n * sizeof(T), cudaMemcpyHostToDevice),
+               SANKHYA_GPU_COPY_FAILED);
+  }
+  return L;
+}
+
+template <class T>
+static int blocks_per_sm() {
+  int a = 0, b = 0, c = 0, d = 0;
+  SIH26_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, iterate_kernel<T>, kThreads, 0),
+             SANKHYA_GPU_INIT_FAILED);
+  SIH26_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, evaluate_kernel<T>, kThreads, 0),
+             SANKHYA_GPU_INIT_FAILED);
+  SIH26_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, report_kernel<T>, kThreads, 0),
+             SANKHYA_GPU_INIT_FAILED);
+  SIH26_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d, power_kernel<T>, kThreads, 0),
+             SANKHYA_GPU_INIT_FAILED);
+  return std::min(std::min(a, b), std::min(c, d));
+}
+
+// Runs (iterate, evaluate) launch pairs until the device reports a final state.
+template <class T>
+static Ctrl run_loop(Level<T>& L, int G, cudaStream_t stream, Ctrl* host_ctrl, int verbose,
+                     const std::vector<double>* log_unused) {
+  (void)log_unused;
+  long long max_attempts = 1ll << 40;
+  int pairs = 4;
+  Ctrl c{};
+  for (;;) {
+    for (int k = 0; k < pairs; ++k) {
+      void* ia[] = {&L.P, &L.S, &max_attempts};
+      launch_coop(reinterpret_cast<const void*>(iterate_kernel<T>), G, ia, stream);
+      void* ea[] = {&L.P, &L.S};
+      launch_coop(reinterpret_cast<const void*>(evaluate_kernel<T>), G, ea, stream);
+    }
+    SIH26_CUDA(cudaMemcpyAsync(host_ctrl, L.S.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, stream),
+               SANKHYA_GPU_COPY_FAILED);
+    SIH26_CUDA(cudaStreamSynchronize(stream), SANKHYA_GPU_SYNC_FAILED);
+    c = *host_ctrl;
+    if (verbose) {
+      std::printf("%10lld %12.5e %10.3e %10.3e %10.3e %9.2e %9.2e\n", c.iteration,
+                  c.best.primal_objective, c.best.primal, c.best.dual, c.best.gap, c.eta,
+                  c.omega);
+      std::fflush(stdout);
+    }
+    if (c.state != kRunning && c.state != kNeedEval) break;
+    if (pairs < 64) pairs *= 2;
+  }
+  return c;
+}
+
+static void fill_message(sankhya_pdhg_result* r, const char* text) {
+  std::snprintf(r->message, sizeof r->message, "%s", text);
+}
+
+static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_params& prm,
+                      sankhya_pdhg_result* res) {
+  const Clock::time_point t_start = Clock::now();
+  check_structure(prob);
+  if (!(prm.tolerance > 0.0)) throw Failure{SANKHYA_GPU_INVALID_ARGUMENT, "tolerance must be > 0"};
+  if (prm.precision != SANKHYA_PDHG_FP64 && prm.precision != SANKHYA_PDHG_MIXED)
+    throw Failure{SANKHYA_GPU_INVALID_ARGUMENT, "unknown precision"};
+  const int m = prob.num_rows, n = prob.num_cols;
+  res->status = SANKHYA_PDHG_NOT_SOLVED;
+  res->converged = 0;
+  res->iterations = res->attempts = res->restarts = res->evaluations = res->fp32_iterations = 0;
+  res->message[0] = '\0';
+  const std::string why = validate_model(prob);
+  if (!why.empty()) {
+    res->status = SANKHYA_PDHG_MODEL_ERROR;
+    fill_message(res, why.c_str());
+    return SANKHYA_GPU_SUCCESS;
+  }
+
+  int devices = 0;
+  if (cudaGetDeviceCount(&devices) != cudaSuccess || devices == 0)
+    throw Failure{SANKHYA_GPU_NO_COMPATIBLE_DEVICE, "no CUDA device is visible"};
+  if (prm.device < 0 || prm.device >= devices)
+    throw Failure{SANKHYA_GPU_INVALID_ARGUMENT, "device ordinal out of range"};
+  SIH26_CUDA(cudaSetDevice(prm.device), SANKHYA_GPU_INIT_FAILED);
+  cudaDeviceProp props{};
+  SIH26_CUDA(cudaGetDeviceProperties(&props, prm.device), SANKHYA_GPU_INIT_FAILED);
+  if (props.major < 10)
+    throw Failure{SANKHYA_GPU_NO_COMPATIBLE_DEVICE, "this library is built for sm_100a (B200)"};
+  if (!props.cooperativeLaunch)
+    throw Failure{SANKHYA_GPU_NO_COMPATIBLE_DEVICE, "device lacks cooperative launch"};
+
+  // ---- the unscaled problem in minimise space (pdhg.cpp:284-301) ----
+  const double sense = prob.maximize ? -1.0 : 1.0;
+  std::vector<double> cmin(n);
+  for (int j = 0; j < n; ++j) cmin[j] = sense * prob.cost[j];
+  double cs2 = 0.0;
+  for (int j = 0; j < n; ++j) cs2 += cmin[j] * cmin[j];
+  const double cost_norm = std::sqrt(cs2);
+  double bs2 = 0.0;
+  for (int i = 0; i < m; ++i) {
+    const double b = host_finite_bound(prob.row_lower[i])
+                         ? prob.row_lower[i]
+                         : (host_finite_bound(prob.row_upper[i]) ? prob.row_upper[i] : 0.0);
+    bs2 += b * b;
+  }
+  const double bound_norm = std::sqrt(bs2);
+
+  // ---- preconditioning and layout ----
+  const Scaling sc = build_scaling(prob, cmin, 10);
+  const PermutedLp q = permute(prob, sc.values);
+
+  int bpsm = std::min(blocks_per_sm<double>(), prm.precision == SANKHYA_PDHG_MIXED ? blocks_per_sm<float>() : 1 << 20);
+  if (bpsm < 1) throw Failure{SANKHYA_GPU_INIT_FAILED, "kernel does not fit on an SM"};
+  int G = props.multiProcessorCount * std::min(bpsm, 2);
+  const long long work = q.nnz + m + n;
+  G = static_cast<int>(std::max<long long>(1, std::min<long long>(G, (work + 4095) / 4096)));
+
+  Arena a;
+  cudaStream_t stream;
+  SIH26_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), SANKHYA_GPU_INIT_FAILED);
+  struct StreamGuard {
+    cudaStream_t s;
+    ~StreamGuard() { cudaStreamDestroy(s); }
+  } guard{stream};
+
+  Common cm{};
+  cm.a_ptr = a.upload_same(q.a_ptr);
+  cm.a_idx = a.upload_same(q.a_idx);
+  cm.at_ptr = a.upload_same(q.at_ptr);
+  cm.at_idx = a.upload_same(q.at_idx);
+  cm.a_val64 = a.upload_same(q.a_val);
+  cm.at_val64 = a.upload_same(q.at_val);
+  cm.dr = a.upload_same(gather(sc.dr, q.row_perm));
+  cm.dc = a.upload_same(gather(sc.dc, q.col_perm));
+  cm.c0 = a.upload_same(gather(cmin, q.col_perm));
+  cm.cl0 = a.upload_same(gather_ptr(prob.col_lower, q.col_perm));
+  cm.cu0 = a.upload_same(gather_ptr(prob.col_upper, q.col_perm));
+  cm.rl0 = a.upload_same(gather_ptr(prob.row_lower, q.row_perm));
+  cm.ru0 = a.upload_same(gather_ptr(prob.row_upper, q.row_perm));
+  cm.pa = upload_part(a, partition(q.a_ptr, G, kWarps, prm.group_size_rows));
+  cm.pat = upload_part(a, partition(q.at_ptr, G, kWarps, prm.group_size_cols));
+  cm.best_x = a.zeros<double>(n);
+  cm.best_y = a.zeros<double>(m);
+  cm.partials = a.zeros<double>(2ull * G * kPartSlots);
+  cm.ctrl = a.zeros<Ctrl>(1);
+  unsigned* bar_words = a.zeros<unsigned>(2);
+  int* flags = a.zeros<int>(2);
+  cm.bar = GridBarrier{bar_words, bar_words + 1, flags, 4000000000ull, flags + 1, 0ull};
+
+  // starting point: the projection of zero (pdhg.cpp:329-334), in permuted order
+  std::vector<double> x0(n);
+  for (int t = 0; t < n; ++t) {
+    const int j = q.col_perm[t];
+    double v = 0.0;
+    if (host_finite_bound(sc.cl[j]) && v < sc.cl[j]) v = sc.cl[j];
+    else if (host_finite_bound(sc.cu[j]) && v > sc.cu[j]) v = sc.cu[j];
+    x0[t] = v;
+  }
+  SIH26_CUDA(cudaMemcpy(cm.best_x, x0.data(), n * sizeof(double), cudaMemcpyHostToDevice),
+             SANKHYA_GPU_COPY_FAILED);
+
+  Level<double> L64 = make_level<double>(a, cm, q, sc, prm.precision == SANKHYA_PDHG_FP64 ? x0 : std::vector<double>());
+  Level<float> L32{};
+  const bool mixed = prm.precision == SANKHYA_PDHG_MIXED;
+  if (mixed) L32 = make_level<float>(a, cm, q, sc, x0);
+
+  // ||A||_2 by power iteration (scaling.cpp:161-194), seed random_seed + 1
+  double spectral_norm = 1.0;
+  if (m > 0 && n > 0 && q.nnz > 0) {
+    std::vector<double> v0(n);
+    uniform_draws(static_cast<uint32_t>(prm.random_seed) + 1u, -1.0, 1.0, n, v0.data());
+    PowerState W{a.upload_same(gather(v0, q.col_perm)), a.zeros<double>(m), cm.partials, cm.bar};
+    double* d_norm = a.zeros<double>(1);
+    int iters = 30;
+    void* pa[] = {&L64.P, &W, &iters, &d_norm};
+    launch_coop(reinterpret_cast<const void*>(power_kernel<double>), G, pa, stream);
+    SIH26_CUDA(cudaMemcpyAsync(&spectral_norm, d_norm, sizeof(double), cudaMemcpyDeviceToHost, stream),
+               SANKHYA_GPU_COPY_FAILED);
+  }
+  // A x0 for the starting point
+  {
+    const int blocks = std::max(1, std::min(4096, (m * 32 + 255) / 256));
+    if (mixed) {
+      spmv_rows_kernel<float><<<blocks, 256, 0, stream>>>(m, cm.a_ptr, cm.a_idx, cm.a_val64, L32.S.x[0], L32.S.ax[0]);
+    } else {
+      spmv_rows_kernel<double><<<blocks, 256, 0, stream>>>(m, cm.a_ptr, cm.a_idx, cm.a_val64, L64.S.x[0], L64.S.ax[0]);
+    }
+    SIH26_CUDA(cudaGetLastError(), SANKHYA_GPU_KERNEL_LAUNCH_FAILED);
+  }
+  int err_flag = 0;
+  SIH26_CUDA(cudaStreamSynchronize(stream), SANKHYA_GPU_SYNC_FAILED);
+  SIH26_CUDA(cudaMemcpy(&err_flag, flags, sizeof(int), cudaMemcpyDeviceToHost), SANKHYA_GPU_COPY_FAILED);
+  if (err_flag) throw Failure{SANKHYA_GPU_DEVICE_TIMEOUT, "grid barrier timed out in the norm estimate"};
+
+  const long long iteration_limit = prm.iteration_limit < 0 ? 1000000ll : prm.iteration_limit;
+  Ctrl c0{};
+  c0.eta = spectral_norm > 0.0 ? 1.0 / spectral_norm : 1.0;
+  c0.omega = 1.0;
+  c0.restart_kkt = INFINITY;
+  c0.best_worst = INFINITY;
+  c0.best.primal = c0.best.dual = c0.best.gap = INFINITY;
+  c0.state = kRunning;
+  c0.spectral_norm = spectral_norm;
+  c0.eta_ceiling = 1.0e3 / std::max(spectral_norm, 1e-12);
+  c0.tolerance = prm.tolerance;
+  c0.bound_norm = bound_norm;
+  c0.cost_norm = cost_norm;
+  c0.iteration_limit = iteration_limit;
+  c0.use_restarts = prm.restart ? 1 : 0;
+  c0.stop_at_request = prm.stop_at_request ? 1 : 0;
+  c0.stop_rule = prm.stop_rule;
+
+  // the time limit counts from the start of the call, like the reference's Timer
+  const double setup_seconds = seconds_since(t_start);
+  if (std::isfinite(prm.time_limit) && prm.time_limit > 0.0) {
+    unsigned long long* d_now = a.zeros<unsigned long long>(1);
+    read_clock_kernel<<<1, 1, 0, stream>>>(d_now);
+    unsigned long long now = 0;
+    SIH26_CUDA(cudaMemcpy(&now, d_now, sizeof now, cudaMemcpyDeviceToHost), SANKHYA_GPU_COPY_FAILED);
+    const double left = prm.time_limit - seconds_since(t_start);
+    cm.bar.deadline_ns = now + static_cast<unsigned long long>(std::max(0.0, left) * 1e9);
+    L64.S.bar = cm.bar;
+    L32.S.bar = cm.bar;
+    if (left <= 0.0) {
+      int one = 1;
+      SIH26_CUDA(cudaMemcpy(flags + 1, &one, sizeof one, cudaMemcpyHostToDevice), SANKHYA_GPU_COPY_FAILED);
+      c0.time_up = 1;
+    }
+  }
+
+  Ctrl* host_ctrl = nullptr;
+  SIH26_CUDA(cudaMallocHost(&host_ctrl, sizeof(Ctrl)), SANKHYA_GPU_OUT_OF_MEMORY);
+  struct HostFree {
+    void* p;
+    ~HostFree() { cudaFreeHost(p); }
+  } hf{host_ctrl};
+
+  cudaEvent_t ev0, ev1;
+  SIH26_CUDA(cudaEventCreate(&ev0), SANKHYA_GPU_INIT_FAILED);
+  SIH26_CUDA(cudaEventCreate(&ev1), SANKHYA_GPU_INIT_FAILED);
+  struct EvFree {
+    cudaEvent_t a, b;
+    ~EvFree() { cudaEventDestroy(a); cudaEventDestroy(b); }
+  } ef{ev0, ev1};
+
+  if (prm.verbose) {
+    std::printf("GPU PDHG: %d rows, %d columns, %lld nonzeros, %d blocks x %d threads, ||A||_2 ~ %.4e\n",
+                m, n, q.nnz, G, kThreads, spectral_norm);
+    std::printf("%10s %12s %10s %10s %10s %9s %9s\n", "iteration", "objective", "primal", "dual",
+                "gap", "eta", "omega");
+  }
+  SIH26_CUDA(cudaEventRecord(ev0, stream), SANKHYA_GPU_INIT_FAILED);
+  Ctrl fin{};
+  long long fp32_iterations = 0;
+  if (!mixed) {
+    SIH26_CUDA(cudaMemcpyAsync(cm.ctrl, &c0, sizeof(Ctrl), cudaMemcpyHostToDevice, stream),
+               SANKHYA_GPU_COPY_FAILED);
+    fin = run_loop(L64, G, stream, host_ctrl, prm.verbose, nullptr);
+  } else {
+    throw Failure{SANKHYA_GPU_INVALID_ARGUMENT, "mixed precision is not built yet"};
+  }
+  SIH26_CUDA(cudaEventRecord(ev1, stream), SANKHYA_GPU_INIT_FAILED);
+  if (fin.state == kDeviceError)
+    throw Failure{SANKHYA_GPU_DEVICE_TIMEOUT, "a grid barrier timed out during the iteration loop"};
+
+  // ---- report (pdhg.cpp:647-716) ----
+  double* d_x = a.zeros<double>(n);
+  double* d_red = a.zeros<double>(n);
+  double* d_y = a.zeros<double>(m);
+  {
+    void* ra[] = {&L64.P, &L64.S, &d_x, &d_red, &d_y};
+    launch_coop(reinterpret_cast<const void*>(report_kernel<double>), G, ra, stream);
+  }
+  SIH26_CUDA(cudaMemcpyAsync(host_ctrl, cm.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, stream),
+             SANKHYA_GPU_COPY_FAILED);
+  std::vector<double> hx(n), hred(n), hy(m);
+  if (n) SIH26_CUDA(cudaMemcpyAsync(hx.data(), d_x, n * 8, cudaMemcpyDeviceToHost, stream), SANKHYA_GPU_COPY_FAILED);
+  if (n) SIH26_CUDA(cudaMemcpyAsync(hred.data(), d_red, n * 8, cudaMemcpyDeviceToHost, stream), SANKHYA_GPU_COPY_FAILED);
+  if (m) SIH26_CUDA(cudaMemcpyAsync(hy.data(), d_y, m * 8, cudaMemcpyDeviceToHost, stream), SANKHYA_GPU_COPY_FAILED);
+  SIH26_CUDA(cudaStreamSynchronize(stream), SANKHYA_GPU_SYNC_FAILED);
+  const Ctrl rep = *host_ctrl;
+  if (rep.state == kDeviceError)
+    throw Failure{SANKHYA_GPU_DEVICE_TIMEOUT, "a grid barrier timed out in the report"};
+  float ms = 0.f;
+  SIH26_CUDA(cudaEventElapsedTime(&ms, ev0, ev1), SANKHYA_GPU_SYNC_FAILED);
+
+  // un-permute
+  std::vector<double> col_value(n), reduced(n), y(m);
+  for (int t = 0; t < n; ++t) {
+    col_value[q.col_perm[t]] = hx[t];
+    reduced[q.col_perm[t]] = hred[t];
+  }
+  for (int t = 0; t < m; ++t) y[q.row_perm[t]] = hy[t];
+  for (double v : col_value)
+    if (!std::isfinite(v)) throw Failure{SANKHYA_GPU_NON_FINITE_OUTPUT, "the reported point is not finite"};
+  if (res->col_value) std::memcpy(res->col_value, col_value.data(), n * sizeof(double));
+  if (res->col_dual) for (int j = 0; j < n; ++j) res->col_dual[j] = sense * reduced[j];
+  if (res->row_dual) for (int i = 0; i < m; ++i) res->row_dual[i] = sense * (-y[i]);
+
+  const Residuals& f = rep.best;
+  res->residuals = sankhya_pdhg_residuals{f.primal, f.dual, f.gap, f.primal_objective,
+                                          f.dual_objective, f.absolute_primal, f.absolute_dual,
+                                          f.gap_as_verified, f.complementarity};
+  res->iterations = fin.iteration;
+  res->attempts = fin.attempts;
+  res->restarts = fin.restarts;
+  res->evaluations = fin.evaluations;
+  res->fp32_iterations = fp32_iterations;
+  res->spectral_norm = spectral_norm;
+  res->converged = fin.converged;
+  double obj = prob.objective_offset;  // Model::evaluate_objective (src/core/model.cpp:99-105)
+  for (int j = 0; j < n; ++j) obj += prob.cost[j] * col_value[j];
+  res->objective = obj;
+
+  const bool project_standard = f.absolute_primal <= 1e-7 && f.absolute_dual <= 1e-7 &&
+                                f.gap_as_verified <= 1e-9 && f.complementarity <= 1e-6;
+  const bool verifiable = fin.converged && project_standard;
+  char msg[512];
+  if (verifiable) {
+    res->status = SANKHYA_PDHG_OPTIMAL;
+    std::snprintf(msg, sizeof msg,
+                  "converged after %lld iterations and %lld restarts; absolute primal %.3e, dual "
+                  "%.3e, relative gap %.3e",
+                  fin.iteration, fin.restarts, f.absolute_primal, f.absolute_dual, f.gap_as_verified);
+  } else if (fin.converged) {
+    res->status = SANKHYA_PDHG_FEASIBLE;
+    std::snprintf(msg, sizeof msg,
+                  "met the requested relative tolerance %.1e after %lld iterations, but NOT the "
+                  "absolute standard this project verifies against (primal %.3e vs 1.0e-07, dual "
+                  "%.3e vs 1.0e-07, relative gap %.3e vs 1.0e-09). Reported as feasible, not "
+                  "optimal. %s",
+                  prm.tolerance, fin.iteration, f.absolute_primal, f.absolute_dual,
+                  f.gap_as_verified,
+                  prm.stop_at_request ? "pdhg_stop_at_request is on, so this is the cheap answer "
+                                        "that was asked for; turn it off to run on to the standard"
+                                      : "Tighten --option pdhg_tolerance to close it");
+  } else {
+    res->status = fin.state == kTimeLimit ? SANKHYA_PDHG_TIME_LIMIT : SANKHYA_PDHG_ITERATION_LIMIT;
+    std::snprintf(msg, sizeof msg,
+                  "stopped at relative primal %.3e, dual %.3e, gap %.3e after %lld iterations and "
+                  "%lld restarts (target %.1e)",
+                  f.primal, f.dual, f.gap, fin.iteration, fin.restarts, prm.tolerance);
+  }
+  fill_message(res, msg);
+  res->dual_bound = verifiable ? sense * f.dual_objective + prob.objective_offset
+                               : (prob.maximize ? INFINITY : -INFINITY);
+  res->setup_seconds = setup_seconds;
+  res->solve_seconds = ms * 1e-3;
+  res->total_seconds = seconds_since(t_start);
+  return SANKHYA_GPU_SUCCESS;
+}
+
+}  // namespace sih26
+
+extern "C" {
+
+void sankhya_pdhg_gpu_default_params(sankhya_pdhg_params* p) {
+  std::memset(p, 0, sizeof *p);
+  p->tolerance = 1e-4;
+  p->iteration_limit = -1;
+  p->time_limit = INFINITY;
+  p->restart = 1;
+  p->stop_at_request = 0;
+  p->random_seed = 0;
+  p->precision = SANKHYA_PDHG_FP64;
+  p->stop_rule = SANKHYA_PDHG_STOP_REFERENCE;
+  p->device = 0;
+  p->verbose = 0;
+  p->detect_infeasibility = 1;
+  p->mixed_switch_tolerance = 1e-5;
+}
+
+int sankhya_pdhg_gpu_solve(const sankhya_pdhg_problem* problem, const sankhya_pdhg_params* params,
+                           sankhya_pdhg_result* result) {
+  using namespace sih26;
+  if (!problem || !result) {
+    g_last_error = "problem and result must not be NULL";
+    return SANKHYA_GPU_INVALID_ARGUMENT;
+  }
+  sankhya_pdhg_params defaults;
+  sankhya_pdhg_gpu_default_params(&defaults);
+  try {
+    return solve_impl(*problem, params ? *params : defaults, result);
+  } catch (const Failure& f) {
+    g_last_error = f.message;
+    std::snprintf(result->message, sizeof result->message, "%s", f.message.c_str());
+    result->status = SANKHYA_PDHG_NUMERICAL_ERROR;
+    return f.code;
+  } catch (const std::bad_alloc&) {
+    g_last_error = "host allocation failed";
+    return SANKHYA_GPU_OUT_OF_MEMORY;
+  } catch (const std::exception& e) {
+    g_last_error = e.what();
+    return SANKHYA_GPU_INVALID_DEVICE_STATE;
+  }
+}
+
+const char* sankhya_pdhg_gpu_last_error(void) { return sih26::g_last_error.c_str(); }
+
+int sankhya_pdhg_gpu_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+  return n;
+}
+
+int sankhya_pdhg_gpu_device_name(int device, char* name, int capacity) {
+  cudaDeviceProp p{};
+  if (cudaGetDeviceProperties(&p, device) != cudaSuccess) {
+    sih26::g_last_error = "no such device";
+    return SANKHYA_GPU_NO_COMPATIBLE_DEVICE;
+  }
+  if (name && capacity > 0) std::snprintf(name, capacity, "%s", p.name);
+  return SANKHYA_GPU_SUCCESS;
+}
+
+}  // extern "C"

@@ -1,0 +1,282 @@
+"""Python face of the GPU PDHG engine, shaped like the reference's own interface.
+
+The reference exposes the path as ``Solution sankhya::pdhg::solve_pdhg(const Model&, const
+Options&, Logger&)`` (include/sankhya/pdhg.hpp:15) reading the option rows ``pdhg_tolerance``,
+``iteration_limit``, ``time_limit``, ``pdhg_restart``, ``pdhg_stop_at_request`` and
+``random_seed`` (src/pdhg/pdhg.cpp:305-315, src/util/options.cpp:83-418). ``solve_pdhg`` here
+takes the same options by the same names and returns a ``Solution`` with the reference's
+fields and sign conventions, computed by the CUDA library through its C ABI
+(include/sankhya_pdhg_gpu.h). There is no CPU fallback: without the library or a GPU the call
+raises ``GpuError``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+import math
+import os
+from typing import Optional
+
+import numpy as np
+
+from .lpgen import LP
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "_lib", "libsankhya_pdhg_gpu.so")
+
+# sankhya_pdhg_gpu_status (mirrors sankhya::gpu::GpuStatus, include/sankhya/gpu_runtime.hpp:19-30)
+GPU_STATUS = {0: "success", 1: "cuda unavailable", 2: "no compatible cuda device",
+              3: "initialization failed", 4: "out of device memory", 5: "kernel launch failed",
+              6: "memory copy failed", 7: "device synchronization failed",
+              8: "invalid device state", 9: "non-finite numerical output detected",
+              10: "invalid argument", 11: "device wait timed out"}
+
+# sankhya_solve_status values (include/sankhya/sankhya.h:53-66) -> SolveStatus names
+# (src/core/model.cpp:19-34)
+SOLVE_STATUS = {0: "not_solved", 1: "optimal", 2: "feasible", 3: "infeasible", 4: "unbounded",
+                5: "iteration_limit", 6: "time_limit", 7: "node_limit", 8: "numerical_error",
+                9: "model_error", 10: "infeasible_or_unbounded"}
+
+PRECISIONS = {"fp64": 0, "mixed": 1}
+STOP_RULES = {"reference": 0, "relative_kkt": 1}
+
+
+class GpuError(RuntimeError):
+    """The GPU path could not run; carries the library's status code."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{GPU_STATUS.get(code, code)}: {message}")
+        self.code = code
+
+
+_i32p = C.POINTER(C.c_int32)
+_f64p = C.POINTER(C.c_double)
+
+
+class _Problem(C.Structure):
+    _fields_ = [("num_rows", C.c_int32), ("num_cols", C.c_int32), ("num_nonzeros", C.c_int32),
+                ("col_starts", _i32p), ("row_indices", _i32p), ("values", _f64p),
+                ("cost", _f64p), ("col_lower", _f64p), ("col_upper", _f64p),
+                ("row_lower", _f64p), ("row_upper", _f64p), ("maximize", C.c_int32),
+                ("objective_offset", C.c_double)]
+
+
+class _Params(C.Structure):
+    _fields_ = [("tolerance", C.c_double), ("iteration_limit", C.c_int64),
+                ("time_limit", C.c_double), ("restart", C.c_int32),
+                ("stop_at_request", C.c_int32), ("random_seed", C.c_int64),
+                ("precision", C.c_int32), ("stop_rule", C.c_int32), ("device", C.c_int32),
+                ("verbose", C.c_int32), ("detect_infeasibility", C.c_int32),
+                ("mixed_switch_tolerance", C.c_double), ("group_size_rows", C.c_int32),
+                ("group_size_cols", C.c_int32), ("reserved", C.c_int32 * 8)]
+
+
+class _Residuals(C.Structure):
+    _fields_ = [(k, C.c_double) for k in (
+        "relative_primal", "relative_dual", "relative_gap", "primal_objective",
+        "dual_objective", "absolute_primal", "absolute_dual", "gap_as_verified",
+        "complementarity")]
+
+
+class _Result(C.Structure):
+    _fields_ = [("col_value", _f64p), ("row_dual", _f64p), ("col_dual", _f64p),
+                ("farkas_dual", _f64p), ("primal_ray", _f64p), ("status", C.c_int32),
+                ("converged", C.c_int32), ("iterations", C.c_int64), ("attempts", C.c_int64),
+                ("restarts", C.c_int64), ("evaluations", C.c_int64),
+                ("fp32_iterations", C.c_int64), ("objective", C.c_double),
+                ("dual_bound", C.c_double), ("spectral_norm", C.c_double),
+                ("setup_seconds", C.c_double), ("solve_seconds", C.c_double),
+                ("total_seconds", C.c_double), ("residuals", _Residuals),
+                ("message", C.c_char * 512)]
+
+
+# Every symbol include/sankhya_pdhg_gpu.h declares.
+EXPORTED_SYMBOLS = ("sankhya_pdhg_gpu_default_params", "sankhya_pdhg_gpu_solve",
+                    "sankhya_pdhg_gpu_last_error", "sankhya_pdhg_gpu_device_count",
+                    "sankhya_pdhg_gpu_device_name")
+
+_lib: Optional[C.CDLL] = None
+
+
+def load_library() -> C.CDLL:
+    """Loads the in-tree CUDA library; raises GpuError when it is missing."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIBPATH):
+            raise GpuError(1, f"{LIBPATH} is not built (python -m sih26_b200.build)")
+        lib = C.CDLL(LIBPATH)
+        lib.sankhya_pdhg_gpu_default_params.argtypes = [C.POINTER(_Params)]
+        lib.sankhya_pdhg_gpu_solve.argtypes = [C.POINTER(_Problem), C.POINTER(_Params),
+                                               C.POINTER(_Result)]
+        lib.sankhya_pdhg_gpu_last_error.restype = C.c_char_p
+        lib.sankhya_pdhg_gpu_device_name.argtypes = [C.c_int, C.c_char_p, C.c_int]
+        _lib = lib
+    return _lib
+
+
+def device_count() -> int:
+    return load_library().sankhya_pdhg_gpu_device_count()
+
+
+class Options:
+    """The option rows the PDHG path reads, with the reference's names and defaults
+    (src/util/options.cpp:83-418), plus the GPU rows this engine adds."""
+
+    _SPECS = {
+        # name: (type, default)
+        "pdhg_tolerance": (float, 1e-4),
+        "iteration_limit": (int, -1),
+        "time_limit": (float, math.inf),
+        "pdhg_restart": (bool, True),
+        "pdhg_stop_at_request": (bool, False),
+        "random_seed": (int, 0),
+        "log_to_console": (bool, False),
+        "pdhg_precision": (str, "fp64"),
+        "pdhg_stop_rule": (str, "reference"),
+        "pdhg_mixed_switch_tolerance": (float, 1e-5),
+        "pdhg_detect_infeasibility": (bool, True),
+        "gpu_device": (int, 0),
+        "pdhg_lanes_rows": (int, 0),
+        "pdhg_lanes_cols": (int, 0),
+    }
+
+    def __init__(self, **values):
+        self._v = {k: d for k, (_, d) in self._SPECS.items()}
+        for k, v in values.items():
+            self.set(k, v)
+
+    def set(self, name, value):
+        if name not in self._SPECS:
+            raise KeyError(f"no such option: {name}")
+        typ = self._SPECS[name][0]
+        if typ is bool and isinstance(value, str):
+            value = value.lower() in ("1", "true", "on", "yes")
+        if typ is str:
+            allowed = {"pdhg_precision": PRECISIONS, "pdhg_stop_rule": STOP_RULES}.get(name)
+            if allowed is not None and value not in allowed:
+                raise ValueError(f"{name} must be one of {sorted(allowed)}")
+        self._v[name] = typ(value)
+
+    def set_from_string(self, text: str):
+        """`name=value`, the CLI's --option form (src/util/options.cpp:481)."""
+        name, _, value = text.partition("=")
+        self.set(name.strip(), value.strip())
+
+    def get(self, name):
+        return self._v[name]
+
+    get_double = get_int = get_bool = get_string = get
+    set_double = set_int = set_bool = set_string = set
+
+
+@dataclasses.dataclass
+class Solution:
+    """The reference's Solution fields this path fills (include/sankhya/model.hpp:233-374)."""
+
+    status: str
+    objective: float
+    dual_bound: float
+    col_value: np.ndarray
+    row_dual: np.ndarray
+    col_dual: np.ndarray
+    iterations: int
+    solve_seconds: float
+    algorithm: str
+    message: str
+    primal_infeasibility: float = 0.0
+    farkas_dual: Optional[np.ndarray] = None
+    primal_ray: Optional[np.ndarray] = None
+    # engine detail
+    attempts: int = 0
+    restarts: int = 0
+    evaluations: int = 0
+    fp32_iterations: int = 0
+    spectral_norm: float = 0.0
+    residuals: Optional[dict] = None
+    setup_seconds: float = 0.0
+    device_seconds: float = 0.0
+
+    def has_primal_values(self) -> bool:
+        return self.status in ("optimal", "feasible")
+
+
+def _arr(a, dtype):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+def _primal_infeasibility(lp: LP, x: np.ndarray) -> float:
+    """Max row/column bound violation (Solution::recompute_quality, src/core/model.cpp:228-283)."""
+    act = lp.to_scipy_csc() @ x if lp.num_rows else np.zeros(0)
+    fin = lambda v: np.abs(v) < 1e30  # noqa: E731
+    viol = [0.0]
+    for lo, val in ((lp.col_lower, x), (lp.row_lower, act)):
+        m = fin(lo)
+        if m.any():
+            viol.append(float(np.max(lo[m] - val[m])))
+    for hi, val in ((lp.col_upper, x), (lp.row_upper, act)):
+        m = fin(hi)
+        if m.any():
+            viol.append(float(np.max(val[m] - hi[m])))
+    return max(0.0, max(viol))
+
+
+def solve_pdhg(model: LP, options: Optional[Options] = None) -> Solution:
+    """GPU successor of sankhya::pdhg::solve_pdhg (src/pdhg/pdhg.cpp:267-726)."""
+    opt = options or Options()
+    lib = load_library()
+    cs = _arr(model.col_starts, np.int32)
+    ri = _arr(model.row_indices, np.int32)
+    vals = _arr(model.values, np.float64)
+    vecs = [_arr(v, np.float64) for v in (model.cost, model.col_lower, model.col_upper,
+                                           model.row_lower, model.row_upper)]
+    prob = _Problem(model.num_rows, model.num_cols, int(cs[-1]) if cs.size else 0,
+                    cs.ctypes.data_as(_i32p), ri.ctypes.data_as(_i32p),
+                    vals.ctypes.data_as(_f64p), *[v.ctypes.data_as(_f64p) for v in vecs],
+                    1 if model.maximize else 0, float(model.objective_offset))
+    prm = _Params()
+    lib.sankhya_pdhg_gpu_default_params(C.byref(prm))
+    prm.tolerance = opt.get("pdhg_tolerance")
+    prm.iteration_limit = opt.get("iteration_limit")
+    prm.time_limit = opt.get("time_limit")
+    prm.restart = int(opt.get("pdhg_restart"))
+    prm.stop_at_request = int(opt.get("pdhg_stop_at_request"))
+    prm.random_seed = opt.get("random_seed")
+    prm.precision = PRECISIONS[opt.get("pdhg_precision")]
+    prm.stop_rule = STOP_RULES[opt.get("pdhg_stop_rule")]
+    prm.device = opt.get("gpu_device")
+    prm.verbose = int(opt.get("log_to_console"))
+    prm.detect_infeasibility = int(opt.get("pdhg_detect_infeasibility"))
+    prm.mixed_switch_tolerance = opt.get("pdhg_mixed_switch_tolerance")
+    prm.group_size_rows = opt.get("pdhg_lanes_rows")
+    prm.group_size_cols = opt.get("pdhg_lanes_cols")
+    n, m = model.num_cols, model.num_rows
+    x = np.zeros(n)
+    rd = np.zeros(m)
+    cd = np.zeros(n)
+    fk = np.zeros(m)
+    ray = np.zeros(n)
+    res = _Result()
+    res.col_value = x.ctypes.data_as(_f64p)
+    res.row_dual = rd.ctypes.data_as(_f64p)
+    res.col_dual = cd.ctypes.data_as(_f64p)
+    res.farkas_dual = fk.ctypes.data_as(_f64p)
+    res.primal_ray = ray.ctypes.data_as(_f64p)
+    code = lib.sankhya_pdhg_gpu_solve(C.byref(prob), C.byref(prm), C.byref(res))
+    if code != 0:
+        raise GpuError(code, lib.sankhya_pdhg_gpu_last_error().decode())
+    status = SOLVE_STATUS[res.status]
+    r = res.residuals
+    sol = Solution(
+        status=status, objective=res.objective, dual_bound=res.dual_bound, col_value=x,
+        row_dual=rd, col_dual=cd, iterations=res.iterations,
+        solve_seconds=res.total_seconds, algorithm="pdhg-gpu",
+        message=res.message.decode(errors="replace"),
+        farkas_dual=fk if status == "infeasible" else None,
+        primal_ray=ray if status == "unbounded" else None,
+        attempts=res.attempts, restarts=res.restarts, evaluations=res.evaluations,
+        fp32_iterations=res.fp32_iterations, spectral_norm=res.spectral_norm,
+        residuals={k: getattr(r, k) for k, _ in _Residuals._fields_},
+        setup_seconds=res.setup_seconds, device_seconds=res.solve_seconds)
+    if status != "model_error":
+        sol.primal_infeasibility = _primal_infeasibility(model, x)
+    return sol

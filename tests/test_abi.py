@@ -1,0 +1,107 @@
+"""The C-ABI library: it loads, exports every symbol include/*.h declares, mirrors the
+reference's option names and defaults, and rejects bad input before touching a GPU."""
+import ctypes as C
+import math
+import os
+import re
+
+import numpy as np
+import pytest
+
+from sih26_b200 import build, lpgen
+from sih26_b200 import pdhg as P
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    build.build_library()
+    return P.load_library()
+
+
+def _declared_functions():
+    names = []
+    inc = os.path.join(ROOT, "include")
+    for f in sorted(os.listdir(inc)):
+        if f.endswith(".h"):
+            text = open(os.path.join(inc, f)).read()
+            names += re.findall(r"^\s*(?:const\s+)?[a-z_0-9]+\**\s+\**(sankhya_[a-z_0-9]+)\s*\(",
+                                text, flags=re.M)
+    return names
+
+
+def test_library_exports_every_declared_symbol(lib):
+    declared = _declared_functions()
+    assert set(P.EXPORTED_SYMBOLS) <= set(declared)
+    for name in declared:
+        assert hasattr(lib, name), name
+
+
+def test_default_params_mirror_reference_option_defaults(lib):
+    prm = P._Params()
+    lib.sankhya_pdhg_gpu_default_params(C.byref(prm))
+    # src/util/options.cpp: pdhg_tolerance = kPdhgLoose 1e-4, iteration_limit -1, time_limit
+    # no limit, pdhg_restart true, pdhg_stop_at_request false, random_seed 0
+    assert prm.tolerance == 1e-4
+    assert prm.iteration_limit == -1
+    assert math.isinf(prm.time_limit)
+    assert prm.restart == 1 and prm.stop_at_request == 0 and prm.random_seed == 0
+    opts = P.Options()
+    assert opts.get("pdhg_tolerance") == prm.tolerance
+    assert opts.get("iteration_limit") == prm.iteration_limit
+
+
+def test_options_parse_like_the_cli():
+    opts = P.Options()
+    opts.set_from_string("pdhg_tolerance=1e-6")
+    opts.set_from_string("pdhg_stop_at_request=true")
+    opts.set_from_string("pdhg_precision=mixed")
+    assert opts.get("pdhg_tolerance") == 1e-6
+    assert opts.get("pdhg_stop_at_request") is True
+    with pytest.raises(KeyError):
+        opts.set("no_such_option", 1)
+    with pytest.raises(ValueError):
+        opts.set("pdhg_precision", "fp16")
+
+
+def _tiny():
+    return lpgen.from_dense([[1, 1]], [2], [math.inf], [1, 1])
+
+
+def test_malformed_matrix_is_an_argument_error(lib):
+    lp = _tiny()
+    lp.row_indices = np.array([0, 5], dtype=np.int32)  # row 5 of a 1-row matrix
+    with pytest.raises(P.GpuError) as e:
+        P.solve_pdhg(lp)
+    assert e.value.code == 10 and "out of range" in str(e.value)
+
+
+def test_unsorted_column_is_an_argument_error(lib):
+    lp = lpgen.from_dense([[1, 0], [1, 1]], [1, 1], [1, 1], [1, 1])
+    lp.row_indices = lp.row_indices[[1, 0, 2]].copy()
+    with pytest.raises(P.GpuError) as e:
+        P.solve_pdhg(lp)
+    assert e.value.code == 10
+
+
+def test_model_errors_come_back_as_a_status(lib):
+    # Model::validate (src/core/model.cpp:188-206) wording; pdhg.cpp:273-278 returns it
+    lp = _tiny()
+    lp.col_lower = np.array([3.0, 0.0])
+    lp.col_upper = np.array([1.0, math.inf])
+    s = P.solve_pdhg(lp)
+    assert s.status == "model_error"
+    assert "column 0 has lower bound 3 above upper bound 1" in s.message
+    lp = _tiny()
+    lp.values = np.array([math.nan, 1.0])
+    s = P.solve_pdhg(lp)
+    assert s.status == "model_error" and "not a usable coefficient" in s.message
+
+
+def test_no_cpu_fallback_without_a_gpu(lib):
+    if P.device_count() > 0:
+        pytest.skip("a GPU is present")
+    with pytest.raises(P.GpuError) as e:
+        P.solve_pdhg(_tiny())
+    assert e.value.code == 2
