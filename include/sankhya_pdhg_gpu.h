@@ -115,11 +115,13 @@ typedef struct sankhya_pdhg_params {
   int32_t verbose;          /* 1 prints the iteration table at each evaluation */
   int32_t detect_infeasibility; /* 1 (default): certify primal infeasibility / dual
                                    unboundedness from iterate differences */
-  double mixed_switch_tolerance; /* MIXED: relative KKT at which the FP32 phase hands over
-                                    to FP64 when the stop rule needs more; default 1e-5 */
+  double mixed_switch_tolerance; /* MIXED: relative KKT at which the FP32 phase hands over to
+                                    the FP64 polish; 0 (default) = run FP32 to the request and
+                                    hand over only if the FP32 iterate stalls */
   int32_t group_size_rows;  /* lanes per row for A x (0 = autotune) */
   int32_t group_size_cols;  /* lanes per row for A'y (0 = autotune) */
-  int32_t reserved[8];
+  int32_t grid_blocks;      /* blocks of the cooperative launches (0 = sized to the problem) */
+  int32_t reserved[7];
 } sankhya_pdhg_params;
 
 /* Unscaled residual block of the reported point (src/pdhg/pdhg.cpp:81-110). */

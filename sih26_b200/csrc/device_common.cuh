@@ -68,11 +68,14 @@ __device__ __forceinline__ void block_reduce(double (&v)[NS], double* shared) {
 }
 
 // Grid-wide barrier for a cooperative launch (all blocks co-resident). Thread 0 of each
-// block arrives on a counter; the last arriver resets it and bumps the generation. Waiters
-// spin on the generation with a deadline: after `limit_ns` they record an error and return
-// false instead of waiting on, so a broken launch ends instead of hanging the GPU. The
-// fences make every write before the barrier visible to every read after it (the same
-// bar.sync / fence / atomic pattern as cooperative groups' grid sync).
+// block arrives on a counter with an acq_rel atomic; the last arriver resets the counter and
+// publishes a new generation with a release store; the others poll the generation with
+// acquire loads. bar.sync on either side extends the ordering to every thread of the block,
+// so every write before the barrier is visible to every read after it.
+//
+// Waiters give up after `limit_ns` (or as soon as another block has given up): they record an
+// error and return false instead of waiting on, so a broken launch ends instead of hanging
+// the GPU.
 struct GridBarrier {
   unsigned* count;
   unsigned* generation;
@@ -82,26 +85,41 @@ struct GridBarrier {
   unsigned long long deadline_ns;   // 0 = no deadline
 };
 
+__device__ __forceinline__ unsigned atom_add_acq_rel(unsigned* p, unsigned v) {
+  unsigned old;
+  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void st_relaxed(unsigned* p, unsigned v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
+}
+
 __device__ __forceinline__ bool grid_barrier(const GridBarrier& b) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned* gen = b.generation;
-    const unsigned g = *gen;
-    __threadfence();
-    const unsigned arrived = atomicAdd(b.count, 1u);
+    const unsigned g = ld_acquire(b.generation);
+    const unsigned arrived = atom_add_acq_rel(b.count, 1u);
     int good = 1;
     if (arrived == gridDim.x - 1) {
       if (b.deadline_ns != 0ull && global_ns() > b.deadline_ns) atomicExch(b.time_up, 1);
-      atomicExch(b.count, 0u);
-      __threadfence();
-      atomicAdd(b.generation, 1u);
+      st_relaxed(b.count, 0u);
+      st_release(b.generation, g + 1u);
     } else {
       const unsigned long long t0 = global_ns();
       unsigned spins = 0;
-      while (*gen == g) {
-        if (++spins > 64) __nanosleep(64);
-        if ((spins & 255u) == 0) {
+      while (ld_acquire(b.generation) == g) {
+        ++spins;
+        if (spins > 4096) __nanosleep(32);
+        if ((spins & 1023u) == 0) {
           if (*((volatile int*)b.error) != 0) {  // another block already gave up
             good = 0;
             break;
@@ -114,7 +132,6 @@ __device__ __forceinline__ bool grid_barrier(const GridBarrier& b) {
         }
       }
     }
-    __threadfence();
     ok = good && (*((volatile int*)b.error) == 0);
   }
   __syncthreads();

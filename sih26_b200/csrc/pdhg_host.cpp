@@ -210,23 +210,65 @@ PermutedLp permute(const sankhya_pdhg_problem& p, const std::vector<double>& v) 
 }
 
 static int lanes_for(int len) {
-  // smallest power of two with at most four nonzeros per lane, capped at a warp
+  // smallest power of two with at most sixteen nonzeros per lane, capped at a warp
   int lanes = 1;
-  while (lanes < 32 && lanes * 4 < len) lanes *= 2;
+  while (lanes < 32 && lanes * 16 < len) lanes *= 2;
   return lanes;
 }
 
+// A warp works through its items one after another and each costs about one round of
+// dependent memory latency, whatever its length, so the balance counts work units: one per
+// item or segment, plus a small term for its nonzeros.
+static double unit_cost(int nnz) { return 1.0 + nnz / 2048.0; }
+
 HostPart partition(const std::vector<int>& ptr, int G, int warps_per_block, int lanes_override) {
-  constexpr int kSeg = 256;  // == kSegment in pdhg_kernels.cuh
+  constexpr int kSeg = 512;        // == kSegment in pdhg_kernels.cuh
+  constexpr int kItem = 512;       // == kItemNnz
+  constexpr int kStreamRow = 32;   // == kStreamRowMax
+  (void)warps_per_block;
   const int rows = static_cast<int>(ptr.size()) - 1;
   const auto len = [&](int r) { return ptr[r + 1] - ptr[r]; };
-  const auto cost = [&](int r) { return static_cast<double>(len(r)) + 2.0; };
-  double total = 0.0;
-  for (int r = 0; r < rows; ++r) total += cost(r);
-  const double target = total / G;
-  // long rows: the prefix longer than one segment (rows are sorted longest first)
+  // long rows: the prefix longer than one item (rows are sorted longest first)
   int L = 0;
-  while (L < rows && len(L) > kSeg) ++L;
+  while (L < rows && len(L) > kItem) ++L;
+  // items of short rows: grouped (one lane group per row) for rows longer than kStreamRow or
+  // when a lane count is forced; stream items for the rest
+  std::vector<int4> items;
+  std::vector<double> item_cost;
+  for (int r = L; r < rows;) {
+    if (lanes_override > 0 || len(r) > kStreamRow) {
+      const int lanes = lanes_override > 0 ? lanes_override : lanes_for(len(r));
+      const int per = 32 / lanes;
+      const int begin = r;
+      int nnz = 0;
+      while (r < rows && r - begin < per &&
+             (lanes_override > 0 || (len(r) > kStreamRow && lanes_for(len(r)) == lanes))) {
+        nnz += len(r);
+        ++r;
+      }
+      items.push_back(make_int4(begin, r, lanes, 0));
+      item_cost.push_back(unit_cost(nnz));
+    } else {
+      const int begin = r;
+      int nnz = 0;
+      while (r < rows && r - begin < 32 && nnz + len(r) <= kItem) {
+        nnz += len(r);
+        ++r;
+      }
+      items.push_back(make_int4(begin, r, 0, 0));
+      item_cost.push_back(unit_cost(nnz));
+    }
+  }
+  // work of each long row: its segments plus the segment-sum step
+  double total = 0.0;
+  std::vector<double> long_cost(L);
+  for (int r = 0; r < L; ++r) {
+    const int segs = (len(r) + kSeg - 1) / kSeg;
+    long_cost[r] = segs * unit_cost(kSeg) + 0.5;
+    total += long_cost[r];
+  }
+  for (double c : item_cost) total += c;
+  const double target = total / G;
   // LPT assignment of long rows to blocks
   std::vector<double> load(G, 0.0);
   std::vector<std::vector<int>> blk_long(G);
@@ -237,7 +279,7 @@ HostPart partition(const std::vector<int>& ptr, int G, int warps_per_block, int 
     auto [l, b] = heap.top();
     heap.pop();
     blk_long[b].push_back(r);
-    load[b] = l + cost(r);
+    load[b] = l + long_cost[r];
     heap.push({load[b], b});
   }
   HostPart hp;
@@ -256,43 +298,28 @@ HostPart partition(const std::vector<int>& ptr, int G, int warps_per_block, int 
     hp.blk_seg_begin[b + 1] = static_cast<int>(hp.segs.size());
     hp.blk_long_begin[b + 1] = static_cast<int>(hp.longs.size());
   }
-  // items of short rows, a few per warp
-  const double budget = std::max(64.0, target / (2.0 * warps_per_block));
-  std::vector<int4> items;
-  std::vector<double> item_cost;
-  for (int r = L; r < rows;) {
-    const int lanes = lanes_override > 0 ? lanes_override : lanes_for(len(r));
-    const int begin = r;
-    double c = 0.0;
-    while (r < rows && (r == begin || (c + cost(r) <= budget &&
-                                       (lanes_override > 0 || lanes_for(len(r)) == lanes)))) {
-      c += cost(r);
-      ++r;
+  // items go one by one, in row order, to the least-loaded block (long rows included in
+  // the loads), so every block gets a similar mix of item kinds; each block's items are then
+  // stored contiguously, in row order
+  std::vector<int> owner(items.size());
+  {
+    std::priority_queue<Entry, std::vector<Entry>, std::greater<Entry>> h2;
+    for (int b = 0; b < G; ++b) h2.push({load[b], b});
+    for (size_t i = 0; i < items.size(); ++i) {
+      auto [l, b] = h2.top();
+      h2.pop();
+      owner[i] = b;
+      h2.push({l + item_cost[i], b});
     }
-    items.push_back(make_int4(begin, r, lanes, 0));
-    item_cost.push_back(c);
   }
-  // contiguous runs of items: block b's capacity is what its long rows leave of the common
-  // target; capacities are scaled to the short-row total and filled cumulatively
-  double short_total = 0.0, capsum = 0.0;
-  for (double c : item_cost) short_total += c;
-  std::vector<double> cap(G);
-  for (int b = 0; b < G; ++b) {
-    cap[b] = std::max(0.0, target - load[b]);
-    capsum += cap[b];
-  }
-  const double f = capsum > 0.0 ? short_total / capsum : 0.0;
   hp.blk_item_begin.assign(G + 1, 0);
-  size_t it = 0;
-  double bound = 0.0, acc = 0.0;
-  for (int b = 0; b < G; ++b) {
-    bound += cap[b] * f;
-    while (it < items.size() && (b == G - 1 || acc + item_cost[it] * 0.5 <= bound)) {
-      acc += item_cost[it];
-      ++it;
-    }
-    hp.blk_item_begin[b + 1] = static_cast<int>(it);
-  }
+  for (size_t i = 0; i < items.size(); ++i) ++hp.blk_item_begin[owner[i] + 1];
+  for (int b = 0; b < G; ++b) hp.blk_item_begin[b + 1] += hp.blk_item_begin[b];
+  std::vector<int4> ordered(items.size());
+  std::vector<int> fill(hp.blk_item_begin.begin(), hp.blk_item_begin.end() - 1);
+  for (size_t i = 0; i < items.size(); ++i) ordered[fill[owner[i]]++] = items[i];
+  items.swap(ordered);
+  (void)target;
   hp.items = std::move(items);
   return hp;
 }

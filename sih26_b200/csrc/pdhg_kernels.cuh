@@ -43,13 +43,13 @@ enum : int {
   kDeviceError = 5
 };
 
-// Host <-> device control block; one per LP. Written only by block 0 at kernel exit; every
-// block reads it at kernel entry.
 struct Residuals {
   double primal, dual, gap, primal_objective, dual_objective, absolute_primal, absolute_dual,
       gap_as_verified, complementarity;
 };
 
+// Host <-> device control block of one LP. Block 0 writes it at kernel exit; every block
+// reads it at kernel entry.
 struct Ctrl {
   // step state
   double eta, omega, restart_kkt, best_worst;
@@ -66,15 +66,21 @@ struct Ctrl {
 
 // SpMV work partition of one CSR matrix in permuted row order (rows sorted by length,
 // longest first). Per block b:
-//   segments  [blk_seg_begin[b], blk_seg_begin[b+1]): {row, nz_begin, nz_end, 0} pieces of at
-//             most kSegment nonzeros of this block's long rows, one warp each;
-//   long rows [blk_long_begin[b], blk_long_begin[b+1]): {row, first segment, segments, 0};
-//             after the block's segments are done, one warp sums a long row's segment
-//             partials in segment order and runs the row's epilogue;
-//   items     [blk_item_begin[b], blk_item_begin[b+1]): {row_begin, row_end, lanes, 0} runs
-//             of short rows, each row reduced by a group of `lanes` lanes.
+//   segments  [blk_seg_begin[b], +1): {row, nz_begin, nz_end, 0}, pieces of <= kSegment
+//             nonzeros of this block's long rows (> kItemNnz nonzeros), one warp each;
+//   long rows [blk_long_begin[b], +1): {row, first segment, segments, 0}; once the block's
+//             segments are done, a warp sums a long row's segment partials in order and
+//             runs the row's epilogue;
+//   items     [blk_item_begin[b], +1): {row_begin, row_end, lanes, 0}:
+//             lanes == 0: a stream item, <= 32 rows of <= kStreamRowMax nonzeros and
+//               <= kItemNnz in total; the warp loads all of it at once, parks the products
+//               in shared memory, then lane r sums row r in order and runs its epilogue;
+//             lanes > 0: 32/lanes rows of up to kItemNnz nonzeros, one group of `lanes`
+//               lanes per row, reduced by shuffles.
 // Every long row lives in one block, so no partial crosses blocks and no atomics are needed.
-constexpr int kSegment = 256;
+constexpr int kSegment = 512;
+constexpr int kItemNnz = 512;
+constexpr int kStreamRowMax = 32;
 
 struct Part {
   const int* blk_seg_begin;
@@ -138,9 +144,29 @@ constexpr int kEvalSlots = 16;
 // complementarity slots of the evaluation are max-reductions
 constexpr unsigned kEvalMaxMask = (1u << 6) | (1u << 7) | (1u << 12) | (1u << 13);
 
+// dynamic shared memory of the phase kernels: one stream buffer of kItemNnz products per warp
+constexpr size_t stream_smem_bytes() { return (size_t)kWarps * kItemNnz * sizeof(double); }
+
+// Loads of iterate vectors written earlier in the same launch by other blocks. Plain
+// (L1-cacheable) loads: the grid barrier's release/acquire pairs order them after the
+// writes, and L1 keeps the hot entries of a gathered vector close.
 template <class T>
 __device__ __forceinline__ double ld(const T* p) {
-  return static_cast<double>(__ldcg(p));
+  return static_cast<double>(*p);
+}
+
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
+// Pulls a contiguous nonzero range [nz0, nz1) of one CSR matrix towards L2, one 128-byte line
+// per lane per step.
+template <class V>
+__device__ __forceinline__ void prefetch_range(const int* idx, const V* val, int nz0, int nz1,
+                                               int lane) {
+  for (int k = nz0 + lane * 32; k < nz1; k += 32 * 32) prefetch_l2(idx + k);
+  constexpr int per_line = 128 / (int)sizeof(V);
+  for (int k = nz0 + lane * per_line; k < nz1; k += 32 * per_line) prefetch_l2(val + k);
 }
 template <class T>
 __device__ __forceinline__ double ro(const T* p) {
@@ -150,23 +176,30 @@ __device__ __forceinline__ double ro(const T* p) {
 // ---- generic fused SpMV phase ----------------------------------------------------------
 //
 // For every row r of the matrix owned by this block: s = sum_k val[k] * gather(idx[k])
-// (NV gathered vectors at once, FP64 accumulation), then epi(r, s, acc). Block rows are
-// reduced over the whole block; short rows over a group of `lanes` lanes.
+// (NV gathered vectors at once, FP64 accumulation), then the epilogue:
+//   typename Epi::In in = epi.load(r);   issued before the row's sum so its loads overlap
+//   epi.apply(r, s, in, acc);
+// `stream` is this warp's kItemNnz doubles of dynamic shared memory; a stream item with
+// NV > 1 gathered vectors passes over it once per vector.
 template <int NV, int NS, class V, class Gather, class Epi>
 __device__ __forceinline__ void run_phase(const int* __restrict__ ptr, const int* __restrict__ idx,
                                           const V* __restrict__ val, const Part& p,
-                                          const Gather& g, const Epi& epi, double (&acc)[NS]) {
+                                          const Gather& g, const Epi& epi, double (&acc)[NS],
+                                          double* stream) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int b = blockIdx.x;
-  // 1. segments of long rows: one warp per segment of <= kSegment nonzeros
+  // 1. segments of long rows: one warp per segment
   const int sb = __ldg(p.blk_seg_begin + b), se = __ldg(p.blk_seg_begin + b + 1);
   for (int q = sb + warp; q < se; q += kWarps) {
     const int4 sg = __ldg(p.segs + q);
     double s[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) s[v] = 0.0;
-#pragma unroll 8
-    for (int k = sg.y + lane; k < sg.z; k += 32) g.add(s, ro(val + k), __ldg(idx + k));
+#pragma unroll
+    for (int t = 0; t < kSegment / 32; ++t) {
+      const int k = sg.y + lane + 32 * t;
+      if (k < sg.z) g.add(s, ro(val + k), __ldg(idx + k));
+    }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
 #pragma unroll
@@ -177,30 +210,68 @@ __device__ __forceinline__ void run_phase(const int* __restrict__ ptr, const int
       for (int v = 0; v < NV; ++v) p.seg_sum[(size_t)q * NV + v] = s[v];
     }
   }
-  // 2. short rows
+  // 2. short rows; each item first pulls the warp's next item towards L2
   const int ib = __ldg(p.blk_item_begin + b), ie = __ldg(p.blk_item_begin + b + 1);
+  int4 item = ib + warp < ie ? __ldg(p.items + ib + warp) : make_int4(0, 0, 0, 0);
   for (int it = ib + warp; it < ie; it += kWarps) {
-    const int4 item = __ldg(p.items + it);
-    const int lanes = item.z;
-    const int groups = 32 / lanes;
-    const int gid = lane / lanes, gl = lane - gid * lanes;
-    for (int base = item.x; base < item.y; base += groups) {
-      const int r = base + gid;
+    int4 next = make_int4(0, 0, 0, 0);
+    if (it + kWarps < ie) {
+      next = __ldg(p.items + it + kWarps);
+      prefetch_range(idx, val, __ldg(ptr + next.x), __ldg(ptr + next.y), lane);
+    }
+    if (item.z == 0) {
+      // stream item
+      const int rows = item.y - item.x;
+      const int r = item.x + lane;
+      const bool mine = lane < rows;
+      typename Epi::In in{};
+      int rb = 0, re = 0;
+      if (mine) {
+        in = epi.load(r);
+        rb = __ldg(ptr + r);
+        re = __ldg(ptr + r + 1);
+      }
+      const int nz0 = __ldg(ptr + item.x), nz1 = __ldg(ptr + item.y);
+      double s[NV];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+#pragma unroll
+        for (int t = 0; t < kItemNnz / 32; ++t) {
+          const int k = nz0 + lane + 32 * t;
+          if (k < nz1) stream[k - nz0] = g.product(v, ro(val + k), __ldg(idx + k));
+        }
+        __syncwarp();
+        double sum = 0.0;
+        if (mine) {
+          for (int k = rb - nz0; k < re - nz0; ++k) sum += stream[k];
+        }
+        s[v] = sum;
+        __syncwarp();
+      }
+      if (mine) epi.apply(r, s, in, acc);
+    } else {
+      // grouped item: one group of item.z lanes per row
+      const int lanes = item.z;
+      const int gid = lane / lanes, gl = lane - gid * lanes;
+      const int r = item.x + gid;
       const bool valid = r < item.y;
+      typename Epi::In in{};
       double s[NV];
 #pragma unroll
       for (int v = 0; v < NV; ++v) s[v] = 0.0;
       if (valid) {
+        if (gl == 0) in = epi.load(r);
         const int kb = __ldg(ptr + r), ke = __ldg(ptr + r + 1);
-#pragma unroll 4
+#pragma unroll 16
         for (int k = kb + gl; k < ke; k += lanes) g.add(s, ro(val + k), __ldg(idx + k));
       }
       for (int off = lanes >> 1; off > 0; off >>= 1) {
 #pragma unroll
         for (int v = 0; v < NV; ++v) s[v] += __shfl_xor_sync(0xffffffffu, s[v], off);
       }
-      if (valid && gl == 0) epi(r, s, acc);
+      if (valid && gl == 0) epi.apply(r, s, in, acc);
     }
+    item = next;
   }
   // 3. long rows: sum the block's segment partials in segment order, then the epilogue
   const int lb = __ldg(p.blk_long_begin + b), le = __ldg(p.blk_long_begin + b + 1);
@@ -208,6 +279,8 @@ __device__ __forceinline__ void run_phase(const int* __restrict__ ptr, const int
     __syncthreads();
     for (int q = lb + warp; q < le; q += kWarps) {
       const int4 lr = __ldg(p.longs + q);
+      typename Epi::In in{};
+      if (lane == 0) in = epi.load(lr.x);
       double s[NV];
 #pragma unroll
       for (int v = 0; v < NV; ++v) s[v] = 0.0;
@@ -220,7 +293,7 @@ __device__ __forceinline__ void run_phase(const int* __restrict__ ptr, const int
 #pragma unroll
         for (int v = 0; v < NV; ++v) s[v] += __shfl_xor_sync(0xffffffffu, s[v], off);
       }
-      if (lane == 0) epi(lr.x, s, acc);
+      if (lane == 0) epi.apply(lr.x, s, in, acc);
     }
   }
 }
@@ -231,6 +304,7 @@ template <class T>
 struct Gather1 {
   const T* v;
   __device__ __forceinline__ void add(double (&s)[1], double a, int k) const { s[0] += a * ld(v + k); }
+  __device__ __forceinline__ double product(int, double a, int k) const { return a * ld(v + k); }
 };
 
 template <class T, class U>
@@ -240,6 +314,9 @@ struct Gather2 {
   __device__ __forceinline__ void add(double (&s)[2], double a, int k) const {
     s[0] += a * ld(v0 + k);
     s[1] += a * ld(v1 + k);
+  }
+  __device__ __forceinline__ double product(int which, double a, int k) const {
+    return which == 0 ? a * ld(v0 + k) : a * ld(v1 + k);
   }
 };
 
@@ -256,13 +333,25 @@ struct PrimalStep {
   double* xsum;
   double tau;
   int pending;
-  __device__ __forceinline__ void operator()(int j, const double (&s)[1], double (&acc)[3]) const {
-    const double xo = ld(x + j);
-    if (pending) xsum[j] = __ldcg(xsum + j) + xo;
-    const double xnew = project(xo - tau * (ro(c + j) + s[0]), ro(cl + j), ro(cu + j));
+  struct In {
+    double xo, c, lo, hi, xs;
+  };
+  __device__ __forceinline__ In load(int j) const {
+    In v;
+    v.xo = ld(x + j);
+    v.c = ro(c + j);
+    v.lo = ro(cl + j);
+    v.hi = ro(cu + j);
+    v.xs = pending ? __ldcg(xsum + j) : 0.0;
+    return v;
+  }
+  __device__ __forceinline__ void apply(int j, const double (&s)[1], const In& v,
+                                        double (&acc)[3]) const {
+    if (pending) xsum[j] = v.xs + v.xo;
+    const double xnew = project(v.xo - tau * (v.c + s[0]), v.lo, v.hi);
     const T xs = static_cast<T>(xnew);
     xn[j] = xs;
-    const double d = static_cast<double>(xs) - xo;
+    const double d = static_cast<double>(xs) - v.xo;
     acc[0] += d * d;
   }
 };
@@ -280,19 +369,43 @@ struct DualStep {
   double* ysum;
   double sigma;
   int pending;
-  __device__ __forceinline__ void operator()(int i, const double (&s)[1], double (&acc)[3]) const {
-    const double yo = ld(y + i);
-    if (pending) ysum[i] = __ldcg(ysum + i) + yo;
+  struct In {
+    double yo, aold, lo, hi, ys;
+  };
+  __device__ __forceinline__ In load(int i) const {
+    In v;
+    v.yo = ld(y + i);
+    v.aold = __ldcg(ax + i);
+    v.lo = ro(rl + i);
+    v.hi = ro(ru + i);
+    v.ys = pending ? __ldcg(ysum + i) : 0.0;
+    return v;
+  }
+  __device__ __forceinline__ void apply(int i, const double (&s)[1], const In& v,
+                                        double (&acc)[3]) const {
+    if (pending) ysum[i] = v.ys + v.yo;
     const double anew = s[0];
-    const double aold = __ldcg(ax + i);
-    const double v = yo + sigma * (2.0 * anew - aold);
-    const double ynew = v - sigma * project(v / sigma, ro(rl + i), ro(ru + i));
+    const double w = v.yo + sigma * (2.0 * anew - v.aold);
+    const double ynew = w - sigma * project(w / sigma, v.lo, v.hi);
     const T ys = static_cast<T>(ynew);
     yn[i] = ys;
     axn[i] = anew;
-    const double d = static_cast<double>(ys) - yo;
+    const double d = static_cast<double>(ys) - v.yo;
     acc[1] += d * d;
-    acc[2] += d * (anew - aold);
+    acc[2] += d * (anew - v.aold);
+  }
+};
+
+// Stores the row sum (setup of A x0, and the power iteration); optionally its square.
+template <int NS>
+struct StoreRow {
+  double* out;
+  int square_into;  // slot that gets s^2, or -1
+  struct In {};
+  __device__ __forceinline__ In load(int) const { return In{}; }
+  __device__ __forceinline__ void apply(int r, const double (&s)[1], const In&, double (&acc)[NS]) const {
+    out[r] = s[0];
+    if (square_into >= 0) acc[square_into] += s[0] * s[0];
   }
 };
 
@@ -321,13 +434,43 @@ __device__ __forceinline__ void write_partials(double* partials, int first_slot,
   }
 }
 
+__device__ __forceinline__ double* warp_stream() {
+  extern __shared__ double dyn_smem[];
+  return dyn_smem + (size_t)(threadIdx.x >> 5) * kItemNnz;
+}
+
 // ---- the iteration kernel ---------------------------------------------------------------
 
+#ifdef SIH26_PHASE_TIMING
+// Instrumented builds only: per-block nanoseconds spent in phase P, barrier 1, phase D,
+// barrier 2 and the control step, summed over attempts (read back with
+// sih26_phase_timing_read).
+__device__ unsigned long long g_phase_ns[4096 * 5];
+#define SIH26_MARK(k)                                                  \
+  do {                                                                 \
+    __syncthreads();                                                   \
+    if (threadIdx.x == 0) {                                            \
+      const unsigned long long now_ = global_ns();                     \
+      g_phase_ns[blockIdx.x * 5 + (k)] += now_ - mark_ns;              \
+      mark_ns = now_;                                                  \
+    }                                                                  \
+  } while (0)
+#define SIH26_MARK_START() (mark_ns = threadIdx.x == 0 ? global_ns() : 0ull)
+#else
+#define SIH26_MARK(k) \
+  do {                \
+  } while (0)
+#define SIH26_MARK_START() (mark_ns = 0ull)
+#endif
+
 template <class T>
-__global__ void __launch_bounds__(kThreads) iterate_kernel(Prob<T> P, State<T> S,
-                                                           long long max_attempts) {
+__global__ void __launch_bounds__(kThreads, 2) iterate_kernel(Prob<T> P, State<T> S,
+                                                              long long max_attempts) {
+  unsigned long long mark_ns = 0;
+  (void)mark_ns;
   __shared__ Ctrl c;
   __shared__ double sh[kWarps * 4];
+  double* stream = warp_stream();
   if (threadIdx.x == 0) c = *S.ctrl;
   __syncthreads();
   if (c.state != kRunning) return;
@@ -350,18 +493,24 @@ __global__ void __launch_bounds__(kThreads) iterate_kernel(Prob<T> P, State<T> S
     const double sigma = c.eta * c.omega;
     double* part = S.partials + (size_t)(c.attempts & 1) * G * kPartSlots;
     double acc[3] = {0.0, 0.0, 0.0};
-
-    PrimalStep<T> ps{S.x[cur], S.x[nxt], P.c, P.cl, P.cu, S.xsum, tau, c.pending};
-    run_phase<1, 3>(P.AT.ptr, P.AT.idx, P.AT.val, P.pat, Gather1<T>{S.y[cur]}, ps, acc);
+    SIH26_MARK_START();
+    {
+      PrimalStep<T> ps{S.x[cur], S.x[nxt], P.c, P.cl, P.cu, S.xsum, tau, c.pending};
+      run_phase<1, 3>(P.AT.ptr, P.AT.idx, P.AT.val, P.pat, Gather1<T>{S.y[cur]}, ps, acc, stream);
+    }
+    SIH26_MARK(0);
     if (!grid_barrier(S.bar)) goto device_error;
+    SIH26_MARK(1);
 
     {
       DualStep<T> ds{S.y[cur], S.y[nxt], S.ax[cur], S.ax[nxt], P.rl, P.ru, S.ysum, sigma, c.pending};
-      run_phase<1, 3>(P.A.ptr, P.A.idx, P.A.val, P.pa, Gather1<T>{S.x[nxt]}, ds, acc);
+      run_phase<1, 3>(P.A.ptr, P.A.idx, P.A.val, P.pa, Gather1<T>{S.x[nxt]}, ds, acc, stream);
     }
+    SIH26_MARK(2);
     block_reduce<3, 0u>(acc, sh);
     write_partials(part, 0, acc, 3);
     if (!grid_barrier(S.bar)) goto device_error;
+    SIH26_MARK(3);
 
     {
       double tot[3];
@@ -391,6 +540,7 @@ __global__ void __launch_bounds__(kThreads) iterate_kernel(Prob<T> P, State<T> S
         if (c.iteration != 0 && (c.iteration % 40 == 0 || no_information)) c.state = kNeedEval;
       }
       __syncthreads();
+      SIH26_MARK(4);
       if (c.state != kRunning) break;
     }
   }
@@ -398,6 +548,18 @@ __global__ void __launch_bounds__(kThreads) iterate_kernel(Prob<T> P, State<T> S
   return;
 device_error:
   if (blockIdx.x == 0 && threadIdx.x == 0) S.ctrl->state = kDeviceError;
+}
+
+// A x for the starting point, through the same phase code and partition as phase D, so that
+// A x' - A x is exactly zero whenever x' == x (the reference's interaction is then exactly
+// zero, pdhg.cpp:424-438, 454).
+template <class T>
+__global__ void __launch_bounds__(kThreads, 2) init_ax_kernel(Prob<T> P, State<T> S) {
+  double* stream = warp_stream();
+  double dummy[1] = {0.0};
+  const int cur = S.ctrl->cur;
+  run_phase<1, 1>(P.A.ptr, P.A.idx, P.A.val, P.pa, Gather1<T>{S.x[cur]},
+                  StoreRow<1>{S.ax[cur], -1}, dummy, stream);
 }
 
 // ---- evaluation ---------------------------------------------------------------------------
@@ -412,14 +574,27 @@ struct RowEval {
   const T* y;          // candidate 0 (scaled)
   const double* yavg;  // candidate 1 (scaled)
   const double* ycand; // when non-null: candidate 0 in FP64 (the report)
-  __device__ __forceinline__ void operator()(int i, const double (&s)[NC], double (&acc)[kEvalSlots]) const {
-    const double d_r = __ldg(dr + i);
-    const double lo = __ldg(rl0 + i), hi = __ldg(ru0 + i);
+  double* y_out;       // report: unscaled multipliers
+  struct In {
+    double dr, lo, hi, y0, y1;
+  };
+  __device__ __forceinline__ In load(int i) const {
+    In v;
+    v.dr = __ldg(dr + i);
+    v.lo = __ldg(rl0 + i);
+    v.hi = __ldg(ru0 + i);
+    v.y0 = ycand ? __ldcg(ycand + i) : ld(y + i);
+    v.y1 = NC > 1 ? __ldcg(yavg + i) : 0.0;
+    return v;
+  }
+  __device__ __forceinline__ void apply(int i, const double (&s)[NC], const In& v,
+                                        double (&acc)[kEvalSlots]) const {
+    const double lo = v.lo, hi = v.hi;
 #pragma unroll
     for (int q = 0; q < NC; ++q) {
-      const double act = s[q] / d_r;
-      const double ys = q == 0 ? (ycand ? __ldcg(ycand + i) : ld(y + i)) : __ldcg(yavg + i);
-      const double yi = ys * d_r;
+      const double act = s[q] / v.dr;
+      const double yi = (q == 0 ? v.y0 : v.y1) * v.dr;
+      if (y_out && q == 0) y_out[i] = yi;
       double viol = 0.0;
       if (finite_bound(lo)) viol = dmax(viol, lo - act);
       if (finite_bound(hi)) viol = dmax(viol, act - hi);
@@ -452,14 +627,26 @@ struct ColEval {
   const double* xcand;  // report: candidate 0 in FP64
   double* x_out;        // report outputs (unscaled, permuted order)
   double* reduced_out;
-  __device__ __forceinline__ void operator()(int j, const double (&s)[NC], double (&acc)[kEvalSlots]) const {
-    const double d_c = __ldg(dc + j);
-    const double lo = __ldg(cl0 + j), hi = __ldg(cu0 + j), cj = __ldg(c0 + j);
+  struct In {
+    double dc, lo, hi, c, x0, x1;
+  };
+  __device__ __forceinline__ In load(int j) const {
+    In v;
+    v.dc = __ldg(dc + j);
+    v.lo = __ldg(cl0 + j);
+    v.hi = __ldg(cu0 + j);
+    v.c = __ldg(c0 + j);
+    v.x0 = xcand ? __ldcg(xcand + j) : ld(x + j);
+    v.x1 = NC > 1 ? __ldcg(xavg + j) : 0.0;
+    return v;
+  }
+  __device__ __forceinline__ void apply(int j, const double (&s)[NC], const In& v,
+                                        double (&acc)[kEvalSlots]) const {
+    const double lo = v.lo, hi = v.hi;
 #pragma unroll
     for (int q = 0; q < NC; ++q) {
-      const double d = cj + s[q] / d_c;
-      const double xs = q == 0 ? (xcand ? __ldcg(xcand + j) : ld(x + j)) : __ldcg(xavg + j);
-      const double xj = xs * d_c;
+      const double d = v.c + s[q] / v.dc;
+      const double xj = (q == 0 ? v.x0 : v.x1) * v.dc;
       if (x_out && q == 0) {
         x_out[j] = xj;
         reduced_out[j] = d;
@@ -474,7 +661,7 @@ struct ColEval {
         const double us = finite_bound(hi) ? hi - xj : INFINITY;
         acc[12 + q] = dmax(acc[12 + q], fabs(d) * dmin(ls, us));
       }
-      acc[14 + q] += cj * xj;
+      acc[14 + q] += v.c * xj;
     }
   }
 };
@@ -507,10 +694,11 @@ __device__ __forceinline__ bool meets_project_standard(const Residuals& r) {
 }
 
 template <class T>
-__global__ void __launch_bounds__(kThreads) evaluate_kernel(Prob<T> P, State<T> S) {
+__global__ void __launch_bounds__(kThreads, 2) evaluate_kernel(Prob<T> P, State<T> S) {
   __shared__ Ctrl c;
   __shared__ double sh[kWarps * kEvalSlots];
   __shared__ int flags[3];  // best updated, restart, chosen average
+  double* stream = warp_stream();
   if (threadIdx.x == 0) c = *S.ctrl;
   __syncthreads();
   if (c.state != kNeedEval) return;
@@ -550,12 +738,12 @@ __global__ void __launch_bounds__(kThreads) evaluate_kernel(Prob<T> P, State<T> 
     double acc[kEvalSlots];
 #pragma unroll
     for (int s = 0; s < kEvalSlots; ++s) acc[s] = 0.0;
-    RowEval<T, 2> re{P.dr, P.rl0, P.ru0, S.y[cur], S.yavg, nullptr};
+    RowEval<T, 2> re{P.dr, P.rl0, P.ru0, S.y[cur], S.yavg, nullptr, nullptr};
     run_phase<2, kEvalSlots>(P.A.ptr, P.A.idx, P.A.val64, P.pa,
-                             Gather2<T, double>{S.x[cur], S.xavg}, re, acc);
+                             Gather2<T, double>{S.x[cur], S.xavg}, re, acc, stream);
     ColEval<T, 2> ce{P.dc, P.cl0, P.cu0, P.c0, S.x[cur], S.xavg, nullptr, nullptr, nullptr};
     run_phase<2, kEvalSlots>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pat,
-                             Gather2<T, double>{S.y[cur], S.yavg}, ce, acc);
+                             Gather2<T, double>{S.y[cur], S.yavg}, ce, acc, stream);
     block_reduce<kEvalSlots, kEvalMaxMask>(acc, sh);
     write_partials(part, 2, acc, kEvalSlots);
   }
@@ -657,23 +845,22 @@ device_error:
   if (blockIdx.x == 0 && threadIdx.x == 0) S.ctrl->state = kDeviceError;
 }
 
-// Final report (pdhg.cpp:647-661): residuals of the best point, its unscaled value and
-// reduced costs. Writes the residual block to ctrl->best.
+// Final report (pdhg.cpp:647-661): residuals of the best point, its unscaled value, reduced
+// costs and multipliers. Writes the residual block to ctrl->best.
 template <class T>
-__global__ void __launch_bounds__(kThreads) report_kernel(Prob<T> P, State<T> S, double* x_out,
-                                                          double* reduced_out, double* y_out) {
+__global__ void __launch_bounds__(kThreads, 2) report_kernel(Prob<T> P, State<T> S, double* x_out,
+                                                             double* reduced_out, double* y_out) {
   __shared__ double sh[kWarps * kEvalSlots];
+  double* stream = warp_stream();
   double acc[kEvalSlots];
 #pragma unroll
   for (int s = 0; s < kEvalSlots; ++s) acc[s] = 0.0;
-  RowEval<T, 1> re{P.dr, P.rl0, P.ru0, nullptr, nullptr, S.best_y};
-  run_phase<1, kEvalSlots>(P.A.ptr, P.A.idx, P.A.val64, P.pa, Gather1<double>{S.best_x}, re, acc);
+  RowEval<T, 1> re{P.dr, P.rl0, P.ru0, nullptr, nullptr, S.best_y, y_out};
+  run_phase<1, kEvalSlots>(P.A.ptr, P.A.idx, P.A.val64, P.pa, Gather1<double>{S.best_x}, re, acc,
+                           stream);
   ColEval<T, 1> ce{P.dc, P.cl0, P.cu0, P.c0, nullptr, nullptr, S.best_x, x_out, reduced_out};
-  run_phase<1, kEvalSlots>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pat, Gather1<double>{S.best_y}, ce, acc);
-  const int stride = gridDim.x * kThreads;
-  for (int i = blockIdx.x * kThreads + threadIdx.x; i < P.m; i += stride) {
-    y_out[i] = __ldcg(S.best_y + i) * __ldg(P.dr + i);
-  }
+  run_phase<1, kEvalSlots>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pat, Gather1<double>{S.best_y}, ce,
+                           acc, stream);
   block_reduce<kEvalSlots, kEvalMaxMask>(acc, sh);
   write_partials(S.partials, 2, acc, kEvalSlots);
   if (!grid_barrier(S.bar)) {
@@ -687,22 +874,27 @@ __global__ void __launch_bounds__(kThreads) report_kernel(Prob<T> P, State<T> S,
   }
 }
 
-// ---- setup kernels ---------------------------------------------------------------------
-
-// ax = A x for the starting point (FP64 values). One warp per row (setup only).
-template <class T>
-__global__ void spmv_rows_kernel(int rows, const int* __restrict__ ptr, const int* __restrict__ idx,
-                                 const double* __restrict__ val, const T* x, double* out) {
-  const int lane = threadIdx.x & 31;
-  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nw = (gridDim.x * blockDim.x) >> 5;
-  for (int r = w; r < rows; r += nw) {
-    double s = 0.0;
-    for (int k = ptr[r] + lane; k < ptr[r + 1]; k += 32) s += val[k] * static_cast<double>(x[idx[k]]);
-    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-    if (lane == 0) out[r] = s;
+// FP32 -> FP64 hand-over of the mixed-precision mode: the FP64 iterate starts at the FP32
+// one, which also becomes the restart anchor; the running sums start empty.
+__global__ void handover_kernel(const float* x32, const float* y32, double* x64, double* y64,
+                                double* xr64, double* yr64, double* xsum, double* ysum, int m,
+                                int n) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
+    const double v = x32[j];
+    x64[j] = v;
+    xr64[j] = v;
+    xsum[j] = 0.0;
+  }
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
+    const double v = y32[i];
+    y64[i] = v;
+    yr64[i] = v;
+    ysum[i] = 0.0;
   }
 }
+
+// ---- norm estimate -----------------------------------------------------------------------
 
 // Power iteration on A'A for ||A||_2 (src/la/scaling.cpp:161-194), cooperative: per step
 // normalise v, u = A v, v = A' u, norm = ||v||^(1/2). Writes the estimate (x1.01) to *out.
@@ -713,35 +905,26 @@ struct PowerState {
   GridBarrier bar;
 };
 
-template <class T>
-struct PowerGather {
+struct ScaledGather {
   const double* v;
   double inv;
-  __device__ __forceinline__ void add(double (&s)[1], double a, int k) const { s[0] += a * (__ldcg(v + k) * inv); }
-};
-
-struct StoreRow {
-  double* out;
-  __device__ __forceinline__ void operator()(int r, const double (&s)[1], double (&acc)[1]) const { out[r] = s[0]; }
-};
-struct StoreRowNorm {
-  double* out;
-  __device__ __forceinline__ void operator()(int r, const double (&s)[1], double (&acc)[1]) const {
-    out[r] = s[0];
-    acc[0] += s[0] * s[0];
-  }
+  __device__ __forceinline__ void add(double (&s)[1], double a, int k) const { s[0] += a * (ld(v + k) * inv); }
+  __device__ __forceinline__ double product(int, double a, int k) const { return a * (ld(v + k) * inv); }
 };
 
 template <class T>
-__global__ void __launch_bounds__(kThreads) power_kernel(Prob<T> P, PowerState W, int iterations,
-                                                         double* out) {
+__global__ void __launch_bounds__(kThreads, 2) power_kernel(Prob<T> P, PowerState W, int iterations,
+                                                            double* out) {
   __shared__ double sh[kWarps * 2];
+  double* stream = warp_stream();
   const int G = gridDim.x, stride = G * kThreads;
   const int gt = blockIdx.x * kThreads + threadIdx.x;
-  double norm = 0.0;
   // ||v||^2 of the random start
   double a0[1] = {0.0};
-  for (int j = gt; j < P.n; j += stride) { const double t = __ldcg(W.v + j); a0[0] += t * t; }
+  for (int j = gt; j < P.n; j += stride) {
+    const double t = __ldcg(W.v + j);
+    a0[0] += t * t;
+  }
   block_reduce<1, 0u>(a0, sh);
   write_partials(W.partials, 0, a0, 1);
   if (!grid_barrier(W.bar)) return;
@@ -754,20 +937,19 @@ __global__ void __launch_bounds__(kThreads) power_kernel(Prob<T> P, PowerState W
       return;
     }
     double dummy[1] = {0.0};
-    run_phase<1, 1>(P.A.ptr, P.A.idx, P.A.val64, P.pa, PowerGather<T>{W.v, 1.0 / length},
-                    StoreRow{W.u}, dummy);
+    run_phase<1, 1>(P.A.ptr, P.A.idx, P.A.val64, P.pa, ScaledGather{W.v, 1.0 / length},
+                    StoreRow<1>{W.u, -1}, dummy, stream);
     if (!grid_barrier(W.bar)) return;
     double nx[1] = {0.0};
-    run_phase<1, 1>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pat, PowerGather<T>{W.u, 1.0},
-                    StoreRowNorm{W.v}, nx);
+    run_phase<1, 1>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pat, ScaledGather{W.u, 1.0},
+                    StoreRow<1>{W.v, 0}, nx, stream);
     block_reduce<1, 0u>(nx, sh);
     write_partials(W.partials + (size_t)((step + 1) & 1) * G * kPartSlots, 0, nx, 1);
     if (!grid_barrier(W.bar)) return;
-    norm = 0.0;  // recomputed from the partials at the next step (or below)
   }
   double fin[1];
   reduce_partials<1, 0u>(W.partials + (size_t)(iterations & 1) * G * kPartSlots, 0, fin, sh);
-  norm = sqrt(sqrt(fin[0]));
+  const double norm = sqrt(sqrt(fin[0]));
   if (blockIdx.x == 0 && threadIdx.x == 0) *out = norm > 0.0 ? norm * 1.01 : 1.0;
 }
 

@@ -104,8 +104,8 @@ static Part upload_part(Arena& a, const HostPart& hp) {
   return p;
 }
 
-static void launch_coop(const void* fn, int grid, void** args, cudaStream_t stream) {
-  SIH26_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kThreads), args, 0, stream),
+static void launch_coop(const void* fn, int grid, void** args, size_t smem, cudaStream_t stream) {
+  SIH26_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kThreads), args, smem, stream),
              SANKHYA_GPU_KERNEL_LAUNCH_FAILED);
 }
 
@@ -191,49 +191,78 @@ static Level<T> make_level(Arena& a, const Common& cm, const PermutedLp& q, cons
   return L;
 }
 
+// Opts every kernel into its dynamic shared memory and returns how many blocks of each fit
+// on an SM (the minimum over the kernels, which share one work partition).
 template <class T>
 static int blocks_per_sm() {
-  int a = 0, b = 0, c = 0, d = 0;
-  SIH26_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, iterate_kernel<T>, kThreads, 0),
+  const void* k1[] = {reinterpret_cast<const void*>(iterate_kernel<T>),
+                      reinterpret_cast<const void*>(init_ax_kernel<T>),
+                      reinterpret_cast<const void*>(report_kernel<T>),
+                      reinterpret_cast<const void*>(power_kernel<T>)};
+  int best = 1 << 20;
+  for (const void* f : k1) {
+    SIH26_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)stream_smem_bytes()), SANKHYA_GPU_INIT_FAILED);
+    int b = 0;
+    SIH26_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, f, kThreads, stream_smem_bytes()),
+               SANKHYA_GPU_INIT_FAILED);
+    best = std::min(best, b);
+  }
+  const void* ek = reinterpret_cast<const void*>(evaluate_kernel<T>);
+  SIH26_CUDA(cudaFuncSetAttribute(ek, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)stream_smem_bytes()), SANKHYA_GPU_INIT_FAILED);
+  int b = 0;
+  SIH26_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, ek, kThreads, stream_smem_bytes()),
              SANKHYA_GPU_INIT_FAILED);
-  SIH26_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, evaluate_kernel<T>, kThreads, 0),
-             SANKHYA_GPU_INIT_FAILED);
-  SIH26_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, report_kernel<T>, kThreads, 0),
-             SANKHYA_GPU_INIT_FAILED);
-  SIH26_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d, power_kernel<T>, kThreads, 0),
-             SANKHYA_GPU_INIT_FAILED);
-  return std::min(std::min(a, b), std::min(c, d));
+  return std::min(best, b);
 }
 
-// Runs (iterate, evaluate) launch pairs until the device reports a final state.
+// Runs (iterate, evaluate) launch pairs until the device reports a final state. With
+// `watch_stall` (the FP32 phase of the mixed mode) it also returns, with *stalled set, once
+// the best KKT error has not moved over two host checks of at least 16 pairs each: the FP32
+// iterate has reached what its precision allows.
 template <class T>
 static Ctrl run_loop(Level<T>& L, int G, cudaStream_t stream, Ctrl* host_ctrl, int verbose,
-                     const std::vector<double>* log_unused) {
-  (void)log_unused;
+                     bool watch_stall, bool* stalled) {
   long long max_attempts = 1ll << 40;
   int pairs = 4;
   Ctrl c{};
+  double last_best = INFINITY;
+  int flat = 0;
+  if (stalled) *stalled = false;
   for (;;) {
     for (int k = 0; k < pairs; ++k) {
       void* ia[] = {&L.P, &L.S, &max_attempts};
-      launch_coop(reinterpret_cast<const void*>(iterate_kernel<T>), G, ia, stream);
+      launch_coop(reinterpret_cast<const void*>(iterate_kernel<T>), G, ia, stream_smem_bytes(), stream);
       void* ea[] = {&L.P, &L.S};
-      launch_coop(reinterpret_cast<const void*>(evaluate_kernel<T>), G, ea, stream);
+      launch_coop(reinterpret_cast<const void*>(evaluate_kernel<T>), G, ea, stream_smem_bytes(), stream);
     }
     SIH26_CUDA(cudaMemcpyAsync(host_ctrl, L.S.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, stream),
                SANKHYA_GPU_COPY_FAILED);
     SIH26_CUDA(cudaStreamSynchronize(stream), SANKHYA_GPU_SYNC_FAILED);
     c = *host_ctrl;
     if (verbose) {
-      std::printf("%10lld %12.5e %10.3e %10.3e %10.3e %9.2e %9.2e\n", c.iteration,
+      std::printf("%10lld %12.5e %10.3e %10.3e %10.3e %9.2e %9.2e %s\n", c.iteration,
                   c.best.primal_objective, c.best.primal, c.best.dual, c.best.gap, c.eta,
-                  c.omega);
+                  c.omega, sizeof(T) == 4 ? "fp32" : "fp64");
       std::fflush(stdout);
     }
     if (c.state != kRunning && c.state != kNeedEval) break;
+    if (watch_stall && pairs >= 16) {
+      flat = (c.best_worst >= last_best) ? flat + 1 : 0;
+      if (flat >= 2) {
+        *stalled = true;
+        break;
+      }
+    }
+    last_best = c.best_worst;
     if (pairs < 64) pairs *= 2;
   }
   return c;
+}
+
+static int G_max_coresident(const cudaDeviceProp& props, int bpsm) {
+  return props.multiProcessorCount * bpsm;
 }
 
 static void fill_message(sankhya_pdhg_result* r, const char* text) {
@@ -297,6 +326,7 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
   int G = props.multiProcessorCount * std::min(bpsm, 2);
   const long long work = q.nnz + m + n;
   G = static_cast<int>(std::max<long long>(1, std::min<long long>(G, (work + 4095) / 4096)));
+  if (prm.grid_blocks > 0) G = std::min(G_max_coresident(props, bpsm), prm.grid_blocks);
 
   Arena a;
   cudaStream_t stream;
@@ -356,20 +386,17 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
     double* d_norm = a.zeros<double>(1);
     int iters = 30;
     void* pa[] = {&L64.P, &W, &iters, &d_norm};
-    launch_coop(reinterpret_cast<const void*>(power_kernel<double>), G, pa, stream);
+    launch_coop(reinterpret_cast<const void*>(power_kernel<double>), G, pa, stream_smem_bytes(), stream);
     SIH26_CUDA(cudaMemcpyAsync(&spectral_norm, d_norm, sizeof(double), cudaMemcpyDeviceToHost, stream),
                SANKHYA_GPU_COPY_FAILED);
   }
-  // A x0 for the starting point
-  {
-    const int blocks = std::max(1, std::min(4096, (m * 32 + 255) / 256));
-    if (mixed) {
-      spmv_rows_kernel<float><<<blocks, 256, 0, stream>>>(m, cm.a_ptr, cm.a_idx, cm.a_val64, L32.S.x[0], L32.S.ax[0]);
-    } else {
-      spmv_rows_kernel<double><<<blocks, 256, 0, stream>>>(m, cm.a_ptr, cm.a_idx, cm.a_val64, L64.S.x[0], L64.S.ax[0]);
-    }
-    SIH26_CUDA(cudaGetLastError(), SANKHYA_GPU_KERNEL_LAUNCH_FAILED);
+  // A x0 for the starting point, with the same phase code as the iteration's A x'
+  if (mixed) {
+    init_ax_kernel<float><<<G, kThreads, stream_smem_bytes(), stream>>>(L32.P, L32.S);
+  } else {
+    init_ax_kernel<double><<<G, kThreads, stream_smem_bytes(), stream>>>(L64.P, L64.S);
   }
+  SIH26_CUDA(cudaGetLastError(), SANKHYA_GPU_KERNEL_LAUNCH_FAILED);
   int err_flag = 0;
   SIH26_CUDA(cudaStreamSynchronize(stream), SANKHYA_GPU_SYNC_FAILED);
   SIH26_CUDA(cudaMemcpy(&err_flag, flags, sizeof(int), cudaMemcpyDeviceToHost), SANKHYA_GPU_COPY_FAILED);
@@ -438,9 +465,48 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
   if (!mixed) {
     SIH26_CUDA(cudaMemcpyAsync(cm.ctrl, &c0, sizeof(Ctrl), cudaMemcpyHostToDevice, stream),
                SANKHYA_GPU_COPY_FAILED);
-    fin = run_loop(L64, G, stream, host_ctrl, prm.verbose, nullptr);
+    fin = run_loop(L64, G, stream, host_ctrl, prm.verbose, false, nullptr);
   } else {
-    throw Failure{SANKHYA_GPU_INVALID_ARGUMENT, "mixed precision is not built yet"};
+    // FP32 phase: relative KKT to the request (or to the switch tolerance when one is set),
+    // handing over early if the FP32 iterate stalls
+    const double fp32_target = prm.mixed_switch_tolerance > 0.0
+                                   ? std::max(prm.tolerance, prm.mixed_switch_tolerance)
+                                   : prm.tolerance;
+    Ctrl c32 = c0;
+    c32.stop_rule = 1;
+    c32.tolerance = fp32_target;
+    SIH26_CUDA(cudaMemcpyAsync(cm.ctrl, &c32, sizeof(Ctrl), cudaMemcpyHostToDevice, stream),
+               SANKHYA_GPU_COPY_FAILED);
+    bool stalled = false;
+    fin = run_loop(L32, G, stream, host_ctrl, prm.verbose, true, &stalled);
+    fp32_iterations = fin.iteration;
+    const bool done_in_fp32 = fin.state == kConverged && prm.stop_rule == 1 &&
+                              fp32_target <= prm.tolerance;
+    const bool limit_hit = fin.state == kIterationLimit || fin.state == kTimeLimit ||
+                           fin.state == kDeviceError;
+    if (!done_in_fp32 && !limit_hit) {
+      // FP64 polish, warm-started from the FP32 iterate
+      const int threads = 256, blocks = std::max(1, std::min(4096, (std::max(m, n) + threads - 1) / threads));
+      handover_kernel<<<blocks, threads, 0, stream>>>(L32.S.x[fin.cur], L32.S.y[fin.cur], L64.S.x[0],
+                                                     L64.S.y[0], L64.S.xr, L64.S.yr, L64.S.xsum,
+                                                     L64.S.ysum, m, n);
+      SIH26_CUDA(cudaGetLastError(), SANKHYA_GPU_KERNEL_LAUNCH_FAILED);
+      Ctrl h = fin;
+      h.cur = 0;
+      h.pending = 0;
+      h.averaged = 0;
+      h.last_restart = h.iteration;
+      h.restart_kkt = h.best_worst;
+      h.state = kRunning;
+      h.converged = 0;
+      h.tolerance = prm.tolerance;
+      h.stop_rule = prm.stop_rule;
+      SIH26_CUDA(cudaMemcpyAsync(cm.ctrl, &h, sizeof(Ctrl), cudaMemcpyHostToDevice, stream),
+                 SANKHYA_GPU_COPY_FAILED);
+      init_ax_kernel<double><<<G, kThreads, stream_smem_bytes(), stream>>>(L64.P, L64.S);
+      SIH26_CUDA(cudaGetLastError(), SANKHYA_GPU_KERNEL_LAUNCH_FAILED);
+      fin = run_loop(L64, G, stream, host_ctrl, prm.verbose, false, nullptr);
+    }
   }
   SIH26_CUDA(cudaEventRecord(ev1, stream), SANKHYA_GPU_INIT_FAILED);
   if (fin.state == kDeviceError)
@@ -452,7 +518,7 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
   double* d_y = a.zeros<double>(m);
   {
     void* ra[] = {&L64.P, &L64.S, &d_x, &d_red, &d_y};
-    launch_coop(reinterpret_cast<const void*>(report_kernel<double>), G, ra, stream);
+    launch_coop(reinterpret_cast<const void*>(report_kernel<double>), G, ra, stream_smem_bytes(), stream);
   }
   SIH26_CUDA(cudaMemcpyAsync(host_ctrl, cm.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, stream),
              SANKHYA_GPU_COPY_FAILED);
@@ -550,7 +616,7 @@ void sankhya_pdhg_gpu_default_params(sankhya_pdhg_params* p) {
   p->device = 0;
   p->verbose = 0;
   p->detect_infeasibility = 1;
-  p->mixed_switch_tolerance = 1e-5;
+  p->mixed_switch_tolerance = 0.0;
 }
 
 int sankhya_pdhg_gpu_solve(const sankhya_pdhg_problem* problem, const sankhya_pdhg_params* params,
@@ -579,6 +645,18 @@ int sankhya_pdhg_gpu_solve(const sankhya_pdhg_problem* problem, const sankhya_pd
 }
 
 const char* sankhya_pdhg_gpu_last_error(void) { return sih26::g_last_error.c_str(); }
+
+#ifdef SIH26_PHASE_TIMING
+// Instrumented builds only (see SIH26_MARK in pdhg_kernels.cuh).
+int sih26_phase_timing_read(unsigned long long* out, int count) {
+  return cudaMemcpyFromSymbol(out, sih26::g_phase_ns, sizeof(unsigned long long) * count) ==
+                 cudaSuccess ? 0 : 1;
+}
+int sih26_phase_timing_reset(void) {
+  static unsigned long long zero[4096 * 5];
+  return cudaMemcpyToSymbol(sih26::g_phase_ns, zero, sizeof zero) == cudaSuccess ? 0 : 1;
+}
+#endif
 
 int sankhya_pdhg_gpu_device_count(void) {
   int n = 0;

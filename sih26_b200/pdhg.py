@@ -68,7 +68,8 @@ class _Params(C.Structure):
                 ("precision", C.c_int32), ("stop_rule", C.c_int32), ("device", C.c_int32),
                 ("verbose", C.c_int32), ("detect_infeasibility", C.c_int32),
                 ("mixed_switch_tolerance", C.c_double), ("group_size_rows", C.c_int32),
-                ("group_size_cols", C.c_int32), ("reserved", C.c_int32 * 8)]
+                ("group_size_cols", C.c_int32), ("grid_blocks", C.c_int32),
+                ("reserved", C.c_int32 * 7)]
 
 
 class _Residuals(C.Structure):
@@ -133,11 +134,12 @@ class Options:
         "log_to_console": (bool, False),
         "pdhg_precision": (str, "fp64"),
         "pdhg_stop_rule": (str, "reference"),
-        "pdhg_mixed_switch_tolerance": (float, 1e-5),
+        "pdhg_mixed_switch_tolerance": (float, 0.0),
         "pdhg_detect_infeasibility": (bool, True),
         "gpu_device": (int, 0),
         "pdhg_lanes_rows": (int, 0),
         "pdhg_lanes_cols": (int, 0),
+        "pdhg_grid_blocks": (int, 0),
     }
 
     def __init__(self, **values):
@@ -249,6 +251,7 @@ def solve_pdhg(model: LP, options: Optional[Options] = None) -> Solution:
     prm.mixed_switch_tolerance = opt.get("pdhg_mixed_switch_tolerance")
     prm.group_size_rows = opt.get("pdhg_lanes_rows")
     prm.group_size_cols = opt.get("pdhg_lanes_cols")
+    prm.grid_blocks = opt.get("pdhg_grid_blocks")
     n, m = model.num_cols, model.num_rows
     x = np.zeros(n)
     rd = np.zeros(m)

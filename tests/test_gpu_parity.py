@@ -59,10 +59,20 @@ def test_reference_unit_test_answers(name, lp, expected):
 
 
 def test_matches_reference_fixture():
+    """Every fixture record: same status, objective within 1e-6, iteration count close.
+
+    The GPU sums in a different order, so its trajectory drifts from the reference's by
+    rounding; restarts and the stopping test can then trigger a few evaluations apart. Under
+    pdhg_stop_at_request both `feasible` and `optimal` mean "stopped on the request"; which
+    one is reported depends on whether the stopping point also happens to meet the absolute
+    standard, and on a borderline point that turns on rounding. That interchange is the one
+    status difference accepted, and it is counted. The GPU may converge faster than the
+    reference; it may not be more than 50 % slower."""
     golden = json.load(open(GOLDEN))
     cases = {n: lp for n, lp, _ in hand_cases()}
     cases.update(dict(generated_cases()))
-    worst_iter = 0.0
+    worst_slowdown = 0.0
+    mismatches, interchanges, lines = [], 0, []
     for rec in golden["cases"]:
         lp = cases[rec["case"]]
         s = P.solve_pdhg(lp, _opts(pdhg_tolerance=rec["opt_tolerance"],
@@ -70,17 +80,28 @@ def test_matches_reference_fixture():
                                    pdhg_restart=rec["opt_restart"],
                                    pdhg_stop_at_request=rec["opt_stop_at_request"]))
         key = (rec["case"], rec["options"])
-        assert s.status == rec["status"], (key, s.message)
+        lines.append(f"{key}: ref {rec['status']} {rec['iterations']} / gpu {s.status} {s.iterations}")
+        if s.status != rec["status"]:
+            if rec["opt_stop_at_request"] and {s.status, rec["status"]} == {"feasible", "optimal"}:
+                interchanges += 1
+            else:
+                mismatches.append((key, rec["status"], s.status, s.message))
+                continue
         if rec["status"] in ("optimal", "feasible"):
             scale = max(1.0, abs(rec["objective"]))
             assert abs(s.objective - rec["objective"]) <= 1e-6 * scale, key
+            assert s.primal_infeasibility <= 1e-7, key
         else:
             assert s.iterations == rec["iterations"], key  # the limit itself
             assert math.isinf(s.dual_bound)
         ref_it = rec["iterations"]
-        worst_iter = max(worst_iter, abs(s.iterations - ref_it) / max(ref_it, 40))
-    # FP64 on the GPU follows the reference's trajectory up to summation order
-    assert worst_iter <= 0.5
+        worst_slowdown = max(worst_slowdown, (s.iterations - ref_it) / max(ref_it, 40))
+    print("\n".join(lines))
+    print(f"feasible/optimal interchanges under stop_at_request: {interchanges}; "
+          f"worst slowdown {worst_slowdown:.2f}")
+    assert not mismatches, mismatches
+    assert interchanges <= 3
+    assert worst_slowdown <= 0.5
 
 
 @pytest.mark.parametrize("name,lp", generated_cases())
@@ -145,3 +166,22 @@ def test_single_lp_2000x5000_against_oracle():
     assert abs(s.objective - lp.optimal_objective) <= 1e-6 * scale
     assert abs(s.objective - o.objective) <= 1e-6 * scale
     assert np.array_equal(_pattern(lp, s.col_value), _pattern(lp, o.col_value))
+
+
+@pytest.mark.parametrize("rule", ["relative_kkt", "reference"])
+def test_mixed_precision_against_oracle(rule):
+    """FP32 iterates with FP64 reductions, then the FP64 polish when the request needs it."""
+    lp = lpgen.uniform_planted(2000, 5000, 10, seed=0)
+    tol = 1e-6
+    s = P.solve_pdhg(lp, _opts(pdhg_tolerance=tol, pdhg_precision="mixed", pdhg_stop_rule=rule))
+    assert s.status in ("optimal", "feasible"), s.message
+    assert s.fp32_iterations > 0
+    r = oracle.oracle_evaluate(lp, s.col_value, _y_pdhg_sign(lp, s))
+    assert max(r["primal"], r["dual"], r["gap"]) <= tol
+    scale = max(1.0, abs(lp.optimal_objective))
+    assert abs(s.objective - lp.optimal_objective) <= 1e-6 * scale
+    if rule == "reference":
+        assert s.status == "optimal"
+        assert s.iterations > s.fp32_iterations  # the FP64 polish ran
+        o = oracle.oracle_solve(lp, tolerance=tol)
+        assert np.array_equal(_pattern(lp, s.col_value), _pattern(lp, o.col_value))
