@@ -121,7 +121,8 @@ typedef struct sankhya_pdhg_params {
   int32_t group_size_rows;  /* lanes per row for A x (0 = autotune) */
   int32_t group_size_cols;  /* lanes per row for A'y (0 = autotune) */
   int32_t grid_blocks;      /* blocks of the cooperative launches (0 = sized to the problem) */
-  int32_t reserved[7];
+  int32_t profile_kernels;  /* 1: time every iteration-kernel launch with CUDA events */
+  int32_t reserved[6];
 } sankhya_pdhg_params;
 
 /* Unscaled residual block of the reported point (src/pdhg/pdhg.cpp:81-110). */
@@ -159,6 +160,11 @@ typedef struct sankhya_pdhg_result {
   double setup_seconds;  /* validation, scaling, upload, norm estimate */
   double solve_seconds;  /* the iteration loop, device-timed */
   double total_seconds;  /* the whole call, host wall clock */
+  int64_t h2d_bytes;     /* host -> device bytes copied by the call */
+  int64_t d2h_bytes;     /* device -> host bytes copied by the call */
+  double iterate_kernel_seconds; /* profile_kernels: summed event-timed iteration launches */
+  int64_t iterate_launches;      /* profile_kernels: how many were timed */
+  int64_t kernel_launches;       /* every kernel this call launched */
   sankhya_pdhg_residuals residuals;
   char message[512];
 } sankhya_pdhg_result;

@@ -35,9 +35,11 @@ static double seconds_since(Clock::time_point t0) {
   return std::chrono::duration<double>(Clock::now() - t0).count();
 }
 
-// Owns every device allocation of one solve.
+// Owns every device allocation of one solve and counts the bytes it copies.
 class Arena {
  public:
+  long long h2d_bytes = 0;
+  long long d2h_bytes = 0;
   ~Arena() {
     for (void* p : ptrs_) cudaFree(p);
   }
@@ -62,6 +64,7 @@ class Arena {
       std::vector<T> conv(host.begin(), host.end());
       SIH26_CUDA(cudaMemcpy(p, conv.data(), conv.size() * sizeof(T), cudaMemcpyHostToDevice),
                  SANKHYA_GPU_COPY_FAILED);
+      h2d_bytes += conv.size() * sizeof(T);
     }
     return p;
   }
@@ -71,8 +74,20 @@ class Arena {
     if (!host.empty()) {
       SIH26_CUDA(cudaMemcpy(p, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice),
                  SANKHYA_GPU_COPY_FAILED);
+      h2d_bytes += host.size() * sizeof(T);
     }
     return p;
+  }
+  // host -> device copy of a plain buffer, counted
+  void put(void* dst, const void* src, size_t bytes, cudaStream_t stream) {
+    if (bytes == 0) return;
+    SIH26_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream), SANKHYA_GPU_COPY_FAILED);
+    h2d_bytes += bytes;
+  }
+  void get(void* dst, const void* src, size_t bytes, cudaStream_t stream) {
+    if (bytes == 0) return;
+    SIH26_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, stream), SANKHYA_GPU_COPY_FAILED);
+    d2h_bytes += bytes;
   }
 
  private:
@@ -104,9 +119,13 @@ static Part upload_part(Arena& a, const HostPart& hp) {
   return p;
 }
 
+// Kernel launches of the current call on this thread (reported in the result).
+thread_local long long g_launches = 0;
+
 static void launch_coop(const void* fn, int grid, void** args, size_t smem, cudaStream_t stream) {
   SIH26_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kThreads), args, smem, stream),
              SANKHYA_GPU_KERNEL_LAUNCH_FAILED);
+  ++g_launches;
 }
 
 __global__ void read_clock_kernel(unsigned long long* out) { *out = global_ns(); }
@@ -183,10 +202,9 @@ static Level<T> make_level(Arena& a, const Common& cm, const PermutedLp& q, cons
   S.bar = cm.bar;
   if (!x0.empty()) {
     std::vector<T> xt(x0.begin(), x0.end());
-    SIH26_CUDA(cudaMemcpy(S.x[0], xt.data(), n * sizeof(T), cudaMemcpyHostToDevice),
-               SANKHYA_GPU_COPY_FAILED);
-    SIH26_CUDA(cudaMemcpy(S.xr, xt.data(), n * sizeof(T), cudaMemcpyHostToDevice),
-               SANKHYA_GPU_COPY_FAILED);
+    a.put(S.x[0], xt.data(), n * sizeof(T), 0);
+    a.put(S.xr, xt.data(), n * sizeof(T), 0);
+    SIH26_CUDA(cudaDeviceSynchronize(), SANKHYA_GPU_SYNC_FAILED);
   }
   return L;
 }
@@ -221,9 +239,42 @@ static int blocks_per_sm() {
 // `watch_stall` (the FP32 phase of the mixed mode) it also returns, with *stalled set, once
 // the best KKT error has not moved over two host checks of at least 16 pairs each: the FP32
 // iterate has reached what its precision allows.
+// Event-timed launches of the iteration kernel (profile_kernels).
+struct LaunchTimer {
+  bool on = false;
+  std::vector<cudaEvent_t> start, stop;
+  double seconds = 0.0;
+  long long launches = 0;
+  ~LaunchTimer() {
+    for (auto e : start) cudaEventDestroy(e);
+    for (auto e : stop) cudaEventDestroy(e);
+  }
+  void ensure(size_t k) {
+    while (start.size() < k) {
+      cudaEvent_t a, b;
+      SIH26_CUDA(cudaEventCreate(&a), SANKHYA_GPU_INIT_FAILED);
+      SIH26_CUDA(cudaEventCreate(&b), SANKHYA_GPU_INIT_FAILED);
+      start.push_back(a);
+      stop.push_back(b);
+    }
+  }
+  void collect(int k) {
+    for (int i = 0; i < k; ++i) {
+      float ms = 0.f;
+      SIH26_CUDA(cudaEventElapsedTime(&ms, start[i], stop[i]), SANKHYA_GPU_SYNC_FAILED);
+      seconds += ms * 1e-3;
+      ++launches;
+    }
+  }
+};
+
+// Runs (iterate, evaluate) launch pairs until the device reports a final state. With
+// `watch_stall` (the FP32 phase of the mixed mode) it also returns, with *stalled set, once
+// the best KKT error has not moved over two host checks of at least 16 pairs each: the FP32
+// iterate has reached what its precision allows.
 template <class T>
 static Ctrl run_loop(Level<T>& L, int G, cudaStream_t stream, Ctrl* host_ctrl, int verbose,
-                     bool watch_stall, bool* stalled) {
+                     bool watch_stall, bool* stalled, LaunchTimer& timer) {
   long long max_attempts = 1ll << 40;
   int pairs = 4;
   Ctrl c{};
@@ -231,15 +282,19 @@ static Ctrl run_loop(Level<T>& L, int G, cudaStream_t stream, Ctrl* host_ctrl, i
   int flat = 0;
   if (stalled) *stalled = false;
   for (;;) {
+    if (timer.on) timer.ensure(pairs);
     for (int k = 0; k < pairs; ++k) {
       void* ia[] = {&L.P, &L.S, &max_attempts};
+      if (timer.on) SIH26_CUDA(cudaEventRecord(timer.start[k], stream), SANKHYA_GPU_INIT_FAILED);
       launch_coop(reinterpret_cast<const void*>(iterate_kernel<T>), G, ia, stream_smem_bytes(), stream);
+      if (timer.on) SIH26_CUDA(cudaEventRecord(timer.stop[k], stream), SANKHYA_GPU_INIT_FAILED);
       void* ea[] = {&L.P, &L.S};
       launch_coop(reinterpret_cast<const void*>(evaluate_kernel<T>), G, ea, stream_smem_bytes(), stream);
     }
     SIH26_CUDA(cudaMemcpyAsync(host_ctrl, L.S.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, stream),
                SANKHYA_GPU_COPY_FAILED);
     SIH26_CUDA(cudaStreamSynchronize(stream), SANKHYA_GPU_SYNC_FAILED);
+    if (timer.on) timer.collect(pairs);
     c = *host_ctrl;
     if (verbose) {
       std::printf("%10lld %12.5e %10.3e %10.3e %10.3e %9.2e %9.2e %s\n", c.iteration,
@@ -272,6 +327,7 @@ static void fill_message(sankhya_pdhg_result* r, const char* text) {
 static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_params& prm,
                       sankhya_pdhg_result* res) {
   const Clock::time_point t_start = Clock::now();
+  g_launches = 0;
   check_structure(prob);
   if (!(prm.tolerance > 0.0)) throw Failure{SANKHYA_GPU_INVALID_ARGUMENT, "tolerance must be > 0"};
   if (prm.precision != SANKHYA_PDHG_FP64 && prm.precision != SANKHYA_PDHG_MIXED)
@@ -369,8 +425,8 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
     else if (host_finite_bound(sc.cu[j]) && v > sc.cu[j]) v = sc.cu[j];
     x0[t] = v;
   }
-  SIH26_CUDA(cudaMemcpy(cm.best_x, x0.data(), n * sizeof(double), cudaMemcpyHostToDevice),
-             SANKHYA_GPU_COPY_FAILED);
+  a.put(cm.best_x, x0.data(), n * sizeof(double), 0);
+  SIH26_CUDA(cudaDeviceSynchronize(), SANKHYA_GPU_SYNC_FAILED);
 
   Level<double> L64 = make_level<double>(a, cm, q, sc, prm.precision == SANKHYA_PDHG_FP64 ? x0 : std::vector<double>());
   Level<float> L32{};
@@ -397,6 +453,7 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
     init_ax_kernel<double><<<G, kThreads, stream_smem_bytes(), stream>>>(L64.P, L64.S);
   }
   SIH26_CUDA(cudaGetLastError(), SANKHYA_GPU_KERNEL_LAUNCH_FAILED);
+  ++g_launches;
   int err_flag = 0;
   SIH26_CUDA(cudaStreamSynchronize(stream), SANKHYA_GPU_SYNC_FAILED);
   SIH26_CUDA(cudaMemcpy(&err_flag, flags, sizeof(int), cudaMemcpyDeviceToHost), SANKHYA_GPU_COPY_FAILED);
@@ -425,6 +482,7 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
   if (std::isfinite(prm.time_limit) && prm.time_limit > 0.0) {
     unsigned long long* d_now = a.zeros<unsigned long long>(1);
     read_clock_kernel<<<1, 1, 0, stream>>>(d_now);
+    ++g_launches;
     unsigned long long now = 0;
     SIH26_CUDA(cudaMemcpy(&now, d_now, sizeof now, cudaMemcpyDeviceToHost), SANKHYA_GPU_COPY_FAILED);
     const double left = prm.time_limit - seconds_since(t_start);
@@ -459,13 +517,14 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
     std::printf("%10s %12s %10s %10s %10s %9s %9s\n", "iteration", "objective", "primal", "dual",
                 "gap", "eta", "omega");
   }
+  LaunchTimer timer;
+  timer.on = prm.profile_kernels != 0;
   SIH26_CUDA(cudaEventRecord(ev0, stream), SANKHYA_GPU_INIT_FAILED);
   Ctrl fin{};
   long long fp32_iterations = 0;
   if (!mixed) {
-    SIH26_CUDA(cudaMemcpyAsync(cm.ctrl, &c0, sizeof(Ctrl), cudaMemcpyHostToDevice, stream),
-               SANKHYA_GPU_COPY_FAILED);
-    fin = run_loop(L64, G, stream, host_ctrl, prm.verbose, false, nullptr);
+    a.put(cm.ctrl, &c0, sizeof(Ctrl), stream);
+    fin = run_loop(L64, G, stream, host_ctrl, prm.verbose, false, nullptr, timer);
   } else {
     // FP32 phase: relative KKT to the request (or to the switch tolerance when one is set),
     // handing over early if the FP32 iterate stalls
@@ -475,10 +534,9 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
     Ctrl c32 = c0;
     c32.stop_rule = 1;
     c32.tolerance = fp32_target;
-    SIH26_CUDA(cudaMemcpyAsync(cm.ctrl, &c32, sizeof(Ctrl), cudaMemcpyHostToDevice, stream),
-               SANKHYA_GPU_COPY_FAILED);
+    a.put(cm.ctrl, &c32, sizeof(Ctrl), stream);
     bool stalled = false;
-    fin = run_loop(L32, G, stream, host_ctrl, prm.verbose, true, &stalled);
+    fin = run_loop(L32, G, stream, host_ctrl, prm.verbose, true, &stalled, timer);
     fp32_iterations = fin.iteration;
     const bool done_in_fp32 = fin.state == kConverged && prm.stop_rule == 1 &&
                               fp32_target <= prm.tolerance;
@@ -491,6 +549,7 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
                                                      L64.S.y[0], L64.S.xr, L64.S.yr, L64.S.xsum,
                                                      L64.S.ysum, m, n);
       SIH26_CUDA(cudaGetLastError(), SANKHYA_GPU_KERNEL_LAUNCH_FAILED);
+      ++g_launches;
       Ctrl h = fin;
       h.cur = 0;
       h.pending = 0;
@@ -501,11 +560,11 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
       h.converged = 0;
       h.tolerance = prm.tolerance;
       h.stop_rule = prm.stop_rule;
-      SIH26_CUDA(cudaMemcpyAsync(cm.ctrl, &h, sizeof(Ctrl), cudaMemcpyHostToDevice, stream),
-                 SANKHYA_GPU_COPY_FAILED);
+      a.put(cm.ctrl, &h, sizeof(Ctrl), stream);
       init_ax_kernel<double><<<G, kThreads, stream_smem_bytes(), stream>>>(L64.P, L64.S);
       SIH26_CUDA(cudaGetLastError(), SANKHYA_GPU_KERNEL_LAUNCH_FAILED);
-      fin = run_loop(L64, G, stream, host_ctrl, prm.verbose, false, nullptr);
+      ++g_launches;
+      fin = run_loop(L64, G, stream, host_ctrl, prm.verbose, false, nullptr, timer);
     }
   }
   SIH26_CUDA(cudaEventRecord(ev1, stream), SANKHYA_GPU_INIT_FAILED);
@@ -523,9 +582,9 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
   SIH26_CUDA(cudaMemcpyAsync(host_ctrl, cm.ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, stream),
              SANKHYA_GPU_COPY_FAILED);
   std::vector<double> hx(n), hred(n), hy(m);
-  if (n) SIH26_CUDA(cudaMemcpyAsync(hx.data(), d_x, n * 8, cudaMemcpyDeviceToHost, stream), SANKHYA_GPU_COPY_FAILED);
-  if (n) SIH26_CUDA(cudaMemcpyAsync(hred.data(), d_red, n * 8, cudaMemcpyDeviceToHost, stream), SANKHYA_GPU_COPY_FAILED);
-  if (m) SIH26_CUDA(cudaMemcpyAsync(hy.data(), d_y, m * 8, cudaMemcpyDeviceToHost, stream), SANKHYA_GPU_COPY_FAILED);
+  a.get(hx.data(), d_x, n * 8, stream);
+  a.get(hred.data(), d_red, n * 8, stream);
+  a.get(hy.data(), d_y, m * 8, stream);
   SIH26_CUDA(cudaStreamSynchronize(stream), SANKHYA_GPU_SYNC_FAILED);
   const Ctrl rep = *host_ctrl;
   if (rep.state == kDeviceError)
@@ -594,6 +653,11 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
   res->dual_bound = verifiable ? sense * f.dual_objective + prob.objective_offset
                                : (prob.maximize ? INFINITY : -INFINITY);
   res->setup_seconds = setup_seconds;
+  res->h2d_bytes = a.h2d_bytes;
+  res->d2h_bytes = a.d2h_bytes;
+  res->iterate_kernel_seconds = timer.seconds;
+  res->iterate_launches = timer.launches;
+  res->kernel_launches = g_launches;
   res->solve_seconds = ms * 1e-3;
   res->total_seconds = seconds_since(t_start);
   return SANKHYA_GPU_SUCCESS;

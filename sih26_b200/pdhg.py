@@ -69,7 +69,7 @@ class _Params(C.Structure):
                 ("verbose", C.c_int32), ("detect_infeasibility", C.c_int32),
                 ("mixed_switch_tolerance", C.c_double), ("group_size_rows", C.c_int32),
                 ("group_size_cols", C.c_int32), ("grid_blocks", C.c_int32),
-                ("reserved", C.c_int32 * 7)]
+                ("profile_kernels", C.c_int32), ("reserved", C.c_int32 * 6)]
 
 
 class _Residuals(C.Structure):
@@ -87,7 +87,10 @@ class _Result(C.Structure):
                 ("fp32_iterations", C.c_int64), ("objective", C.c_double),
                 ("dual_bound", C.c_double), ("spectral_norm", C.c_double),
                 ("setup_seconds", C.c_double), ("solve_seconds", C.c_double),
-                ("total_seconds", C.c_double), ("residuals", _Residuals),
+                ("total_seconds", C.c_double), ("h2d_bytes", C.c_int64),
+                ("d2h_bytes", C.c_int64), ("iterate_kernel_seconds", C.c_double),
+                ("iterate_launches", C.c_int64), ("kernel_launches", C.c_int64),
+                ("residuals", _Residuals),
                 ("message", C.c_char * 512)]
 
 
@@ -140,6 +143,7 @@ class Options:
         "pdhg_lanes_rows": (int, 0),
         "pdhg_lanes_cols": (int, 0),
         "pdhg_grid_blocks": (int, 0),
+        "pdhg_profile_kernels": (bool, False),
     }
 
     def __init__(self, **values):
@@ -197,6 +201,11 @@ class Solution:
     residuals: Optional[dict] = None
     setup_seconds: float = 0.0
     device_seconds: float = 0.0
+    h2d_bytes: int = 0
+    d2h_bytes: int = 0
+    iterate_kernel_seconds: float = 0.0
+    iterate_launches: int = 0
+    kernel_launches: int = 0
 
     def has_primal_values(self) -> bool:
         return self.status in ("optimal", "feasible")
@@ -252,6 +261,7 @@ def solve_pdhg(model: LP, options: Optional[Options] = None) -> Solution:
     prm.group_size_rows = opt.get("pdhg_lanes_rows")
     prm.group_size_cols = opt.get("pdhg_lanes_cols")
     prm.grid_blocks = opt.get("pdhg_grid_blocks")
+    prm.profile_kernels = int(opt.get("pdhg_profile_kernels"))
     n, m = model.num_cols, model.num_rows
     x = np.zeros(n)
     rd = np.zeros(m)
@@ -279,7 +289,10 @@ def solve_pdhg(model: LP, options: Optional[Options] = None) -> Solution:
         attempts=res.attempts, restarts=res.restarts, evaluations=res.evaluations,
         fp32_iterations=res.fp32_iterations, spectral_norm=res.spectral_norm,
         residuals={k: getattr(r, k) for k, _ in _Residuals._fields_},
-        setup_seconds=res.setup_seconds, device_seconds=res.solve_seconds)
+        setup_seconds=res.setup_seconds, device_seconds=res.solve_seconds,
+        h2d_bytes=res.h2d_bytes, d2h_bytes=res.d2h_bytes,
+        iterate_kernel_seconds=res.iterate_kernel_seconds, iterate_launches=res.iterate_launches,
+        kernel_launches=res.kernel_launches)
     if status != "model_error":
         sol.primal_infeasibility = _primal_infeasibility(model, x)
     return sol
