@@ -179,6 +179,34 @@ void sankhya_pdhg_gpu_default_params(sankhya_pdhg_params* params);
 int sankhya_pdhg_gpu_solve(const sankhya_pdhg_problem* problem,
                            const sankhya_pdhg_params* params, sankhya_pdhg_result* result);
 
+/* Unscaled KKT residuals of a point, on the GPU, without allocating any memory.
+ *
+ * This entry point has no counterpart in the reference. It exists for callers that cannot
+ * allocate device memory while they run: an application whose device memory belongs to its
+ * own pool or arena and forbids raw cudaMalloc/cudaFree, a service that fixes its device
+ * budget at start-up, or a latency-critical loop that cannot afford the device-wide
+ * synchronisation cudaMalloc/cudaFree imply. It computes the residual block of
+ * src/pdhg/pdhg.cpp:143-263 (the same definitions sankhya_pdhg_gpu_solve reports in
+ * result->residuals) for the point (x, row_dual) of the LP `problem`.
+ *
+ * Every pointer inside `problem`, and x[n], row_dual[m] (reference sign: sense * -y) and
+ * residuals_out[9] (written in sankhya_pdhg_residuals field order), are DEVICE pointers on
+ * the current device; the struct itself is read on the host. Work is queued on `stream`
+ * (a cudaStream_t; NULL = the legacy default stream) and residuals_out is valid once that
+ * stream reaches it. An out-of-range row index makes every output NaN.
+ *
+ * Scratch is a fixed 4 MiB device array inside the library (held by every GPU that loads
+ * it until the process exits), so problems with more than SANKHYA_PDHG_NOALLOC_MAX_ROWS rows
+ * are rejected with SANKHYA_GPU_INVALID_ARGUMENT. The first call on each device resolves the
+ * array's device address (cudaGetSymbolAddress); make that first call before any stream
+ * capture. All calls share the array and each leaves its contents behind (each clears what it
+ * needs zeroed before use): calls whose work overlaps on the GPU race and must be ordered on
+ * one stream. Nothing is allocated, host or device. */
+#define SANKHYA_PDHG_NOALLOC_MAX_ROWS 516064
+int sankhya_pdhg_gpu_residuals_noalloc(const sankhya_pdhg_problem* problem, const double* x,
+                                       const double* row_dual, double* residuals_out,
+                                       void* stream);
+
 /* Reason for the most recent failing call on this thread (never NULL). */
 const char* sankhya_pdhg_gpu_last_error(void);
 

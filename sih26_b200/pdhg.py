@@ -97,7 +97,10 @@ class _Result(C.Structure):
 # Every symbol include/sankhya_pdhg_gpu.h declares.
 EXPORTED_SYMBOLS = ("sankhya_pdhg_gpu_default_params", "sankhya_pdhg_gpu_solve",
                     "sankhya_pdhg_gpu_last_error", "sankhya_pdhg_gpu_device_count",
-                    "sankhya_pdhg_gpu_device_name")
+                    "sankhya_pdhg_gpu_device_name", "sankhya_pdhg_gpu_residuals_noalloc")
+
+# SANKHYA_PDHG_NOALLOC_MAX_ROWS: rows the allocation-free residual check's fixed scratch holds
+NOALLOC_MAX_ROWS = 516064
 
 _lib: Optional[C.CDLL] = None
 
