@@ -45,7 +45,8 @@ typedef enum sankhya_pdhg_gpu_status {
   SANKHYA_GPU_INVALID_DEVICE_STATE = 8,
   SANKHYA_GPU_NON_FINITE_OUTPUT = 9,
   SANKHYA_GPU_INVALID_ARGUMENT = 10, /* malformed problem or parameters; see last_error */
-  SANKHYA_GPU_DEVICE_TIMEOUT = 11    /* a bounded device-side wait gave up; context intact */
+  SANKHYA_GPU_DEVICE_TIMEOUT = 11,   /* a bounded device-side wait gave up; context intact */
+  SANKHYA_GPU_NOT_READY = 12         /* server: the LP has not finished yet */
 } sankhya_pdhg_gpu_status;
 
 /* ---- Solve status of a result: the values of sankhya_solve_status
@@ -206,6 +207,51 @@ int sankhya_pdhg_gpu_solve(const sankhya_pdhg_problem* problem,
 int sankhya_pdhg_gpu_residuals_noalloc(const sankhya_pdhg_problem* problem, const double* x,
                                        const double* row_dual, double* residuals_out,
                                        void* stream);
+
+/* ---- Many LPs at once: the served / batched engine ------------------------------------
+ *
+ * A server keeps LPs resident on one GPU and runs every admitted LP in one persistent kernel
+ * launch per step: each thread block takes LPs from a device work queue (largest first) and
+ * runs the restarted PDHG of src/pdhg/pdhg.cpp on one LP with its own step size, primal
+ * weight, restarts, termination and norm estimate, for at most chunk_attempts attempts per
+ * step. LPs submitted while others run are admitted between steps when their device image
+ * fits the memory pool (a fraction of free HBM taken at creation) and join the next launch;
+ * finished LPs are retired with their answers. Primal infeasibility is certified from the
+ * dual movement between restarts and every certificate is re-checked on the host against
+ * the original model (the test of src/core/certificate.cpp:29-119) before it is reported.
+ * These entry points are the batch / server successors the reference's GPU slot never had. */
+typedef struct sankhya_pdhg_server sankhya_pdhg_server;
+
+typedef struct sankhya_pdhg_server_config {
+  int32_t device;          /* CUDA device ordinal */
+  double memory_fraction;  /* share of free device memory for the pool (default 0.8) */
+  int64_t pool_bytes;      /* explicit pool size; 0 = use memory_fraction */
+  int32_t max_active;      /* LP slots (default 4096) */
+  int64_t chunk_attempts;  /* attempts per LP per step; 0 = run each LP to its end */
+  int32_t reserved[8];
+} sankhya_pdhg_server_config;
+
+void sankhya_pdhg_server_default_config(sankhya_pdhg_server_config* config);
+int sankhya_pdhg_server_create(const sankhya_pdhg_server_config* config,
+                               sankhya_pdhg_server** server);
+/* Prepares the LP on the host (validation, scaling, layout) and queues it; thread-safe. */
+int sankhya_pdhg_server_submit(sankhya_pdhg_server* server, const sankhya_pdhg_problem* problem,
+                               const sankhya_pdhg_params* params, int64_t* ticket);
+/* Admits what fits, runs one launch over every active LP, retires the finished ones. */
+int sankhya_pdhg_server_step(sankhya_pdhg_server* server, int32_t* active, int32_t* waiting,
+                             int32_t* finished);
+/* SANKHYA_GPU_NOT_READY until the LP has finished; then fills `result` (the caller's arrays,
+ * as for sankhya_pdhg_gpu_solve, plus farkas_dual for INFEASIBLE) and forgets the ticket.
+ * setup_seconds / solve_seconds / total_seconds are queueing, device and submit-to-finish
+ * times. */
+int sankhya_pdhg_server_result(sankhya_pdhg_server* server, int64_t ticket,
+                               sankhya_pdhg_result* result);
+void sankhya_pdhg_server_free(sankhya_pdhg_server* server);
+
+/* Solves `count` independent LPs concurrently on one GPU (a server, every LP submitted, run
+ * to the end, results collected). results[k] is filled like sankhya_pdhg_gpu_solve's. */
+int sankhya_pdhg_gpu_batch_solve(const sankhya_pdhg_problem* problems, int32_t count,
+                                 const sankhya_pdhg_params* params, sankhya_pdhg_result* results);
 
 /* Reason for the most recent failing call on this thread (never NULL). */
 const char* sankhya_pdhg_gpu_last_error(void);

@@ -1,0 +1,315 @@
+// Batched restarted PDHG: many independent LPs in one persistent launch.
+//
+// Each block takes LPs from a device work queue (largest first) and runs the whole
+// restarted PDHG of src/pdhg/pdhg.cpp:267-726 on one LP with block-level barriers only: the
+// norm estimate, the attempts (phase P, phase D, step control), the evaluations every 40
+// accepted iterations with per-LP restarts and termination, and the final report. An LP
+// runs for at most `chunk_attempts` attempts per launch and keeps its state in device
+// memory between launches, so a host loop can admit and retire LPs between launches.
+//
+// Per-LP state and work partitions are those of the single-LP kernels with one block
+// (G = 1), so the row sums follow the same code and summation order whatever the batch
+// around an LP: a result is the same alone and in the mix.
+//
+// Primal infeasibility: at every evaluation the dual movement since the last restart,
+// f = -Dr (y - y_r) in original units, is tested as a Farkas certificate in the sense of
+// src/core/certificate.cpp:29-119 (rows aggregate to S = sum f_i * bound chosen by the sign
+// of f_i; the column box allows at most M = max d.x with d = A'f; S > M proves
+// infeasibility). For a feasible LP S <= M for every f, so the test cannot fire on one;
+// the host re-checks every certificate exactly before reporting it.
+#pragma once
+
+#include "pdhg_kernels.cuh"
+
+namespace sih26 {
+
+struct BatchSlot {
+  Prob<double> P;       // single-block partitions
+  State<double> S;      // partials and barrier unused
+  double* x_out;        // report: unscaled x, permuted
+  double* red_out;      // report: min-space reduced costs, permuted
+  double* y_out;        // report: unscaled y (PDHG sign), permuted
+  double* farkas_out;   // certificate f (reference sign, normalised), permuted
+};
+
+// sum_k A'_jk (y - y_r)_k, the column side of the Farkas candidate
+struct DiffGather {
+  const double* y;
+  const double* yr;
+  __device__ __forceinline__ void add(double (&s)[1], double a, int k) const {
+    s[0] += a * (ld(y + k) - ld(yr + k));
+  }
+  __device__ __forceinline__ double product(int, double a, int k) const {
+    return a * (ld(y + k) - ld(yr + k));
+  }
+};
+
+// Column terms of the Farkas test for d = A'f = -(A'_scaled (y - y_r)) / Dc.
+// slots: 0 max |d|, 1 reachable M, 2 max |d| over columns leaning on a missing bound
+struct FarkasCol {
+  const double* dc;
+  const double* cl0;
+  const double* cu0;
+  struct In {
+    double dc, lo, hi;
+  };
+  __device__ __forceinline__ In load(int j) const {
+    return In{__ldg(dc + j), __ldg(cl0 + j), __ldg(cu0 + j)};
+  }
+  __device__ __forceinline__ void apply(int j, const double (&s)[1], const In& v,
+                                        double (&acc)[3]) const {
+    const double d = -s[0] / v.dc;
+    acc[0] = dmax(acc[0], fabs(d));
+    if (d > 0.0) {
+      if (finite_bound(v.hi)) acc[1] += d * v.hi; else acc[2] = dmax(acc[2], d);
+    } else if (d < 0.0) {
+      if (finite_bound(v.lo)) acc[1] += d * v.lo; else acc[2] = dmax(acc[2], -d);
+    }
+  }
+};
+
+// Norm estimate of the LP's scaled matrix (src/la/scaling.cpp:161-194) with one block:
+// v = S.xavg holds the random start, u = S.yavg is scratch.
+__device__ __noinline__ double block_power(const Prob<double>& P, const State<double>& S, int nnz,
+                                     double* sh, double* stream) {
+  if (P.m == 0 || P.n == 0 || nnz == 0) return 1.0;
+  double len2[1] = {0.0};
+  for (int j = threadIdx.x; j < P.n; j += kThreads) {
+    const double t = S.xavg[j];
+    len2[0] += t * t;
+  }
+  block_reduce<1, 0u>(len2, sh);
+  for (int step = 0; step < 30; ++step) {
+    const double length = sqrt(len2[0]);
+    if (length == 0.0) return 1.0;
+    double dummy[1] = {0.0};
+    run_phase<1, 1>(P.A.ptr, P.A.idx, P.A.val64, P.pa, ScaledGather{S.xavg, 1.0 / length},
+                    StoreRow<1>{S.yavg, -1}, dummy, stream, 0);
+    __syncthreads();
+    double nx[1] = {0.0};
+    run_phase<1, 1>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pat, ScaledGather{S.yavg, 1.0},
+                    StoreRow<1>{S.xavg, 0}, nx, stream, 0);
+    block_reduce<1, 0u>(nx, sh);
+    len2[0] = nx[0];
+  }
+  const double norm = sqrt(sqrt(len2[0]));
+  return norm > 0.0 ? norm * 1.01 : 1.0;
+}
+
+// One evaluation of one LP (pdhg.cpp:502-643) with block-level reductions, plus the Farkas
+// candidate test. Leaves c.state at kRunning, kConverged or kInfeasible.
+__device__ __noinline__ void block_evaluate(const BatchSlot& B, Ctrl& c, double* sh, double* stream,
+                                      int* flags) {
+  const Prob<double>& P = B.P;
+  const State<double>& S = B.S;
+  const int cur = c.cur;
+  const bool has_average = c.averaged > 0;
+  const double count = (double)c.averaged;
+  // E1 + Farkas rows. slots: 0 |x-x_r|^2, 1 |y-y_r|^2, 2 S, 3 max|f|, 4 max|f| leaning on a
+  // missing row bound
+  double e1[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  for (int j = threadIdx.x; j < P.n; j += kThreads) {
+    const double xo = ld(S.x[cur] + j);
+    const double xs = S.xsum[j] + (c.pending ? xo : 0.0);
+    S.xsum[j] = xs;
+    S.xavg[j] = has_average ? xs / count : 0.0;
+    const double d = xo - ld(S.xr + j);
+    e1[0] += d * d;
+  }
+  for (int i = threadIdx.x; i < P.m; i += kThreads) {
+    const double yo = ld(S.y[cur] + i);
+    const double ys = S.ysum[i] + (c.pending ? yo : 0.0);
+    S.ysum[i] = ys;
+    S.yavg[i] = has_average ? ys / count : 0.0;
+    const double d = yo - ld(S.yr + i);
+    e1[1] += d * d;
+    const double f = -__ldg(P.dr + i) * d;
+    const double lo = __ldg(P.rl0 + i), hi = __ldg(P.ru0 + i);
+    e1[3] = dmax(e1[3], fabs(f));
+    if (f > 0.0) {
+      if (finite_bound(lo)) e1[2] += f * lo; else e1[4] = dmax(e1[4], f);
+    } else if (f < 0.0) {
+      if (finite_bound(hi)) e1[2] += f * hi; else e1[4] = dmax(e1[4], -f);
+    }
+  }
+  block_reduce<5, (1u << 3) | (1u << 4)>(e1, sh);
+  // E2: residual terms of both candidates (FP64 values)
+  double acc[kEvalSlots];
+#pragma unroll
+  for (int s = 0; s < kEvalSlots; ++s) acc[s] = 0.0;
+  RowEval<double, 2> re{P.dr, P.rl0, P.ru0, S.y[cur], S.yavg, nullptr, nullptr};
+  run_phase<2, kEvalSlots>(P.A.ptr, P.A.idx, P.A.val64, P.pa,
+                           Gather2<double, double>{S.x[cur], S.xavg}, re, acc, stream, 0);
+  ColEval<double, 2> ce{P.dc, P.cl0, P.cu0, P.c0, S.x[cur], S.xavg, nullptr, nullptr, nullptr};
+  run_phase<2, kEvalSlots>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pat,
+                           Gather2<double, double>{S.y[cur], S.yavg}, ce, acc, stream, 0);
+  block_reduce<kEvalSlots, kEvalMaxMask>(acc, sh);
+  // Farkas columns
+  double fk[3] = {0.0, 0.0, 0.0};
+  const bool test_farkas = c.farkas_cooldown == 0 && e1[3] > 0.0;
+  if (test_farkas) {
+    run_phase<1, 3>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pat, DiffGather{S.y[cur], S.yr},
+                    FarkasCol{P.dc, P.cl0, P.cu0}, fk, stream, 0);
+    block_reduce<3, (1u << 0) | (1u << 2)>(fk, sh);
+  }
+  if (threadIdx.x == 0) {
+    const double mv[2] = {e1[0], e1[1]};
+    evaluation_decision(c, acc, mv, has_average, flags);
+    flags[3] = 0;
+    if (c.farkas_cooldown > 0) --c.farkas_cooldown;
+    if (test_farkas && c.state != kConverged) {
+      const double Sn = e1[2] / e1[3], Mn = fk[1] / e1[3];
+      const double margin = Sn - Mn;
+      const bool rows_ok = e1[4] <= 1e-9 * e1[3];
+      const bool cols_ok = fk[2] <= 1e-9 * dmax(fk[0], 1e-300);
+      c.farkas_margin = margin;
+      if (rows_ok && cols_ok && margin > 1e-6 * dmax(1.0, dmax(fabs(Sn), fabs(Mn)))) {
+        c.state = kInfeasible;
+        flags[1] = 0;  // keep the restart anchor: the certificate is read from it
+        flags[3] = 1;
+      }
+    }
+  }
+  __syncthreads();
+  const double fmax = e1[3];  // block_reduce left the totals in every thread
+  // E3: certificate, best point, restart reset
+  if (flags[0] || flags[1] || flags[3]) {
+    for (int j = threadIdx.x; j < P.n; j += kThreads) {
+      const double xo = ld(S.x[cur] + j);
+      if (flags[0]) S.best_x[j] = flags[2] ? S.xavg[j] : xo;
+      if (flags[1]) {
+        S.xr[j] = S.x[cur][j];
+        S.xsum[j] = 0.0;
+      }
+    }
+    for (int i = threadIdx.x; i < P.m; i += kThreads) {
+      const double yo = ld(S.y[cur] + i);
+      if (flags[3]) B.farkas_out[i] = -__ldg(P.dr + i) * (yo - ld(S.yr + i)) / fmax;
+      if (flags[0]) S.best_y[i] = flags[2] ? S.yavg[i] : yo;
+      if (flags[1]) {
+        S.yr[i] = S.y[cur][i];
+        S.ysum[i] = 0.0;
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// Report of one finished LP (pdhg.cpp:647-661): unscaled point, reduced costs, multipliers
+// and the residual block of the best point into c.best.
+__device__ __noinline__ void block_report(const BatchSlot& B, Ctrl& c, double* sh, double* stream) {
+  const Prob<double>& P = B.P;
+  const State<double>& S = B.S;
+  double acc[kEvalSlots];
+#pragma unroll
+  for (int s = 0; s < kEvalSlots; ++s) acc[s] = 0.0;
+  RowEval<double, 1> re{P.dr, P.rl0, P.ru0, nullptr, nullptr, S.best_y, B.y_out};
+  run_phase<1, kEvalSlots>(P.A.ptr, P.A.idx, P.A.val64, P.pa, Gather1<double>{S.best_x}, re, acc,
+                           stream, 0);
+  ColEval<double, 1> ce{P.dc, P.cl0, P.cu0, P.c0, nullptr, nullptr, S.best_x, B.x_out, B.red_out};
+  run_phase<1, kEvalSlots>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pat, Gather1<double>{S.best_y}, ce,
+                           acc, stream, 0);
+  block_reduce<kEvalSlots, kEvalMaxMask>(acc, sh);
+  if (threadIdx.x == 0) c.best = make_residuals(acc, 0, c.bound_norm, c.cost_norm);
+  __syncthreads();
+}
+
+__device__ inline void run_instance(const BatchSlot& B, Ctrl& c, double* sh, double* stream,
+                                    int* flags, long long chunk_attempts) {
+  const Prob<double>& P = B.P;
+  const State<double>& S = B.S;
+  if (threadIdx.x == 0) c = *S.ctrl;
+  __syncthreads();
+  if (c.state == kSetup) {
+    const int nnz = __ldg(P.A.ptr + P.m);
+    const double norm = block_power(P, S, nnz, sh, stream);
+    if (threadIdx.x == 0) {
+      c.spectral_norm = norm;
+      c.eta = norm > 0.0 ? 1.0 / norm : 1.0;
+      c.eta_ceiling = 1.0e3 / dmax(norm, 1e-12);
+      c.state = kRunning;
+    }
+    double dummy[1] = {0.0};
+    run_phase<1, 1>(P.A.ptr, P.A.idx, P.A.val, P.pa, Gather1<double>{S.x[0]},
+                    StoreRow<1>{S.ax[0], -1}, dummy, stream, 0);
+    __syncthreads();
+  }
+  long long a = 0;
+  while (c.state == kRunning) {
+    if (threadIdx.x == 0) {
+      flags[5] = 0;
+      if (c.iteration >= c.iteration_limit) {
+        c.state = kIterationLimit;
+      } else if (c.deadline_ns != 0ull && global_ns() > c.deadline_ns) {
+        c.state = kTimeLimit;
+      } else if (a >= chunk_attempts) {
+        flags[5] = 1;
+      }
+    }
+    __syncthreads();
+    if (c.state != kRunning || flags[5]) break;
+    ++a;
+    const int cur = c.cur, nxt = cur ^ 1;
+    const double tau = c.eta / c.omega;
+    const double sigma = c.eta * c.omega;
+    double acc[3] = {0.0, 0.0, 0.0};
+    {
+      PrimalStep<double> ps{S.x[cur], S.x[nxt], P.c, P.cl, P.cu, S.xsum, tau, c.pending};
+      run_phase<1, 3>(P.AT.ptr, P.AT.idx, P.AT.val, P.pat, Gather1<double>{S.y[cur]}, ps, acc,
+                      stream, 0);
+    }
+    __syncthreads();
+    {
+      DualStep<double> ds{S.y[cur], S.y[nxt], S.ax[cur], S.ax[nxt], P.rl, P.ru, S.ysum, sigma,
+                          c.pending};
+      run_phase<1, 3>(P.A.ptr, P.A.idx, P.A.val, P.pa, Gather1<double>{S.x[nxt]}, ds, acc,
+                      stream, 0);
+    }
+    block_reduce<3, 0u>(acc, sh);
+    if (threadIdx.x == 0) step_control(c, acc);
+    __syncthreads();
+    if (c.state == kNeedEval) block_evaluate(B, c, sh, stream, flags);
+  }
+  if (c.state == kConverged || c.state == kIterationLimit || c.state == kTimeLimit ||
+      c.state == kInfeasible) {
+    block_report(B, c, sh, stream);
+  }
+  if (threadIdx.x == 0) *S.ctrl = c;
+  __syncthreads();
+}
+
+// The persistent batch kernel: blocks take LPs from the active list through a device
+// counter (the list is ordered largest first) until it is exhausted.
+__global__ void __launch_bounds__(kThreads, 2) batch_kernel(const BatchSlot* slots,
+                                                            const int* active,
+                                                            const int* active_count,
+                                                            int* queue_head,
+                                                            long long chunk_attempts) {
+  __shared__ Ctrl c;
+  __shared__ double sh[kWarps * kEvalSlots];
+  __shared__ int flags[8];
+  __shared__ int s_take;
+  double* stream = warp_stream();
+  const int count = *active_count;
+  for (;;) {
+    if (threadIdx.x == 0) s_take = atomicAdd(queue_head, 1);
+    __syncthreads();
+    const int q = s_take;
+    __syncthreads();
+    if (q >= count) break;
+    run_instance(slots[active[q]], c, sh, stream, flags, chunk_attempts);
+  }
+}
+
+// Copies the control blocks of the active LPs into one compact array for the host.
+__global__ void gather_ctrl_kernel(const Ctrl* ctrls, const int* active, const int* active_count,
+                                   Ctrl* out) {
+  const int count = *active_count;
+  for (int q = blockIdx.x; q < count; q += gridDim.x) {
+    const int* src = reinterpret_cast<const int*>(ctrls + active[q]);
+    int* dst = reinterpret_cast<int*>(out + q);
+    for (int w = threadIdx.x; w < (int)(sizeof(Ctrl) / sizeof(int)); w += blockDim.x) dst[w] = src[w];
+  }
+}
+
+}  // namespace sih26

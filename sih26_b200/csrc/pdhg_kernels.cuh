@@ -40,7 +40,9 @@ enum : int {
   kConverged = 2,
   kIterationLimit = 3,
   kTimeLimit = 4,
-  kDeviceError = 5
+  kDeviceError = 5,
+  kSetup = 6,       // batched LPs: norm estimate and A x0 still to do
+  kInfeasible = 7   // batched LPs: a Farkas certificate passed the device test
 };
 
 struct Residuals {
@@ -61,7 +63,9 @@ struct Ctrl {
   double spectral_norm, eta_ceiling, tolerance, bound_norm, cost_norm;
   long long iteration_limit;
   int use_restarts, stop_at_request, stop_rule, pad2;
-  int time_up, pad3;
+  int time_up, farkas_cooldown;
+  unsigned long long deadline_ns;  // batched LPs: device-clock deadline, 0 = none
+  double farkas_margin;            // batched LPs: normalised margin S - M of the last test
 };
 
 // SpMV work partition of one CSR matrix in permuted row order (rows sorted by length,
@@ -185,9 +189,9 @@ template <int NV, int NS, class V, class Gather, class Epi>
 __device__ __forceinline__ void run_phase(const int* __restrict__ ptr, const int* __restrict__ idx,
                                           const V* __restrict__ val, const Part& p,
                                           const Gather& g, const Epi& epi, double (&acc)[NS],
-                                          double* stream) {
+                                          double* stream, int blk = -1) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int b = blockIdx.x;
+  const int b = blk >= 0 ? blk : (int)blockIdx.x;
   // 1. segments of long rows: one warp per segment
   const int sb = __ldg(p.blk_seg_begin + b), se = __ldg(p.blk_seg_begin + b + 1);
   for (int q = sb + warp; q < se; q += kWarps) {
@@ -439,6 +443,33 @@ __device__ __forceinline__ double* warp_stream() {
   return dyn_smem + (size_t)(threadIdx.x >> 5) * kItemNnz;
 }
 
+
+// Adaptive step size and acceptance (pdhg.cpp:413-496) from the attempt's reductions
+// tot = {sum (x'-x)^2, sum (y'-y)^2, sum (y'-y)(A dx)}; flags an evaluation when one is due
+// (pdhg.cpp:502-503). One thread calls it.
+__device__ __forceinline__ void step_control(Ctrl& c, const double (&tot)[3]) {
+  const double movement = 0.5 * c.omega * tot[0] + 0.5 * tot[1] / c.omega;
+  const double interaction = fabs(tot[2]);
+  const bool no_information = interaction <= 0.0;
+  const double limit = no_information ? INFINITY : movement / interaction;
+  const double exponent = (double)(c.iteration + 1 > 2 ? c.iteration + 1 : 2);
+  const double shrink = 1.0 - pow(exponent, -0.3);
+  const double grow = 1.0 + pow(exponent, -0.6);
+  const double proposed = dmin(shrink * limit, grow * c.eta);
+  const bool accept = c.eta <= limit;
+  if (accept) {
+    c.cur ^= 1;
+    ++c.averaged;
+    ++c.iteration;
+  }
+  c.pending = accept ? 1 : 0;
+  if (!no_information) {
+    c.eta = proposed < 1e-12 ? 1e-12 : (c.eta_ceiling < proposed ? c.eta_ceiling : proposed);
+  }
+  ++c.attempts;
+  if (c.iteration != 0 && (c.iteration % 40 == 0 || no_information)) c.state = kNeedEval;
+}
+
 // ---- the iteration kernel ---------------------------------------------------------------
 
 #ifdef SIH26_PHASE_TIMING
@@ -516,28 +547,8 @@ __global__ void __launch_bounds__(kThreads, 2) iterate_kernel(Prob<T> P, State<T
       double tot[3];
       reduce_partials<3, 0u>(part, 0, tot, sh);
       if (threadIdx.x == 0) {
-        // adaptive step size, pdhg.cpp:413-496
-        const double movement = 0.5 * c.omega * tot[0] + 0.5 * tot[1] / c.omega;
-        const double interaction = fabs(tot[2]);
-        const bool no_information = interaction <= 0.0;
-        const double limit = no_information ? INFINITY : movement / interaction;
-        const double exponent = (double)(c.iteration + 1 > 2 ? c.iteration + 1 : 2);
-        const double shrink = 1.0 - pow(exponent, -0.3);
-        const double grow = 1.0 + pow(exponent, -0.6);
-        const double proposed = dmin(shrink * limit, grow * c.eta);
-        const bool accept = c.eta <= limit;
-        if (accept) {
-          c.cur ^= 1;
-          ++c.averaged;
-          ++c.iteration;
-        }
-        c.pending = accept ? 1 : 0;
-        if (!no_information) {
-          c.eta = proposed < 1e-12 ? 1e-12 : (c.eta_ceiling < proposed ? c.eta_ceiling : proposed);
-        }
-        ++c.attempts;
+        step_control(c, tot);
         c.time_up = *((volatile int*)S.bar.time_up);
-        if (c.iteration != 0 && (c.iteration % 40 == 0 || no_information)) c.state = kNeedEval;
       }
       __syncthreads();
       SIH26_MARK(4);
@@ -693,6 +704,77 @@ __device__ __forceinline__ bool meets_project_standard(const Residuals& r) {
          r.complementarity <= 1e-6;
 }
 
+
+// The evaluation's decisions (pdhg.cpp:505-643) from the reduced residual terms t (slots of
+// RowEval / ColEval) and the movement since the last restart mv = {|x-x_r|^2, |y-y_r|^2}:
+// candidate choice, best point, stopping test, restart and primal weight. Sets
+// flags = {best updated, restart, chosen is the average}. One thread calls it.
+__device__ __forceinline__ void evaluation_decision(Ctrl& c, const double (&t)[kEvalSlots],
+                                                    const double (&mv)[2], bool has_average,
+                                                    int* flags) {
+  ++c.evaluations;
+  c.pending = 0;
+  const Residuals current = make_residuals(t, 0, c.bound_norm, c.cost_norm);
+  Residuals better = current;
+  int chosen_average = 0;
+  if (has_average) {
+    const Residuals average = make_residuals(t, 1, c.bound_norm, c.cost_norm);
+    c.average = average;
+    if (worst(average) < worst(current)) {
+      better = average;
+      chosen_average = 1;
+    }
+  }
+  c.current = current;
+  c.chosen_average = chosen_average;
+  int best_updated = 0, restart = 0;
+  if (worst(better) < c.best_worst) {
+    c.best = better;
+    c.best_worst = worst(better);
+    best_updated = 1;
+  }
+  bool stop_here;
+  if (c.stop_rule == 1) {
+    stop_here = worst(better) <= c.tolerance;
+  } else {
+    stop_here = meets_request(better, c.tolerance) &&
+                (c.stop_at_request || meets_project_standard(better));
+  }
+  if (stop_here) {
+    c.best = better;
+    c.best_worst = worst(better);
+    best_updated = 1;
+    c.converged = 1;
+    c.state = kConverged;
+  } else {
+    c.state = kRunning;
+    if (c.use_restarts) {
+      const double kkt = worst(better);
+      const long long since = c.iteration - c.last_restart;
+      const bool sufficient = kkt <= 0.2 * c.restart_kkt;
+      const long long art = (long long)(0.36 * (double)c.iteration);
+      const bool artificial = since >= (art > 40 ? art : 40);
+      if (sufficient || artificial) {
+        const double dx_norm = sqrt(mv[0]), dy_norm = sqrt(mv[1]);
+        if (dx_norm > 1e-12 && dy_norm > 1e-12) {
+          const double theta = 0.5;
+          double w = exp(theta * log(dy_norm / dx_norm) + (1.0 - theta) * log(c.omega));
+          c.omega = w < 1e-6 ? 1e-6 : (1e6 < w ? 1e6 : w);
+        }
+        c.averaged = 0;
+        c.restart_kkt = kkt;
+        c.last_restart = c.iteration;
+        ++c.restarts;
+        restart = 1;
+      }
+    }
+  }
+  c.best_is_set |= best_updated;
+  flags[0] = best_updated;
+  flags[1] = restart;
+  flags[2] = chosen_average;
+}
+
 template <class T>
 __global__ void __launch_bounds__(kThreads, 2) evaluate_kernel(Prob<T> P, State<T> S) {
   __shared__ Ctrl c;
@@ -754,69 +836,7 @@ __global__ void __launch_bounds__(kThreads, 2) evaluate_kernel(Prob<T> P, State<
     reduce_partials<2, 0u>(part, 0, mv, sh);
     double t[kEvalSlots];
     reduce_partials<kEvalSlots, kEvalMaxMask>(part, 2, t, sh);
-    if (threadIdx.x == 0) {
-      ++c.evaluations;
-      c.pending = 0;
-      const Residuals current = make_residuals(t, 0, c.bound_norm, c.cost_norm);
-      Residuals better = current;
-      int chosen_average = 0;
-      if (has_average) {
-        const Residuals average = make_residuals(t, 1, c.bound_norm, c.cost_norm);
-        c.average = average;
-        if (worst(average) < worst(current)) {
-          better = average;
-          chosen_average = 1;
-        }
-      }
-      c.current = current;
-      c.chosen_average = chosen_average;
-      int best_updated = 0, restart = 0;
-      if (worst(better) < c.best_worst) {
-        c.best = better;
-        c.best_worst = worst(better);
-        best_updated = 1;
-      }
-      bool stop_here;
-      if (c.stop_rule == 1) {
-        stop_here = worst(better) <= c.tolerance;
-      } else {
-        stop_here = meets_request(better, c.tolerance) &&
-                    (c.stop_at_request || meets_project_standard(better));
-      }
-      if (stop_here) {
-        c.best = better;
-        c.best_worst = worst(better);
-        best_updated = 1;
-        c.converged = 1;
-        c.state = kConverged;
-      } else {
-        c.state = kRunning;
-        if (c.use_restarts) {
-          const double kkt = worst(better);
-          const long long since = c.iteration - c.last_restart;
-          const bool sufficient = kkt <= 0.2 * c.restart_kkt;
-          const long long art = (long long)(0.36 * (double)c.iteration);
-          const bool artificial = since >= (art > 40 ? art : 40);
-          if (sufficient || artificial) {
-            const double dx_norm = sqrt(mv[0]), dy_norm = sqrt(mv[1]);
-            if (dx_norm > 1e-12 && dy_norm > 1e-12) {
-              const double theta = 0.5;
-              double w = exp(theta * log(dy_norm / dx_norm) + (1.0 - theta) * log(c.omega));
-              c.omega = w < 1e-6 ? 1e-6 : (1e6 < w ? 1e6 : w);
-            }
-            c.averaged = 0;
-            c.restart_kkt = kkt;
-            c.last_restart = c.iteration;
-            ++c.restarts;
-            restart = 1;
-          }
-        }
-      }
-      c.best_is_set |= best_updated;
-      flags[0] = best_updated;
-      flags[1] = restart;
-      flags[2] = chosen_average;
-    }
+    if (threadIdx.x == 0) evaluation_decision(c, t, mv, has_average, flags);
     __syncthreads();
   }
 
@@ -876,7 +896,7 @@ __global__ void __launch_bounds__(kThreads, 2) report_kernel(Prob<T> P, State<T>
 
 // FP32 -> FP64 hand-over of the mixed-precision mode: the FP64 iterate starts at the FP32
 // one, which also becomes the restart anchor; the running sums start empty.
-__global__ void handover_kernel(const float* x32, const float* y32, double* x64, double* y64,
+static __global__ void handover_kernel(const float* x32, const float* y32, double* x64, double* y64,
                                 double* xr64, double* yr64, double* xsum, double* ysum, int m,
                                 int n) {
   const int stride = gridDim.x * blockDim.x;

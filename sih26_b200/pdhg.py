@@ -97,7 +97,11 @@ class _Result(C.Structure):
 # Every symbol include/sankhya_pdhg_gpu.h declares.
 EXPORTED_SYMBOLS = ("sankhya_pdhg_gpu_default_params", "sankhya_pdhg_gpu_solve",
                     "sankhya_pdhg_gpu_last_error", "sankhya_pdhg_gpu_device_count",
-                    "sankhya_pdhg_gpu_device_name", "sankhya_pdhg_gpu_residuals_noalloc")
+                    "sankhya_pdhg_gpu_device_name", "sankhya_pdhg_gpu_residuals_noalloc",
+                    "sankhya_pdhg_server_default_config", "sankhya_pdhg_server_create",
+                    "sankhya_pdhg_server_submit", "sankhya_pdhg_server_step",
+                    "sankhya_pdhg_server_result", "sankhya_pdhg_server_free",
+                    "sankhya_pdhg_gpu_batch_solve")
 
 # SANKHYA_PDHG_NOALLOC_MAX_ROWS: rows the allocation-free residual check's fixed scratch holds
 NOALLOC_MAX_ROWS = 516064
@@ -299,3 +303,175 @@ def solve_pdhg(model: LP, options: Optional[Options] = None) -> Solution:
     if status != "model_error":
         sol.primal_infeasibility = _primal_infeasibility(model, x)
     return sol
+
+
+# ---- many LPs at once (the served / batched engine) ---------------------------------------
+
+class _ServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int32), ("memory_fraction", C.c_double),
+                ("pool_bytes", C.c_int64), ("max_active", C.c_int32),
+                ("chunk_attempts", C.c_int64), ("reserved", C.c_int32 * 8)]
+
+
+def _bind_server(lib):
+    if getattr(lib, "_server_bound", False):
+        return
+    lib.sankhya_pdhg_server_default_config.argtypes = [C.POINTER(_ServerConfig)]
+    lib.sankhya_pdhg_server_create.argtypes = [C.POINTER(_ServerConfig), C.POINTER(C.c_void_p)]
+    lib.sankhya_pdhg_server_submit.argtypes = [C.c_void_p, C.POINTER(_Problem), C.POINTER(_Params),
+                                               C.POINTER(C.c_int64)]
+    lib.sankhya_pdhg_server_step.argtypes = [C.c_void_p, C.POINTER(C.c_int32),
+                                             C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+    lib.sankhya_pdhg_server_result.argtypes = [C.c_void_p, C.c_int64, C.POINTER(_Result)]
+    lib.sankhya_pdhg_server_free.argtypes = [C.c_void_p]
+    lib.sankhya_pdhg_gpu_batch_solve.argtypes = [C.POINTER(_Problem), C.c_int32,
+                                                 C.POINTER(_Params), C.POINTER(_Result)]
+    lib._server_bound = True
+
+
+def _params(opt: Options, lib) -> _Params:
+    prm = _Params()
+    lib.sankhya_pdhg_gpu_default_params(C.byref(prm))
+    prm.tolerance = opt.get("pdhg_tolerance")
+    prm.iteration_limit = opt.get("iteration_limit")
+    prm.time_limit = opt.get("time_limit")
+    prm.restart = int(opt.get("pdhg_restart"))
+    prm.stop_at_request = int(opt.get("pdhg_stop_at_request"))
+    prm.random_seed = opt.get("random_seed")
+    prm.precision = PRECISIONS[opt.get("pdhg_precision")]
+    prm.stop_rule = STOP_RULES[opt.get("pdhg_stop_rule")]
+    prm.device = opt.get("gpu_device")
+    prm.verbose = int(opt.get("log_to_console"))
+    prm.detect_infeasibility = int(opt.get("pdhg_detect_infeasibility"))
+    prm.mixed_switch_tolerance = opt.get("pdhg_mixed_switch_tolerance")
+    prm.group_size_rows = opt.get("pdhg_lanes_rows")
+    prm.group_size_cols = opt.get("pdhg_lanes_cols")
+    prm.grid_blocks = opt.get("pdhg_grid_blocks")
+    prm.profile_kernels = int(opt.get("pdhg_profile_kernels"))
+    return prm
+
+
+class _Held:
+    """A problem struct and the contiguous arrays it points into."""
+
+    def __init__(self, model: LP):
+        self.arrays = [_arr(model.col_starts, np.int32), _arr(model.row_indices, np.int32)] + [
+            _arr(v, np.float64) for v in (model.values, model.cost, model.col_lower,
+                                          model.col_upper, model.row_lower, model.row_upper)]
+        cs, ri, vals, *vecs = self.arrays
+        self.problem = _Problem(model.num_rows, model.num_cols, int(cs[-1]) if cs.size else 0,
+                                cs.ctypes.data_as(_i32p), ri.ctypes.data_as(_i32p),
+                                vals.ctypes.data_as(_f64p),
+                                *[v.ctypes.data_as(_f64p) for v in vecs],
+                                1 if model.maximize else 0, float(model.objective_offset))
+
+
+class _Outputs:
+    def __init__(self, model: LP):
+        n, m = model.num_cols, model.num_rows
+        self.x, self.cd, self.rd, self.fk, self.ray = (np.zeros(n), np.zeros(n), np.zeros(m),
+                                                       np.zeros(m), np.zeros(n))
+        self.res = _Result()
+        self.res.col_value = self.x.ctypes.data_as(_f64p)
+        self.res.col_dual = self.cd.ctypes.data_as(_f64p)
+        self.res.row_dual = self.rd.ctypes.data_as(_f64p)
+        self.res.farkas_dual = self.fk.ctypes.data_as(_f64p)
+        self.res.primal_ray = self.ray.ctypes.data_as(_f64p)
+
+    def solution(self, model: LP) -> Solution:
+        res = self.res
+        status = SOLVE_STATUS[res.status]
+        r = res.residuals
+        sol = Solution(
+            status=status, objective=res.objective, dual_bound=res.dual_bound,
+            col_value=self.x, row_dual=self.rd, col_dual=self.cd, iterations=res.iterations,
+            solve_seconds=res.total_seconds, algorithm="pdhg-gpu-batch",
+            message=res.message.decode(errors="replace"),
+            farkas_dual=self.fk if status == "infeasible" else None,
+            attempts=res.attempts, restarts=res.restarts, evaluations=res.evaluations,
+            spectral_norm=res.spectral_norm,
+            residuals={k: getattr(r, k) for k, _ in _Residuals._fields_},
+            setup_seconds=res.setup_seconds, device_seconds=res.solve_seconds,
+            kernel_launches=res.kernel_launches)
+        if status not in ("model_error", "infeasible"):
+            sol.primal_infeasibility = _primal_infeasibility(model, self.x)
+        return sol
+
+
+def batch_solve(models, options: Optional[Options] = None):
+    """Solves independent LPs concurrently on one GPU (sankhya_pdhg_gpu_batch_solve)."""
+    opt = options or Options()
+    lib = load_library()
+    _bind_server(lib)
+    held = [_Held(m) for m in models]
+    outs = [_Outputs(m) for m in models]
+    probs = (_Problem * len(models))(*[h.problem for h in held])
+    results = (_Result * len(models))(*[o.res for o in outs])
+    prm = _params(opt, lib)
+    code = lib.sankhya_pdhg_gpu_batch_solve(probs, len(models), C.byref(prm), results)
+    if code != 0:
+        raise GpuError(code, lib.sankhya_pdhg_gpu_last_error().decode())
+    sols = []
+    for k, m in enumerate(models):
+        outs[k].res = results[k]
+        sols.append(outs[k].solution(m))
+    return sols
+
+
+class Server:
+    """A resident GPU server for many LPs (sankhya_pdhg_server_*): submit() queues an LP,
+    step() admits what fits and runs one launch over every active LP, result() collects."""
+
+    def __init__(self, device: int = 0, memory_fraction: float = 0.8, pool_bytes: int = 0,
+                 max_active: int = 4096, chunk_attempts: int = 2048):
+        self.lib = load_library()
+        _bind_server(self.lib)
+        cfg = _ServerConfig()
+        self.lib.sankhya_pdhg_server_default_config(C.byref(cfg))
+        cfg.device, cfg.memory_fraction, cfg.pool_bytes = device, memory_fraction, pool_bytes
+        cfg.max_active, cfg.chunk_attempts = max_active, chunk_attempts
+        self.handle = C.c_void_p()
+        code = self.lib.sankhya_pdhg_server_create(C.byref(cfg), C.byref(self.handle))
+        if code != 0:
+            raise GpuError(code, self.lib.sankhya_pdhg_gpu_last_error().decode())
+        self.pending = {}
+
+    def submit(self, model: LP, options: Optional[Options] = None) -> int:
+        held = _Held(model)
+        prm = _params(options or Options(), self.lib)
+        ticket = C.c_int64()
+        code = self.lib.sankhya_pdhg_server_submit(self.handle, C.byref(held.problem),
+                                                   C.byref(prm), C.byref(ticket))
+        if code != 0:
+            raise GpuError(code, self.lib.sankhya_pdhg_gpu_last_error().decode())
+        self.pending[ticket.value] = model
+        return ticket.value
+
+    def step(self):
+        a, w, f = C.c_int32(), C.c_int32(), C.c_int32()
+        code = self.lib.sankhya_pdhg_server_step(self.handle, C.byref(a), C.byref(w), C.byref(f))
+        if code != 0:
+            raise GpuError(code, self.lib.sankhya_pdhg_gpu_last_error().decode())
+        return a.value, w.value, f.value
+
+    def result(self, ticket: int) -> Optional[Solution]:
+        model = self.pending[ticket]
+        out = _Outputs(model)
+        code = self.lib.sankhya_pdhg_server_result(self.handle, ticket, C.byref(out.res))
+        if code == 12:
+            return None
+        if code != 0:
+            raise GpuError(code, self.lib.sankhya_pdhg_gpu_last_error().decode())
+        del self.pending[ticket]
+        return out.solution(model)
+
+    def close(self):
+        if self.handle:
+            self.lib.sankhya_pdhg_server_free(self.handle)
+            self.handle = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
