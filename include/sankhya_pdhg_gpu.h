@@ -228,7 +228,10 @@ typedef struct sankhya_pdhg_server_config {
   int64_t pool_bytes;      /* explicit pool size; 0 = use memory_fraction */
   int32_t max_active;      /* LP slots (default 4096) */
   int64_t chunk_attempts;  /* attempts per LP per step; 0 = run each LP to its end */
-  int32_t reserved[8];
+  int64_t cluster_min_nnz; /* LPs with at least this many nonzeros run on an 8-block thread
+                              block cluster instead of one block (default 16384; 0 = never) */
+  int32_t clusters;        /* clusters kept for those LPs (default 16) */
+  int32_t reserved[7];
 } sankhya_pdhg_server_config;
 
 void sankhya_pdhg_server_default_config(sankhya_pdhg_server_config* config);

@@ -1,15 +1,18 @@
 // Batched restarted PDHG: many independent LPs in one persistent launch.
 //
-// Each block takes LPs from a device work queue (largest first) and runs the whole
-// restarted PDHG of src/pdhg/pdhg.cpp:267-726 on one LP with block-level barriers only: the
-// norm estimate, the attempts (phase P, phase D, step control), the evaluations every 40
-// accepted iterations with per-LP restarts and termination, and the final report. An LP
-// runs for at most `chunk_attempts` attempts per launch and keeps its state in device
-// memory between launches, so a host loop can admit and retire LPs between launches.
+// A group of thread blocks -- one block, or a thread-block cluster for the larger LPs --
+// takes LPs from a device work queue (largest first) and runs the whole restarted PDHG of
+// src/pdhg/pdhg.cpp:267-726 on one LP: the norm estimate, the attempts (phase P, phase D,
+// step control), the evaluations every 40 accepted iterations with per-LP restarts and
+// termination, and the final report. Phase barriers are __syncthreads for a single block
+// and the hardware cluster barrier for a cluster; cluster reductions combine the blocks'
+// totals through distributed shared memory in rank order. An LP runs for at most
+// `chunk_attempts` attempts per launch and keeps its state in device memory between
+// launches, so a host loop can admit and retire LPs between launches.
 //
-// Per-LP state and work partitions are those of the single-LP kernels with one block
-// (G = 1), so the row sums follow the same code and summation order whatever the batch
-// around an LP: a result is the same alone and in the mix.
+// An LP's work partition is built for its group size alone, so its row sums follow the same
+// code and summation order whatever else is in the batch: a result is the same alone and in
+// the mix.
 //
 // Primal infeasibility: at every evaluation the dual movement since the last restart,
 // f = -Dr (y - y_r) in original units, is tested as a Farkas certificate in the sense of
@@ -19,17 +22,84 @@
 // the host re-checks every certificate exactly before reporting it.
 #pragma once
 
+#include <cooperative_groups.h>
+
 #include "pdhg_kernels.cuh"
 
 namespace sih26 {
 
+namespace cg = cooperative_groups;
+
+constexpr int kClusterSize = 8;
+constexpr int kGroupSlots = 16;
+
 struct BatchSlot {
-  Prob<double> P;       // single-block partitions
+  Prob<double> P;       // partitions built for the LP's group size
   State<double> S;      // partials and barrier unused
   double* x_out;        // report: unscaled x, permuted
   double* red_out;      // report: min-space reduced costs, permuted
   double* y_out;        // report: unscaled y (PDHG sign), permuted
   double* farkas_out;   // certificate f (reference sign, normalised), permuted
+};
+
+// One block.
+struct BlockGroup {
+  static constexpr int kSize = 1;
+  double* red;  // unused
+  double* tmp;  // unused
+  __device__ __forceinline__ int rank() const { return 0; }
+  __device__ __forceinline__ void sync() const { __syncthreads(); }
+  template <int NS, unsigned MAXMASK>
+  __device__ __forceinline__ void reduce(double (&v)[NS], double* sh) const {
+    block_reduce<NS, MAXMASK>(v, sh);
+  }
+  // rank 0's value of a per-block flag, in every block
+  __device__ __forceinline__ int agree(int* shared_flag) const {
+    __syncthreads();
+    return *shared_flag;
+  }
+};
+
+// A cluster of CS blocks. red[kGroupSlots] and tmp[CS * kGroupSlots] are shared arrays.
+template <int CS>
+struct ClusterGroup {
+  static constexpr int kSize = CS;
+  double* red;
+  double* tmp;
+  __device__ __forceinline__ int rank() const { return (int)cg::this_cluster().block_rank(); }
+  __device__ __forceinline__ void sync() const { cg::this_cluster().sync(); }
+  template <int NS, unsigned MAXMASK>
+  __device__ __forceinline__ void reduce(double (&v)[NS], double* sh) const {
+    block_reduce<NS, MAXMASK>(v, sh);
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int s = 0; s < NS; ++s) red[s] = v[s];
+    }
+    cg::cluster_group cl = cg::this_cluster();
+    cl.sync();
+    if (threadIdx.x < CS * NS) {
+      const int r = threadIdx.x / NS, s = threadIdx.x - r * NS;
+      tmp[threadIdx.x] = cl.map_shared_rank(red, r)[s];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      double t = tmp[s];
+      for (int r = 1; r < CS; ++r) {
+        const double o = tmp[r * NS + s];
+        t = ((MAXMASK >> s) & 1u) ? dmax(t, o) : t + o;
+      }
+      v[s] = t;
+    }
+    cl.sync();  // red and tmp are free again
+  }
+  __device__ __forceinline__ int agree(int* shared_flag) const {
+    cg::cluster_group cl = cg::this_cluster();
+    cl.sync();
+    const int v = *cl.map_shared_rank(shared_flag, 0);
+    cl.sync();
+    return v;
+  }
 };
 
 // sum_k A'_jk (y - y_r)_k, the column side of the Farkas candidate
@@ -68,47 +138,53 @@ struct FarkasCol {
   }
 };
 
-// Norm estimate of the LP's scaled matrix (src/la/scaling.cpp:161-194) with one block:
+// Norm estimate of the LP's scaled matrix (src/la/scaling.cpp:161-194):
 // v = S.xavg holds the random start, u = S.yavg is scratch.
-__device__ __noinline__ double block_power(const Prob<double>& P, const State<double>& S, int nnz,
-                                     double* sh, double* stream) {
+template <class Grp>
+__device__ __noinline__ double group_power(const Prob<double>& P, const State<double>& S, int nnz,
+                                           double* sh, double* stream, Grp grp) {
   if (P.m == 0 || P.n == 0 || nnz == 0) return 1.0;
+  const int rank = grp.rank();
+  const int base = rank * kThreads + threadIdx.x, stride = Grp::kSize * kThreads;
   double len2[1] = {0.0};
-  for (int j = threadIdx.x; j < P.n; j += kThreads) {
+  for (int j = base; j < P.n; j += stride) {
     const double t = S.xavg[j];
     len2[0] += t * t;
   }
-  block_reduce<1, 0u>(len2, sh);
+  grp.template reduce<1, 0u>(len2, sh);
   for (int step = 0; step < 30; ++step) {
     const double length = sqrt(len2[0]);
     if (length == 0.0) return 1.0;
     double dummy[1] = {0.0};
     run_phase<1, 1>(P.A.ptr, P.A.idx, P.A.val64, P.pa, ScaledGather{S.xavg, 1.0 / length},
-                    StoreRow<1>{S.yavg, -1}, dummy, stream, 0);
-    __syncthreads();
+                    StoreRow<1>{S.yavg, -1}, dummy, stream, rank);
+    grp.sync();
     double nx[1] = {0.0};
     run_phase<1, 1>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pat, ScaledGather{S.yavg, 1.0},
-                    StoreRow<1>{S.xavg, 0}, nx, stream, 0);
-    block_reduce<1, 0u>(nx, sh);
+                    StoreRow<1>{S.xavg, 0}, nx, stream, rank);
+    grp.template reduce<1, 0u>(nx, sh);
     len2[0] = nx[0];
   }
   const double norm = sqrt(sqrt(len2[0]));
   return norm > 0.0 ? norm * 1.01 : 1.0;
 }
 
-// One evaluation of one LP (pdhg.cpp:502-643) with block-level reductions, plus the Farkas
-// candidate test. Leaves c.state at kRunning, kConverged or kInfeasible.
-__device__ __noinline__ void block_evaluate(const BatchSlot& B, Ctrl& c, double* sh, double* stream,
-                                      int* flags) {
+// One evaluation of one LP (pdhg.cpp:502-643) plus the Farkas candidate test. Leaves
+// c.state at kRunning, kConverged or kInfeasible.
+template <class Grp>
+__device__ __noinline__ void group_evaluate(const BatchSlot& B, Ctrl& c, double* sh,
+                                            double* stream, int* flags, Grp grp) {
   const Prob<double>& P = B.P;
   const State<double>& S = B.S;
+  const int rank = grp.rank();
+  const int base = rank * kThreads + threadIdx.x, stride = Grp::kSize * kThreads;
   const int cur = c.cur;
   const bool has_average = c.averaged > 0;
   const double count = (double)c.averaged;
   // E1 + Farkas rows. slots: 0 |x-x_r|^2, 1 |y-y_r|^2, 2 S, 3 max|f|, 4 max|f| leaning on a
   // missing row bound
   double e1[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-  for (int j = threadIdx.x; j < P.n; j += kThreads) {
+  for (int j = base; j < P.n; j += stride) {
     const double xo = ld(S.x[cur] + j);
     const double xs = S.xsum[j] + (c.pending ? xo : 0.0);
     S.xsum[j] = xs;
@@ -116,7 +192,7 @@ __device__ __noinline__ void block_evaluate(const BatchSlot& B, Ctrl& c, double*
     const double d = xo - ld(S.xr + j);
     e1[0] += d * d;
   }
-  for (int i = threadIdx.x; i < P.m; i += kThreads) {
+  for (int i = base; i < P.m; i += stride) {
     const double yo = ld(S.y[cur] + i);
     const double ys = S.ysum[i] + (c.pending ? yo : 0.0);
     S.ysum[i] = ys;
@@ -132,26 +208,27 @@ __device__ __noinline__ void block_evaluate(const BatchSlot& B, Ctrl& c, double*
       if (finite_bound(hi)) e1[2] += f * hi; else e1[4] = dmax(e1[4], -f);
     }
   }
-  block_reduce<5, (1u << 3) | (1u << 4)>(e1, sh);
+  grp.template reduce<5, (1u << 3) | (1u << 4)>(e1, sh);
   // E2: residual terms of both candidates (FP64 values)
   double acc[kEvalSlots];
 #pragma unroll
   for (int s = 0; s < kEvalSlots; ++s) acc[s] = 0.0;
   RowEval<double, 2> re{P.dr, P.rl0, P.ru0, S.y[cur], S.yavg, nullptr, nullptr};
   run_phase<2, kEvalSlots>(P.A.ptr, P.A.idx, P.A.val64, P.pa,
-                           Gather2<double, double>{S.x[cur], S.xavg}, re, acc, stream, 0);
+                           Gather2<double, double>{S.x[cur], S.xavg}, re, acc, stream, rank);
   ColEval<double, 2> ce{P.dc, P.cl0, P.cu0, P.c0, S.x[cur], S.xavg, nullptr, nullptr, nullptr};
   run_phase<2, kEvalSlots>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pat,
-                           Gather2<double, double>{S.y[cur], S.yavg}, ce, acc, stream, 0);
-  block_reduce<kEvalSlots, kEvalMaxMask>(acc, sh);
+                           Gather2<double, double>{S.y[cur], S.yavg}, ce, acc, stream, rank);
+  grp.template reduce<kEvalSlots, kEvalMaxMask>(acc, sh);
   // Farkas columns
   double fk[3] = {0.0, 0.0, 0.0};
   const bool test_farkas = c.farkas_cooldown == 0 && e1[3] > 0.0;
   if (test_farkas) {
     run_phase<1, 3>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pat, DiffGather{S.y[cur], S.yr},
-                    FarkasCol{P.dc, P.cl0, P.cu0}, fk, stream, 0);
-    block_reduce<3, (1u << 0) | (1u << 2)>(fk, sh);
+                    FarkasCol{P.dc, P.cl0, P.cu0}, fk, stream, rank);
+    grp.template reduce<3, (1u << 0) | (1u << 2)>(fk, sh);
   }
+  // every block takes the same decisions from the same totals
   if (threadIdx.x == 0) {
     const double mv[2] = {e1[0], e1[1]};
     evaluation_decision(c, acc, mv, has_average, flags);
@@ -171,10 +248,10 @@ __device__ __noinline__ void block_evaluate(const BatchSlot& B, Ctrl& c, double*
     }
   }
   __syncthreads();
-  const double fmax = e1[3];  // block_reduce left the totals in every thread
+  const double fmax = e1[3];
   // E3: certificate, best point, restart reset
   if (flags[0] || flags[1] || flags[3]) {
-    for (int j = threadIdx.x; j < P.n; j += kThreads) {
+    for (int j = base; j < P.n; j += stride) {
       const double xo = ld(S.x[cur] + j);
       if (flags[0]) S.best_x[j] = flags[2] ? S.xavg[j] : xo;
       if (flags[1]) {
@@ -182,7 +259,7 @@ __device__ __noinline__ void block_evaluate(const BatchSlot& B, Ctrl& c, double*
         S.xsum[j] = 0.0;
       }
     }
-    for (int i = threadIdx.x; i < P.m; i += kThreads) {
+    for (int i = base; i < P.m; i += stride) {
       const double yo = ld(S.y[cur] + i);
       if (flags[3]) B.farkas_out[i] = -__ldg(P.dr + i) * (yo - ld(S.yr + i)) / fmax;
       if (flags[0]) S.best_y[i] = flags[2] ? S.yavg[i] : yo;
@@ -192,37 +269,42 @@ __device__ __noinline__ void block_evaluate(const BatchSlot& B, Ctrl& c, double*
       }
     }
   }
-  __syncthreads();
+  grp.sync();
 }
 
 // Report of one finished LP (pdhg.cpp:647-661): unscaled point, reduced costs, multipliers
 // and the residual block of the best point into c.best.
-__device__ __noinline__ void block_report(const BatchSlot& B, Ctrl& c, double* sh, double* stream) {
+template <class Grp>
+__device__ __noinline__ void group_report(const BatchSlot& B, Ctrl& c, double* sh, double* stream,
+                                          Grp grp) {
   const Prob<double>& P = B.P;
   const State<double>& S = B.S;
+  const int rank = grp.rank();
   double acc[kEvalSlots];
 #pragma unroll
   for (int s = 0; s < kEvalSlots; ++s) acc[s] = 0.0;
   RowEval<double, 1> re{P.dr, P.rl0, P.ru0, nullptr, nullptr, S.best_y, B.y_out};
   run_phase<1, kEvalSlots>(P.A.ptr, P.A.idx, P.A.val64, P.pa, Gather1<double>{S.best_x}, re, acc,
-                           stream, 0);
+                           stream, rank);
   ColEval<double, 1> ce{P.dc, P.cl0, P.cu0, P.c0, nullptr, nullptr, S.best_x, B.x_out, B.red_out};
   run_phase<1, kEvalSlots>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pat, Gather1<double>{S.best_y}, ce,
-                           acc, stream, 0);
-  block_reduce<kEvalSlots, kEvalMaxMask>(acc, sh);
+                           acc, stream, rank);
+  grp.template reduce<kEvalSlots, kEvalMaxMask>(acc, sh);
   if (threadIdx.x == 0) c.best = make_residuals(acc, 0, c.bound_norm, c.cost_norm);
   __syncthreads();
 }
 
+template <class Grp>
 __device__ inline void run_instance(const BatchSlot& B, Ctrl& c, double* sh, double* stream,
-                                    int* flags, long long chunk_attempts) {
+                                    int* flags, long long chunk_attempts, Grp grp) {
   const Prob<double>& P = B.P;
   const State<double>& S = B.S;
+  const int rank = grp.rank();
   if (threadIdx.x == 0) c = *S.ctrl;
   __syncthreads();
   if (c.state == kSetup) {
     const int nnz = __ldg(P.A.ptr + P.m);
-    const double norm = block_power(P, S, nnz, sh, stream);
+    const double norm = group_power(P, S, nnz, sh, stream, grp);
     if (threadIdx.x == 0) {
       c.spectral_norm = norm;
       c.eta = norm > 0.0 ? 1.0 / norm : 1.0;
@@ -231,20 +313,25 @@ __device__ inline void run_instance(const BatchSlot& B, Ctrl& c, double* sh, dou
     }
     double dummy[1] = {0.0};
     run_phase<1, 1>(P.A.ptr, P.A.idx, P.A.val, P.pa, Gather1<double>{S.x[0]},
-                    StoreRow<1>{S.ax[0], -1}, dummy, stream, 0);
-    __syncthreads();
+                    StoreRow<1>{S.ax[0], -1}, dummy, stream, rank);
+    grp.sync();
   }
   long long a = 0;
   while (c.state == kRunning) {
+    // loop top (pdhg.cpp:384-385); the deadline is read by rank 0 and agreed on
+    const bool check_clock = c.deadline_ns != 0ull && (a & 63) == 0;
     if (threadIdx.x == 0) {
       flags[5] = 0;
+      flags[6] = (check_clock && global_ns() > c.deadline_ns) ? 1 : 0;
       if (c.iteration >= c.iteration_limit) {
         c.state = kIterationLimit;
-      } else if (c.deadline_ns != 0ull && global_ns() > c.deadline_ns) {
-        c.state = kTimeLimit;
       } else if (a >= chunk_attempts) {
         flags[5] = 1;
       }
+    }
+    if (check_clock) {
+      const int late = grp.agree(&flags[6]);
+      if (late && threadIdx.x == 0 && c.state == kRunning) c.state = kTimeLimit;
     }
     __syncthreads();
     if (c.state != kRunning || flags[5]) break;
@@ -256,30 +343,30 @@ __device__ inline void run_instance(const BatchSlot& B, Ctrl& c, double* sh, dou
     {
       PrimalStep<double> ps{S.x[cur], S.x[nxt], P.c, P.cl, P.cu, S.xsum, tau, c.pending};
       run_phase<1, 3>(P.AT.ptr, P.AT.idx, P.AT.val, P.pat, Gather1<double>{S.y[cur]}, ps, acc,
-                      stream, 0);
+                      stream, rank);
     }
-    __syncthreads();
+    grp.sync();
     {
       DualStep<double> ds{S.y[cur], S.y[nxt], S.ax[cur], S.ax[nxt], P.rl, P.ru, S.ysum, sigma,
                           c.pending};
       run_phase<1, 3>(P.A.ptr, P.A.idx, P.A.val, P.pa, Gather1<double>{S.x[nxt]}, ds, acc,
-                      stream, 0);
+                      stream, rank);
     }
-    block_reduce<3, 0u>(acc, sh);
+    grp.template reduce<3, 0u>(acc, sh);
     if (threadIdx.x == 0) step_control(c, acc);
     __syncthreads();
-    if (c.state == kNeedEval) block_evaluate(B, c, sh, stream, flags);
+    if (c.state == kNeedEval) group_evaluate(B, c, sh, stream, flags, grp);
   }
   if (c.state == kConverged || c.state == kIterationLimit || c.state == kTimeLimit ||
       c.state == kInfeasible) {
-    block_report(B, c, sh, stream);
+    group_report(B, c, sh, stream, grp);
   }
-  if (threadIdx.x == 0) *S.ctrl = c;
-  __syncthreads();
+  if (threadIdx.x == 0 && rank == 0) *S.ctrl = c;
+  grp.sync();
 }
 
-// The persistent batch kernel: blocks take LPs from the active list through a device
-// counter (the list is ordered largest first) until it is exhausted.
+// The persistent batch kernels: blocks (or clusters) take LPs from the active list through a
+// device counter (the list is ordered largest first) until it is exhausted.
 __global__ void __launch_bounds__(kThreads, 2) batch_kernel(const BatchSlot* slots,
                                                             const int* active,
                                                             const int* active_count,
@@ -297,7 +384,31 @@ __global__ void __launch_bounds__(kThreads, 2) batch_kernel(const BatchSlot* slo
     const int q = s_take;
     __syncthreads();
     if (q >= count) break;
-    run_instance(slots[active[q]], c, sh, stream, flags, chunk_attempts);
+    run_instance(slots[active[q]], c, sh, stream, flags, chunk_attempts,
+                 BlockGroup{nullptr, nullptr});
+  }
+}
+
+__global__ void __cluster_dims__(kClusterSize, 1, 1) __launch_bounds__(kThreads, 2)
+    cluster_batch_kernel(const BatchSlot* slots, const int* active, const int* active_count,
+                         int* queue_head, long long chunk_attempts) {
+  __shared__ Ctrl c;
+  __shared__ double sh[kWarps * kEvalSlots];
+  __shared__ double red[kGroupSlots];
+  __shared__ double tmp[kClusterSize * kGroupSlots];
+  __shared__ int flags[8];
+  __shared__ int s_take;
+  double* stream = warp_stream();
+  const ClusterGroup<kClusterSize> grp{red, tmp};
+  cg::cluster_group cl = cg::this_cluster();
+  const int count = *active_count;
+  for (;;) {
+    if (cl.block_rank() == 0 && threadIdx.x == 0) s_take = atomicAdd(queue_head, 1);
+    cl.sync();
+    const int q = *cl.map_shared_rank(&s_take, 0);
+    cl.sync();
+    if (q >= count) break;
+    run_instance(slots[active[q]], c, sh, stream, flags, chunk_attempts, grp);
   }
 }
 

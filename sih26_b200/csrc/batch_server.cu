@@ -3,9 +3,11 @@
 //
 // A server owns one device memory pool (a fraction of free HBM, taken once at creation),
 // a table of LP slots and one CUDA graph. submit() prepares an LP on the host (validation,
-// scaling, permutation, single-block work partition) into one contiguous device image;
-// step() admits waiting LPs whose image fits the pool, replays the graph (one launch of the
-// persistent batch kernel over every active LP, each for at most chunk_attempts attempts),
+// scaling, permutation, work partition for one block -- or for an 8-block cluster when the
+// LP has at least cluster_min_nnz nonzeros) into one contiguous device image; step() admits
+// waiting LPs whose image fits the pool, replays the graph (the single-block and the cluster
+// persistent kernels side by side on two forked streams, over every active LP of their
+// class, each LP for at most chunk_attempts attempts),
 // reads the compact control blocks back, re-checks every Farkas certificate on the host, and
 // retires finished LPs with their answers. LPs admitted while others run simply join the
 // next launch: that is continuous batching.
@@ -120,6 +122,7 @@ struct Job {
   } off{};
   Ctrl ctrl0{};
   // lifecycle
+  int group = 1;  // blocks working on this LP: 1, or kClusterSize
   int slot = -1;
   size_t pool_offset = 0;
   size_t pool_bytes = 0;
@@ -146,7 +149,8 @@ std::vector<T> gathered(const std::vector<T>& v, const std::vector<int>& perm) {
 }
 
 // Host preparation of one LP (the setup half of the single-LP solve, with G = 1).
-void prepare(Job& J, const sankhya_pdhg_problem& p, const sankhya_pdhg_params& prm) {
+void prepare(Job& J, const sankhya_pdhg_problem& p, const sankhya_pdhg_params& prm,
+             long long cluster_min_nnz) {
   check_structure(p);
   const int m = p.num_rows, n = p.num_cols;
   J.m = m;
@@ -184,8 +188,9 @@ void prepare(Job& J, const sankhya_pdhg_problem& p, const sankhya_pdhg_params& p
   }
   const Scaling sc = build_scaling(J.view, cmin, 10);
   const PermutedLp q = permute(J.view, sc.values);
-  const HostPart pa = partition(q.a_ptr, 1, kWarps, prm.group_size_rows);
-  const HostPart pat = partition(q.at_ptr, 1, kWarps, prm.group_size_cols);
+  J.group = (cluster_min_nnz > 0 && q.nnz >= cluster_min_nnz) ? kClusterSize : 1;
+  const HostPart pa = partition(q.a_ptr, J.group, kWarps, prm.group_size_rows);
+  const HostPart pat = partition(q.at_ptr, J.group, kWarps, prm.group_size_cols);
   J.row_perm = q.row_perm;
   J.col_perm = q.col_perm;
 
@@ -330,15 +335,21 @@ struct Server {
   BatchSlot* d_slots = nullptr;
   Ctrl* d_ctrls = nullptr;
   Ctrl* d_compact = nullptr;
-  int* d_active = nullptr;
-  int* d_count = nullptr;
-  int* d_head = nullptr;
+  // per class (0: one block per LP, 1: a cluster per LP): active list, count, queue head
+  int* d_active[2] = {nullptr, nullptr};
+  int* d_count[2] = {nullptr, nullptr};
+  int* d_head[2] = {nullptr, nullptr};
+  Ctrl* d_compact2 = nullptr;
   Ctrl* h_compact = nullptr;
+  Ctrl* h_compact2 = nullptr;
   int* h_active = nullptr;
+  int* h_active2 = nullptr;
+  int* h_counts = nullptr;
   cudaGraphExec_t graph = nullptr;
   std::vector<int> free_slots;
   std::vector<std::shared_ptr<Job>> slot_job;
   std::vector<int> active;  // slot indices, largest LP first
+  std::vector<int> active_big;  // the same for the cluster class
   std::deque<std::shared_ptr<Job>> waiting;
   std::map<int64_t, std::shared_ptr<Job>> jobs;
   int64_t next_ticket = 1;
@@ -408,27 +419,63 @@ BatchSlot relocate(const Job& J, unsigned char* base, Ctrl* ctrl) {
 }
 
 void build_graph(Server& s) {
-  cudaStream_t cap;
+  cudaStream_t cap, side;
   SIH26_SCUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), SANKHYA_GPU_INIT_FAILED);
+  SIH26_SCUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking), SANKHYA_GPU_INIT_FAILED);
+  cudaEvent_t fork, join;
+  SIH26_SCUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), SANKHYA_GPU_INIT_FAILED);
+  SIH26_SCUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming), SANKHYA_GPU_INIT_FAILED);
   int bpsm = 0;
   SIH26_SCUDA(cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)stream_smem_bytes()), SANKHYA_GPU_INIT_FAILED);
+  SIH26_SCUDA(cudaFuncSetAttribute(cluster_batch_kernel,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)stream_smem_bytes()), SANKHYA_GPU_INIT_FAILED);
   SIH26_SCUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, batch_kernel, kThreads,
                                                             stream_smem_bytes()),
               SANKHYA_GPU_INIT_FAILED);
   cudaDeviceProp props{};
   SIH26_SCUDA(cudaGetDeviceProperties(&props, s.cfg.device), SANKHYA_GPU_INIT_FAILED);
-  const int grid = props.multiProcessorCount * std::max(1, std::min(bpsm, 2));
+  const int slots_total = props.multiProcessorCount * std::max(1, std::min(bpsm, 2));
+  // clusters that fit at once
+  cudaLaunchConfig_t lc{};
+  lc.gridDim = dim3(kClusterSize);
+  lc.blockDim = dim3(kThreads);
+  lc.dynamicSmemBytes = stream_smem_bytes();
+  cudaLaunchAttribute attr{};
+  attr.id = cudaLaunchAttributeClusterDimension;
+  attr.val.clusterDim.x = kClusterSize;
+  attr.val.clusterDim.y = 1;
+  attr.val.clusterDim.z = 1;
+  lc.attrs = &attr;
+  lc.numAttrs = 1;
+  int max_clusters = 0;
+  SIH26_SCUDA(cudaOccupancyMaxActiveClusters(&max_clusters, cluster_batch_kernel, &lc),
+              SANKHYA_GPU_INIT_FAILED);
+  const int want = s.cfg.clusters > 0 ? s.cfg.clusters : 16;  // clusters for big LPs
+  const int clusters = std::max(1, std::min(want, max_clusters / 2 > 0 ? max_clusters / 2 : 1));
+  const int small_grid = std::max(1, slots_total - clusters * kClusterSize);
   const long long chunk = s.cfg.chunk_attempts > 0 ? s.cfg.chunk_attempts : (1ll << 40);
   cudaGraph_t g;
   SIH26_SCUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal), SANKHYA_GPU_INIT_FAILED);
-  cudaMemsetAsync(s.d_head, 0, sizeof(int), cap);
-  batch_kernel<<<grid, kThreads, stream_smem_bytes(), cap>>>(s.d_slots, s.d_active, s.d_count,
-                                                              s.d_head, chunk);
-  gather_ctrl_kernel<<<128, 128, 0, cap>>>(s.d_ctrls, s.d_active, s.d_count, s.d_compact);
+  cudaMemsetAsync(s.d_head[0], 0, sizeof(int), cap);
+  cudaMemsetAsync(s.d_head[1], 0, sizeof(int), cap);
+  cudaEventRecord(fork, cap);
+  cudaStreamWaitEvent(side, fork, 0);
+  cluster_batch_kernel<<<clusters * kClusterSize, kThreads, stream_smem_bytes(), side>>>(
+      s.d_slots, s.d_active[1], s.d_count[1], s.d_head[1], chunk);
+  gather_ctrl_kernel<<<64, 128, 0, side>>>(s.d_ctrls, s.d_active[1], s.d_count[1], s.d_compact2);
+  batch_kernel<<<small_grid, kThreads, stream_smem_bytes(), cap>>>(s.d_slots, s.d_active[0],
+                                                                   s.d_count[0], s.d_head[0], chunk);
+  gather_ctrl_kernel<<<128, 128, 0, cap>>>(s.d_ctrls, s.d_active[0], s.d_count[0], s.d_compact);
+  cudaEventRecord(join, side);
+  cudaStreamWaitEvent(cap, join, 0);
   SIH26_SCUDA(cudaStreamEndCapture(cap, &g), SANKHYA_GPU_INIT_FAILED);
   SIH26_SCUDA(cudaGraphInstantiate(&s.graph, g, 0), SANKHYA_GPU_INIT_FAILED);
   cudaGraphDestroy(g);
+  cudaEventDestroy(fork);
+  cudaEventDestroy(join);
+  cudaStreamDestroy(side);
   cudaStreamDestroy(cap);
 }
 
@@ -515,34 +562,25 @@ static void admit(Server& s) {
     J->image.clear();
     J->image.shrink_to_fit();
     s.slot_job[slot] = J;
-    s.active.push_back(slot);
+    (J->group > 1 ? s.active_big : s.active).push_back(slot);
     changed = true;
   }
   if (changed) {
-    std::stable_sort(s.active.begin(), s.active.end(), [&](int a, int b) {
-      return s.slot_job[a]->nnz > s.slot_job[b]->nnz;
-    });
+    const auto larger = [&](int a, int b) { return s.slot_job[a]->nnz > s.slot_job[b]->nnz; };
+    std::stable_sort(s.active.begin(), s.active.end(), larger);
+    std::stable_sort(s.active_big.begin(), s.active_big.end(), larger);
   }
 }
 
-static void run_round(Server& s) {
-  const int count = static_cast<int>(s.active.size());
-  if (count == 0) return;
-  std::memcpy(s.h_active, s.active.data(), count * sizeof(int));
-  SIH26_SCUDA(cudaMemcpyAsync(s.d_active, s.h_active, count * sizeof(int), cudaMemcpyHostToDevice,
-                              s.stream), SANKHYA_GPU_COPY_FAILED);
-  SIH26_SCUDA(cudaMemcpyAsync(s.d_count, &count, sizeof(int), cudaMemcpyHostToDevice, s.stream),
-              SANKHYA_GPU_COPY_FAILED);
-  SIH26_SCUDA(cudaGraphLaunch(s.graph, s.stream), SANKHYA_GPU_KERNEL_LAUNCH_FAILED);
-  ++s.launches;
-  SIH26_SCUDA(cudaMemcpyAsync(s.h_compact, s.d_compact, count * sizeof(Ctrl),
-                              cudaMemcpyDeviceToHost, s.stream), SANKHYA_GPU_COPY_FAILED);
-  SIH26_SCUDA(cudaStreamSynchronize(s.stream), SANKHYA_GPU_SYNC_FAILED);
+// Handles the LPs of one class whose control blocks came back in `compact`; returns those
+// still running.
+static std::vector<int> settle(Server& s, const std::vector<int>& list, const Ctrl* compact) {
   std::vector<int> still;
-  for (int q = 0; q < count; ++q) {
-    const int slot = s.active[q];
-    const Ctrl& c = s.h_compact[q];
+  for (size_t q = 0; q < list.size(); ++q) {
+    const int slot = list[q];
+    const Ctrl& c = compact[q];
     Job& J = *s.slot_job[slot];
+    if (c.state == kDeviceError) throw Failure{SANKHYA_GPU_DEVICE_TIMEOUT, "batch kernel error"};
     bool done = c.state == kConverged || c.state == kIterationLimit || c.state == kTimeLimit;
     if (c.state == kInfeasible) {
       std::vector<double> f(J.m);
@@ -563,7 +601,6 @@ static void run_round(Server& s) {
                     SANKHYA_GPU_COPY_FAILED);
       }
     }
-    if (c.state == kDeviceError) throw Failure{SANKHYA_GPU_DEVICE_TIMEOUT, "batch kernel error"};
     if (done) {
       finish_job(s, J, c);
       s.alloc->release(J.pool_offset, J.pool_bytes);
@@ -573,7 +610,37 @@ static void run_round(Server& s) {
       still.push_back(slot);
     }
   }
-  s.active.swap(still);
+  return still;
+}
+
+static void run_round(Server& s) {
+  const int c0 = static_cast<int>(s.active.size()), c1 = static_cast<int>(s.active_big.size());
+  if (c0 + c1 == 0) return;
+  std::memcpy(s.h_active, s.active.data(), c0 * sizeof(int));
+  std::memcpy(s.h_active2, s.active_big.data(), c1 * sizeof(int));
+  s.h_counts[0] = c0;
+  s.h_counts[1] = c1;
+  if (c0)
+    SIH26_SCUDA(cudaMemcpyAsync(s.d_active[0], s.h_active, c0 * sizeof(int),
+                                cudaMemcpyHostToDevice, s.stream), SANKHYA_GPU_COPY_FAILED);
+  if (c1)
+    SIH26_SCUDA(cudaMemcpyAsync(s.d_active[1], s.h_active2, c1 * sizeof(int),
+                                cudaMemcpyHostToDevice, s.stream), SANKHYA_GPU_COPY_FAILED);
+  SIH26_SCUDA(cudaMemcpyAsync(s.d_count[0], &s.h_counts[0], sizeof(int), cudaMemcpyHostToDevice,
+                              s.stream), SANKHYA_GPU_COPY_FAILED);
+  SIH26_SCUDA(cudaMemcpyAsync(s.d_count[1], &s.h_counts[1], sizeof(int), cudaMemcpyHostToDevice,
+                              s.stream), SANKHYA_GPU_COPY_FAILED);
+  SIH26_SCUDA(cudaGraphLaunch(s.graph, s.stream), SANKHYA_GPU_KERNEL_LAUNCH_FAILED);
+  ++s.launches;
+  if (c0)
+    SIH26_SCUDA(cudaMemcpyAsync(s.h_compact, s.d_compact, c0 * sizeof(Ctrl),
+                                cudaMemcpyDeviceToHost, s.stream), SANKHYA_GPU_COPY_FAILED);
+  if (c1)
+    SIH26_SCUDA(cudaMemcpyAsync(s.h_compact2, s.d_compact2, c1 * sizeof(Ctrl),
+                                cudaMemcpyDeviceToHost, s.stream), SANKHYA_GPU_COPY_FAILED);
+  SIH26_SCUDA(cudaStreamSynchronize(s.stream), SANKHYA_GPU_SYNC_FAILED);
+  s.active = settle(s, s.active, s.h_compact);
+  s.active_big = settle(s, s.active_big, s.h_compact2);
 }
 
 }  // namespace sih26
@@ -592,6 +659,8 @@ void sankhya_pdhg_server_default_config(sankhya_pdhg_server_config* c) {
   c->pool_bytes = 0;
   c->max_active = 4096;
   c->chunk_attempts = 2048;
+  c->cluster_min_nnz = 16384;
+  c->clusters = 16;
 }
 
 int sankhya_pdhg_server_create(const sankhya_pdhg_server_config* config,
@@ -621,11 +690,18 @@ int sankhya_pdhg_server_create(const sankhya_pdhg_server_config* config,
     SIH26_SCUDA(cudaMalloc(&s->d_slots, cap * sizeof(sih26::BatchSlot)), SANKHYA_GPU_OUT_OF_MEMORY);
     SIH26_SCUDA(cudaMalloc(&s->d_ctrls, cap * sizeof(sih26::Ctrl)), SANKHYA_GPU_OUT_OF_MEMORY);
     SIH26_SCUDA(cudaMalloc(&s->d_compact, cap * sizeof(sih26::Ctrl)), SANKHYA_GPU_OUT_OF_MEMORY);
-    SIH26_SCUDA(cudaMalloc(&s->d_active, cap * sizeof(int)), SANKHYA_GPU_OUT_OF_MEMORY);
-    SIH26_SCUDA(cudaMalloc(&s->d_count, sizeof(int)), SANKHYA_GPU_OUT_OF_MEMORY);
-    SIH26_SCUDA(cudaMalloc(&s->d_head, sizeof(int)), SANKHYA_GPU_OUT_OF_MEMORY);
+    for (int k = 0; k < 2; ++k) {
+      SIH26_SCUDA(cudaMalloc(&s->d_active[k], cap * sizeof(int)), SANKHYA_GPU_OUT_OF_MEMORY);
+      SIH26_SCUDA(cudaMalloc(&s->d_count[k], sizeof(int)), SANKHYA_GPU_OUT_OF_MEMORY);
+      SIH26_SCUDA(cudaMalloc(&s->d_head[k], sizeof(int)), SANKHYA_GPU_OUT_OF_MEMORY);
+      SIH26_SCUDA(cudaMemset(s->d_count[k], 0, sizeof(int)), SANKHYA_GPU_INIT_FAILED);
+    }
+    SIH26_SCUDA(cudaMalloc(&s->d_compact2, cap * sizeof(sih26::Ctrl)), SANKHYA_GPU_OUT_OF_MEMORY);
     SIH26_SCUDA(cudaMallocHost(&s->h_compact, cap * sizeof(sih26::Ctrl)), SANKHYA_GPU_OUT_OF_MEMORY);
+    SIH26_SCUDA(cudaMallocHost(&s->h_compact2, cap * sizeof(sih26::Ctrl)), SANKHYA_GPU_OUT_OF_MEMORY);
     SIH26_SCUDA(cudaMallocHost(&s->h_active, cap * sizeof(int)), SANKHYA_GPU_OUT_OF_MEMORY);
+    SIH26_SCUDA(cudaMallocHost(&s->h_active2, cap * sizeof(int)), SANKHYA_GPU_OUT_OF_MEMORY);
+    SIH26_SCUDA(cudaMallocHost(&s->h_counts, 2 * sizeof(int)), SANKHYA_GPU_OUT_OF_MEMORY);
     s->slot_job.resize(cap);
     for (int k = cap - 1; k >= 0; --k) s->free_slots.push_back(k);
     sih26::build_graph(*s);
@@ -655,11 +731,17 @@ void sankhya_pdhg_server_free(sankhya_pdhg_server* server) {
   cudaFree(s->d_slots);
   cudaFree(s->d_ctrls);
   cudaFree(s->d_compact);
-  cudaFree(s->d_active);
-  cudaFree(s->d_count);
-  cudaFree(s->d_head);
+  for (int k = 0; k < 2; ++k) {
+    cudaFree(s->d_active[k]);
+    cudaFree(s->d_count[k]);
+    cudaFree(s->d_head[k]);
+  }
+  cudaFree(s->d_compact2);
   cudaFreeHost(s->h_compact);
+  cudaFreeHost(s->h_compact2);
   cudaFreeHost(s->h_active);
+  cudaFreeHost(s->h_active2);
+  cudaFreeHost(s->h_counts);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
 }
@@ -676,7 +758,8 @@ int sankhya_pdhg_server_submit(sankhya_pdhg_server* server, const sankhya_pdhg_p
   auto J = std::make_shared<sih26::Job>();
   try {
     J->submit_time = s->now();
-    sih26::prepare(*J, *problem, params ? *params : defaults);  // host work, outside the lock
+    sih26::prepare(*J, *problem, params ? *params : defaults,
+                   s->cfg.cluster_min_nnz);  // host work, outside the lock
   } catch (const Failure& f) {
     sih26::g_last_error = f.message;
     return f.code;
@@ -719,7 +802,7 @@ int sankhya_pdhg_server_step(sankhya_pdhg_server* server, int32_t* active, int32
     sih26::g_last_error = f.message;
     return f.code;
   }
-  if (active) *active = static_cast<int32_t>(s->active.size());
+  if (active) *active = static_cast<int32_t>(s->active.size() + s->active_big.size());
   if (waiting) *waiting = static_cast<int32_t>(s->waiting.size());
   if (finished) {
     int32_t k = 0;

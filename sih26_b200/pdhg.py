@@ -15,7 +15,7 @@ import ctypes as C
 import dataclasses
 import math
 import os
-from typing import Optional
+from typing import List, Optional
 
 import numpy as np
 
@@ -310,7 +310,8 @@ def solve_pdhg(model: LP, options: Optional[Options] = None) -> Solution:
 class _ServerConfig(C.Structure):
     _fields_ = [("device", C.c_int32), ("memory_fraction", C.c_double),
                 ("pool_bytes", C.c_int64), ("max_active", C.c_int32),
-                ("chunk_attempts", C.c_int64), ("reserved", C.c_int32 * 8)]
+                ("chunk_attempts", C.c_int64), ("cluster_min_nnz", C.c_int64),
+                ("clusters", C.c_int32), ("reserved", C.c_int32 * 7)]
 
 
 def _bind_server(lib):
@@ -420,16 +421,20 @@ def batch_solve(models, options: Optional[Options] = None):
 
 class Server:
     """A resident GPU server for many LPs (sankhya_pdhg_server_*): submit() queues an LP,
-    step() admits what fits and runs one launch over every active LP, result() collects."""
+    step() admits what fits and runs one launch over every active LP, result() collects.
+    LPs with at least `cluster_min_nnz` nonzeros run on an 8-block thread-block cluster
+    (`clusters` of them are kept), the others on one block each."""
 
     def __init__(self, device: int = 0, memory_fraction: float = 0.8, pool_bytes: int = 0,
-                 max_active: int = 4096, chunk_attempts: int = 2048):
+                 max_active: int = 4096, chunk_attempts: int = 2048,
+                 cluster_min_nnz: int = 16384, clusters: int = 16):
         self.lib = load_library()
         _bind_server(self.lib)
         cfg = _ServerConfig()
         self.lib.sankhya_pdhg_server_default_config(C.byref(cfg))
         cfg.device, cfg.memory_fraction, cfg.pool_bytes = device, memory_fraction, pool_bytes
         cfg.max_active, cfg.chunk_attempts = max_active, chunk_attempts
+        cfg.cluster_min_nnz, cfg.clusters = cluster_min_nnz, clusters
         self.handle = C.c_void_p()
         code = self.lib.sankhya_pdhg_server_create(C.byref(cfg), C.byref(self.handle))
         if code != 0:
@@ -464,6 +469,21 @@ class Server:
             raise GpuError(code, self.lib.sankhya_pdhg_gpu_last_error().decode())
         del self.pending[ticket]
         return out.solution(model)
+
+    def solve_all(self, models, options: Optional[Options] = None) -> List[Solution]:
+        """Submits every model, steps until all have finished, returns the answers in order."""
+        tickets = [self.submit(m, options) for m in models]
+        done = {}
+        while len(done) < len(tickets):
+            active, waiting, _ = self.step()
+            for t in tickets:
+                if t not in done:
+                    r = self.result(t)
+                    if r is not None:
+                        done[t] = r
+            if active == 0 and waiting == 0 and len(done) < len(tickets):
+                raise GpuError(1, "server idle with unfinished tickets")
+        return [done[t] for t in tickets]
 
     def close(self):
         if self.handle:

@@ -120,3 +120,44 @@ def test_server_admits_while_others_run_and_matches_the_batch(batch):
         assert r.status == sols[k].status
         assert r.iterations == sols[k].iterations  # chunking pauses, it changes nothing
         assert np.array_equal(r.col_value, sols[k].col_value)
+
+
+def test_cluster_class_meets_the_tolerance_and_is_the_same_alone(batch):
+    """Every LP forced onto 8-block clusters: same bar, and the same bits alone and in the mix."""
+    lps, sols = batch
+    subset = lps[:16]
+    with P.Server(chunk_attempts=0, cluster_min_nnz=1, clusters=4) as srv:
+        got = srv.solve_all(subset, _opts())
+    for lp, s, ref in zip(subset, got, sols):
+        assert s.status == ref.status, (lp.name, s.status, ref.status)
+        if lp.farkas_star is not None:
+            ok, why = _farkas_ok(lp, s.farkas_dual)
+            assert ok, (lp.name, why)
+            continue
+        r = oracle.oracle_evaluate(lp, s.col_value, -s.row_dual)
+        assert max(r["primal"], r["dual"], r["gap"]) <= TOL, (lp.name, r)
+    with P.Server(chunk_attempts=0, cluster_min_nnz=1, clusters=4) as srv:
+        alone = srv.solve_all([subset[3]], _opts())[0]
+    assert alone.iterations == got[3].iterations
+    assert np.array_equal(alone.col_value, got[3].col_value)
+
+
+def test_both_classes_in_one_server_match_their_own_runs(batch):
+    """A threshold that splits the batch: each LP gets what its class gives it alone."""
+    lps, sols = batch
+    nnz = sorted(lp.num_nonzeros for lp in lps)
+    cut = nnz[len(nnz) // 2]
+    with P.Server(chunk_attempts=512, cluster_min_nnz=cut, clusters=4) as srv:
+        mixed = srv.solve_all(lps, _opts())
+    big = [k for k, lp in enumerate(lps) if lp.num_nonzeros >= cut]
+    small = [k for k in range(len(lps)) if lps[k].num_nonzeros < cut]
+    assert big and small
+    for k in small[:6]:
+        assert mixed[k].iterations == sols[k].iterations
+        assert np.array_equal(mixed[k].col_value, sols[k].col_value)
+    with P.Server(chunk_attempts=0, cluster_min_nnz=1, clusters=4) as srv:
+        own = srv.solve_all([lps[k] for k in big[:6]], _opts())
+    for k, o in zip(big[:6], own):
+        assert mixed[k].status == o.status
+        assert mixed[k].iterations == o.iterations
+        assert np.array_equal(mixed[k].col_value, o.col_value)
