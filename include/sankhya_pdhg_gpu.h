@@ -66,10 +66,10 @@ enum {
 /* Arithmetic of the iteration. */
 enum {
   SANKHYA_PDHG_FP64 = 0,  /* FP64 matrix, iterates and reductions throughout */
-  SANKHYA_PDHG_MIXED = 1  /* FP32 matrix and iterates with FP64 reductions and FP64 KKT,
-                             restart and step-size logic; then an FP64 polish phase
-                             warm-started from the FP32 iterate when the request is below
-                             what FP32 reaches */
+  SANKHYA_PDHG_MIXED = 1  /* FP32 matrix and FP32 iterate deltas about an FP64 restart
+                             anchor, FP64 reductions and FP64 KKT, restart and step-size
+                             logic; an FP64 polish phase takes over from the FP32 state when
+                             the FP32 level stops improving before the request */
 };
 
 /* Stopping rule. */
@@ -117,13 +117,17 @@ typedef struct sankhya_pdhg_params {
   int32_t detect_infeasibility; /* 1 (default): certify primal infeasibility / dual
                                    unboundedness from iterate differences */
   double mixed_switch_tolerance; /* MIXED: relative KKT at which the FP32 phase hands over to
-                                    the FP64 polish; 0 (default) = run FP32 to the request and
-                                    hand over only if the FP32 iterate stalls */
+                                    the FP64 polish (with its whole restart state); 0 (default)
+                                    = the request (no finer than 1e-10), or earlier if the FP32
+                                    level stops improving */
   int32_t group_size_rows;  /* lanes per row for A x (0 = autotune) */
   int32_t group_size_cols;  /* lanes per row for A'y (0 = autotune) */
   int32_t grid_blocks;      /* blocks of the cooperative launches (0 = sized to the problem) */
   int32_t profile_kernels;  /* 1: time every iteration-kernel launch with CUDA events */
-  int32_t reserved[6];
+  int32_t mixed_stall_checks; /* MIXED: host checks (about 2,600 iterations each) without a
+                                 better KKT error before the FP32 phase hands over; 0 = auto
+                                 (no 1% gain over the last 30% of the iterations), -1 = never */
+  int32_t reserved[5];
 } sankhya_pdhg_params;
 
 /* Unscaled residual block of the reported point (src/pdhg/pdhg.cpp:81-110). */

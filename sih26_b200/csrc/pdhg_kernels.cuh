@@ -21,6 +21,10 @@
 //     the running average (pdhg.cpp:143-263), candidate choice, best point, stopping test
 //     and restart with the primal-weight update (pdhg.cpp:505-643).
 //
+// Two precision levels share this code: FP64 (iterates, matrix and reductions in FP64) and
+// the FP32 level of the mixed mode (FP32 matrix and FP32 iterate deltas about an FP64 restart
+// anchor, FP64 accumulation; see kDelta), which hands over to FP64 only if it stops improving.
+//
 // Internal index spaces are permuted: rows of A sorted by nonzero count (descending) and
 // columns likewise, so a work item holds rows of similar length; the host un-permutes
 // outputs. Reductions use fixed trees over a fixed work partition, so a run is bit-for-bit
@@ -115,6 +119,12 @@ struct Prob {
   const T* cu;
   const T* rl;
   const T* ru;
+  // the same in FP64 (the FP32 level projects and forms its anchor terms with these)
+  const double* c64;
+  const double* cl64;
+  const double* cu64;
+  const double* rl64;
+  const double* ru64;
   const double* dr;  // row scaling Dr, permuted
   const double* dc;  // column scaling Dc, permuted
   // unscaled problem, permuted; c0 is the min-space cost (pdhg.cpp:287-291)
@@ -127,13 +137,22 @@ struct Prob {
 
 template <class T>
 struct State {
+  // FP64 level: x, y are the iterates and ax = A x. FP32 level: x, y are FP32 deltas from the
+  // FP64 restart anchor (xr, yr), ax = A dx, and xsum, ysum sum the deltas (see kDelta).
   T* x[2];
   T* y[2];
   double* ax[2];
   double* xsum;
   double* ysum;
-  T* xr;
-  T* yr;
+  double* xr;  // restart anchor
+  double* yr;
+  // FP32 level only: the anchor's terms, refreshed at every restart
+  double* cg;     // [n] c + A'yr (scaled)
+  float* dl;      // [n] lower bound - xr, rounded to FP32
+  float* du;      // [n] upper bound - xr
+  double* axr;    // [m] A xr
+  double* xfull;  // [n] evaluation scratch: xr + dx
+  double* yfull;  // [m] yr + dy
   double* xavg;
   double* yavg;
   double* best_x;  // scaled, FP64
@@ -413,6 +432,119 @@ struct StoreRow {
   }
 };
 
+// ---- the FP32 level: deltas from an FP64 restart anchor ---------------------------------
+//
+// The FP32 level keeps x = xr + dx and y = yr + dy with the anchor (xr, yr) in FP64 and the
+// deltas in FP32. The anchor's terms are formed once per restart in FP64 (cg = c + A'yr,
+// axr = A xr, bounds relative to xr), so each iteration streams the FP32 matrix and gathers
+// FP32 deltas only, and a rounding error is relative to the distance from the anchor rather
+// than to the iterate itself: as the restarts close in on the optimum the FP32 iterate keeps
+// its accuracy, where a plain FP32 iterate stalls at a few hundred units of FP32 rounding.
+template <class T>
+constexpr bool kDelta = sizeof(T) == 4;
+
+// dx' = proj_[dl,du](dx - tau (cg + A'dy)): the primal step of pdhg.cpp:392-400 in deltas.
+template <class T>
+struct PrimalStepDelta {
+  const T* x;
+  T* xn;
+  const double* cg;
+  const float* dl;
+  const float* du;
+  double* xsum;
+  double tau;
+  int pending;
+  struct In {
+    double xo, c, lo, hi, xs;
+  };
+  __device__ __forceinline__ In load(int j) const {
+    In v;
+    v.xo = ld(x + j);
+    v.c = ro(cg + j);
+    v.lo = ro(dl + j);
+    v.hi = ro(du + j);
+    v.xs = pending ? __ldcg(xsum + j) : 0.0;
+    return v;
+  }
+  __device__ __forceinline__ void apply(int j, const double (&s)[1], const In& v,
+                                        double (&acc)[3]) const {
+    if (pending) xsum[j] = v.xs + v.xo;
+    const double xnew = project(v.xo - tau * (v.c + s[0]), v.lo, v.hi);
+    const T xs = static_cast<T>(xnew);
+    xn[j] = xs;
+    const double d = static_cast<double>(xs) - v.xo;
+    acc[0] += d * d;
+  }
+};
+
+// The dual step of pdhg.cpp:402-408 in deltas: with a' = A dx' (this phase), a = A dx,
+// A xbar = axr + 2 a' - a and v = yr + dy + sigma A xbar in FP64; dy' = y' - yr.
+template <class T>
+struct DualStepDelta {
+  const T* y;
+  T* yn;
+  const double* ax;
+  double* axn;
+  const double* yr;
+  const double* axr;
+  const double* rl;
+  const double* ru;
+  double* ysum;
+  double sigma;
+  int pending;
+  struct In {
+    double yo, aold, yr, axr, lo, hi, ys;
+  };
+  __device__ __forceinline__ In load(int i) const {
+    In v;
+    v.yo = ld(y + i);
+    v.aold = __ldcg(ax + i);
+    v.yr = ro(yr + i);
+    v.axr = ro(axr + i);
+    v.lo = ro(rl + i);
+    v.hi = ro(ru + i);
+    v.ys = pending ? __ldcg(ysum + i) : 0.0;
+    return v;
+  }
+  __device__ __forceinline__ void apply(int i, const double (&s)[1], const In& v,
+                                        double (&acc)[3]) const {
+    if (pending) ysum[i] = v.ys + v.yo;
+    const double anew = s[0];
+    const double w = (v.yr + v.yo) + sigma * (v.axr + 2.0 * anew - v.aold);
+    const double ynew = w - sigma * project(w / sigma, v.lo, v.hi);
+    const T ys = static_cast<T>(ynew - v.yr);
+    yn[i] = ys;
+    axn[i] = anew;
+    const double d = static_cast<double>(ys) - v.yo;
+    acc[1] += d * d;
+    acc[2] += d * (anew - v.aold);
+  }
+};
+
+// Column side of the anchor terms: cg = c + A'yr and the bounds relative to xr (an absent
+// bound stays absent).
+struct AnchorCol {
+  const double* c;
+  const double* cl;
+  const double* cu;
+  const double* xr;
+  double* cg;
+  float* dl;
+  float* du;
+  struct In {
+    double c, lo, hi, xr;
+  };
+  __device__ __forceinline__ In load(int j) const {
+    return In{__ldg(c + j), __ldg(cl + j), __ldg(cu + j), __ldcg(xr + j)};
+  }
+  __device__ __forceinline__ void apply(int j, const double (&s)[1], const In& v,
+                                        double (&)[1]) const {
+    cg[j] = v.c + s[0];
+    dl[j] = finite_bound(v.lo) ? static_cast<float>(v.lo - v.xr) : -INFINITY;
+    du[j] = finite_bound(v.hi) ? static_cast<float>(v.hi - v.xr) : INFINITY;
+  }
+};
+
 // Sum (or max) of kPartSlots-wide block partials over all blocks, in block order. Every
 // block calls it after a barrier and gets identical totals.
 template <int NS, unsigned MAXMASK>
@@ -525,7 +657,10 @@ __global__ void __launch_bounds__(kThreads, 2) iterate_kernel(Prob<T> P, State<T
     double* part = S.partials + (size_t)(c.attempts & 1) * G * kPartSlots;
     double acc[3] = {0.0, 0.0, 0.0};
     SIH26_MARK_START();
-    {
+    if constexpr (kDelta<T>) {
+      PrimalStepDelta<T> ps{S.x[cur], S.x[nxt], S.cg, S.dl, S.du, S.xsum, tau, c.pending};
+      run_phase<1, 3>(P.AT.ptr, P.AT.idx, P.AT.val, P.pat, Gather1<T>{S.y[cur]}, ps, acc, stream);
+    } else {
       PrimalStep<T> ps{S.x[cur], S.x[nxt], P.c, P.cl, P.cu, S.xsum, tau, c.pending};
       run_phase<1, 3>(P.AT.ptr, P.AT.idx, P.AT.val, P.pat, Gather1<T>{S.y[cur]}, ps, acc, stream);
     }
@@ -533,7 +668,11 @@ __global__ void __launch_bounds__(kThreads, 2) iterate_kernel(Prob<T> P, State<T
     if (!grid_barrier(S.bar)) goto device_error;
     SIH26_MARK(1);
 
-    {
+    if constexpr (kDelta<T>) {
+      DualStepDelta<T> ds{S.y[cur], S.y[nxt], S.ax[cur], S.ax[nxt], S.yr, S.axr, P.rl64,
+                          P.ru64, S.ysum, sigma, c.pending};
+      run_phase<1, 3>(P.A.ptr, P.A.idx, P.A.val, P.pa, Gather1<T>{S.x[nxt]}, ds, acc, stream);
+    } else {
       DualStep<T> ds{S.y[cur], S.y[nxt], S.ax[cur], S.ax[nxt], P.rl, P.ru, S.ysum, sigma, c.pending};
       run_phase<1, 3>(P.A.ptr, P.A.idx, P.A.val, P.pa, Gather1<T>{S.x[nxt]}, ds, acc, stream);
     }
@@ -571,6 +710,25 @@ __global__ void __launch_bounds__(kThreads, 2) init_ax_kernel(Prob<T> P, State<T
   const int cur = S.ctrl->cur;
   run_phase<1, 1>(P.A.ptr, P.A.idx, P.A.val, P.pa, Gather1<T>{S.x[cur]},
                   StoreRow<1>{S.ax[cur], -1}, dummy, stream);
+}
+
+// The FP32 level's anchor terms from (xr, yr), FP64 values: axr = A xr, cg = c + A'yr, the
+// relative bounds. Needs xr and yr complete in every block.
+template <class T>
+__device__ __forceinline__ void anchor_phases(const Prob<T>& P, const State<T>& S,
+                                              double* stream) {
+  double dummy[1] = {0.0};
+  run_phase<1, 1>(P.A.ptr, P.A.idx, P.A.val64, P.pa, Gather1<double>{S.xr},
+                  StoreRow<1>{S.axr, -1}, dummy, stream);
+  run_phase<1, 1>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pat, Gather1<double>{S.yr},
+                  AnchorCol{P.c64, P.cl64, P.cu64, S.xr, S.cg, S.dl, S.du}, dummy, stream);
+}
+
+// Start of the FP32 level: the anchor terms of the starting anchor (the deltas start at 0).
+template <class T>
+__global__ void __launch_bounds__(kThreads, 2) anchor_kernel(Prob<T> P, State<T> S) {
+  double* stream = warp_stream();
+  anchor_phases(P, S, stream);
 }
 
 // ---- evaluation ---------------------------------------------------------------------------
@@ -794,21 +952,39 @@ __global__ void __launch_bounds__(kThreads, 2) evaluate_kernel(Prob<T> P, State<
 
   // E1: fold the pending running-sum term, form the scaled averages, and measure the
   // movement since the last restart (pdhg.cpp:519-528, 613-624).
+  // On the FP32 level the iterates and sums are deltas from the anchor: the movement is the
+  // delta itself, and the full FP64 iterate goes to xfull / yfull for the passes below.
   double acc1[2] = {0.0, 0.0};
   for (int j = gt; j < P.n; j += stride) {
     const double xo = ld(S.x[cur] + j);
     const double xs = S.xsum[j] + (c.pending ? xo : 0.0);
     S.xsum[j] = xs;
-    S.xavg[j] = has_average ? xs / count : 0.0;
-    const double d = xo - ld(S.xr + j);
+    double d;
+    if constexpr (kDelta<T>) {
+      const double r = S.xr[j];
+      S.xfull[j] = r + xo;
+      S.xavg[j] = has_average ? r + xs / count : 0.0;
+      d = xo;
+    } else {
+      S.xavg[j] = has_average ? xs / count : 0.0;
+      d = xo - ld(S.xr + j);
+    }
     acc1[0] += d * d;
   }
   for (int i = gt; i < P.m; i += stride) {
     const double yo = ld(S.y[cur] + i);
     const double ys = S.ysum[i] + (c.pending ? yo : 0.0);
     S.ysum[i] = ys;
-    S.yavg[i] = has_average ? ys / count : 0.0;
-    const double d = yo - ld(S.yr + i);
+    double d;
+    if constexpr (kDelta<T>) {
+      const double r = S.yr[i];
+      S.yfull[i] = r + yo;
+      S.yavg[i] = has_average ? r + ys / count : 0.0;
+      d = yo;
+    } else {
+      S.yavg[i] = has_average ? ys / count : 0.0;
+      d = yo - ld(S.yr + i);
+    }
     acc1[1] += d * d;
   }
   block_reduce<2, 0u>(acc1, sh);
@@ -820,12 +996,21 @@ __global__ void __launch_bounds__(kThreads, 2) evaluate_kernel(Prob<T> P, State<
     double acc[kEvalSlots];
 #pragma unroll
     for (int s = 0; s < kEvalSlots; ++s) acc[s] = 0.0;
-    RowEval<T, 2> re{P.dr, P.rl0, P.ru0, S.y[cur], S.yavg, nullptr, nullptr};
-    run_phase<2, kEvalSlots>(P.A.ptr, P.A.idx, P.A.val64, P.pa,
-                             Gather2<T, double>{S.x[cur], S.xavg}, re, acc, stream);
-    ColEval<T, 2> ce{P.dc, P.cl0, P.cu0, P.c0, S.x[cur], S.xavg, nullptr, nullptr, nullptr};
-    run_phase<2, kEvalSlots>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pat,
-                             Gather2<T, double>{S.y[cur], S.yavg}, ce, acc, stream);
+    if constexpr (kDelta<T>) {
+      RowEval<T, 2> re{P.dr, P.rl0, P.ru0, nullptr, S.yavg, S.yfull, nullptr};
+      run_phase<2, kEvalSlots>(P.A.ptr, P.A.idx, P.A.val64, P.pa,
+                               Gather2<double, double>{S.xfull, S.xavg}, re, acc, stream);
+      ColEval<T, 2> ce{P.dc, P.cl0, P.cu0, P.c0, nullptr, S.xavg, S.xfull, nullptr, nullptr};
+      run_phase<2, kEvalSlots>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pat,
+                               Gather2<double, double>{S.yfull, S.yavg}, ce, acc, stream);
+    } else {
+      RowEval<T, 2> re{P.dr, P.rl0, P.ru0, S.y[cur], S.yavg, nullptr, nullptr};
+      run_phase<2, kEvalSlots>(P.A.ptr, P.A.idx, P.A.val64, P.pa,
+                               Gather2<T, double>{S.x[cur], S.xavg}, re, acc, stream);
+      ColEval<T, 2> ce{P.dc, P.cl0, P.cu0, P.c0, S.x[cur], S.xavg, nullptr, nullptr, nullptr};
+      run_phase<2, kEvalSlots>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pat,
+                               Gather2<T, double>{S.y[cur], S.yavg}, ce, acc, stream);
+    }
     block_reduce<kEvalSlots, kEvalMaxMask>(acc, sh);
     write_partials(part, 2, acc, kEvalSlots);
   }
@@ -843,20 +1028,32 @@ __global__ void __launch_bounds__(kThreads, 2) evaluate_kernel(Prob<T> P, State<
   // E3: keep the best point (scaled, FP64) and reset the average at a restart.
   if (flags[0] || flags[1]) {
     for (int j = gt; j < P.n; j += stride) {
-      const double xo = ld(S.x[cur] + j);
+      const double xo = kDelta<T> ? S.xfull[j] : ld(S.x[cur] + j);
       if (flags[0]) S.best_x[j] = flags[2] ? S.xavg[j] : xo;
       if (flags[1]) {
-        S.xr[j] = S.x[cur][j];
+        S.xr[j] = xo;
         S.xsum[j] = 0.0;
+        if constexpr (kDelta<T>) S.x[cur][j] = T(0);
       }
     }
     for (int i = gt; i < P.m; i += stride) {
-      const double yo = ld(S.y[cur] + i);
+      const double yo = kDelta<T> ? S.yfull[i] : ld(S.y[cur] + i);
       if (flags[0]) S.best_y[i] = flags[2] ? S.yavg[i] : yo;
       if (flags[1]) {
-        S.yr[i] = S.y[cur][i];
+        S.yr[i] = yo;
         S.ysum[i] = 0.0;
+        if constexpr (kDelta<T>) {
+          S.y[cur][i] = T(0);
+          S.ax[cur][i] = 0.0;
+        }
       }
+    }
+  }
+  if constexpr (kDelta<T>) {
+    // a restart moved the anchor: form its terms (every block takes the same branch)
+    if (flags[1]) {
+      if (!grid_barrier(S.bar)) goto device_error;
+      anchor_phases(P, S, stream);
     }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) *S.ctrl = c;
@@ -894,23 +1091,23 @@ __global__ void __launch_bounds__(kThreads, 2) report_kernel(Prob<T> P, State<T>
   }
 }
 
-// FP32 -> FP64 hand-over of the mixed-precision mode: the FP64 iterate starts at the FP32
-// one, which also becomes the restart anchor; the running sums start empty.
-static __global__ void handover_kernel(const float* x32, const float* y32, double* x64, double* y64,
-                                double* xr64, double* yr64, double* xsum, double* ysum, int m,
-                                int n) {
+// FP32 -> FP64 hand-over of the mixed-precision mode: the FP32 level's restart state into
+// the FP64 level -- iterate (into slot 0), restart anchor and running sums, the deltas added
+// back to the anchor (`count` iterates are summed).
+static __global__ void handover_kernel(State<float> from, int cur, double count, State<double> to,
+                                       int m, int n) {
   const int stride = gridDim.x * blockDim.x;
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
-    const double v = x32[j];
-    x64[j] = v;
-    xr64[j] = v;
-    xsum[j] = 0.0;
+    const double r = from.xr[j];
+    to.x[0][j] = r + static_cast<double>(from.x[cur][j]);
+    to.xr[j] = r;
+    to.xsum[j] = count * r + from.xsum[j];
   }
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
-    const double v = y32[i];
-    y64[i] = v;
-    yr64[i] = v;
-    ysum[i] = 0.0;
+    const double r = from.yr[i];
+    to.y[0][i] = r + static_cast<double>(from.y[cur][i]);
+    to.yr[i] = r;
+    to.ysum[i] = count * r + from.ysum[i];
   }
 }
 

@@ -142,6 +142,7 @@ struct Common {
   const int *a_ptr, *a_idx, *at_ptr, *at_idx;
   const double *a_val64, *at_val64;
   const double *dr, *dc, *c0, *cl0, *cu0, *rl0, *ru0;
+  const double *c64, *cl64, *cu64, *rl64, *ru64;  // scaled, FP64
   Part pa, pat;
   double *best_x, *best_y, *partials;
   Ctrl* ctrl;
@@ -171,11 +172,18 @@ static Level<T> make_level(Arena& a, const Common& cm, const PermutedLp& q, cons
   }
   P.pa = cm.pa;
   P.pat = cm.pat;
-  P.c = a.upload<T>(gather(s.cost, q.col_perm));
-  P.cl = a.upload<T>(gather(s.cl, q.col_perm));
-  P.cu = a.upload<T>(gather(s.cu, q.col_perm));
-  P.rl = a.upload<T>(gather(s.rl, q.row_perm));
-  P.ru = a.upload<T>(gather(s.ru, q.row_perm));
+  P.c64 = cm.c64;
+  P.cl64 = cm.cl64;
+  P.cu64 = cm.cu64;
+  P.rl64 = cm.rl64;
+  P.ru64 = cm.ru64;
+  if constexpr (std::is_same<T, double>::value) {
+    P.c = cm.c64;
+    P.cl = cm.cl64;
+    P.cu = cm.cu64;
+    P.rl = cm.rl64;
+    P.ru = cm.ru64;
+  }
   P.dr = cm.dr;
   P.dc = cm.dc;
   P.c0 = cm.c0;
@@ -191,19 +199,27 @@ static Level<T> make_level(Arena& a, const Common& cm, const PermutedLp& q, cons
   }
   S.xsum = a.zeros<double>(n);
   S.ysum = a.zeros<double>(m);
-  S.xr = a.zeros<T>(n);
-  S.yr = a.zeros<T>(m);
+  S.xr = a.zeros<double>(n);
+  S.yr = a.zeros<double>(m);
   S.xavg = a.zeros<double>(n);
   S.yavg = a.zeros<double>(m);
+  if constexpr (kDelta<T>) {
+    S.cg = a.zeros<double>(n);
+    S.dl = a.zeros<float>(n);
+    S.du = a.zeros<float>(n);
+    S.axr = a.zeros<double>(m);
+    S.xfull = a.zeros<double>(n);
+    S.yfull = a.zeros<double>(m);
+  }
   S.best_x = cm.best_x;
   S.best_y = cm.best_y;
   S.partials = cm.partials;
   S.ctrl = cm.ctrl;
   S.bar = cm.bar;
   if (!x0.empty()) {
-    std::vector<T> xt(x0.begin(), x0.end());
-    a.put(S.x[0], xt.data(), n * sizeof(T), 0);
-    a.put(S.xr, xt.data(), n * sizeof(T), 0);
+    // the FP64 level starts at x0; the FP32 level at the anchor x0 with zero deltas
+    if constexpr (!kDelta<T>) a.put(S.x[0], x0.data(), n * sizeof(double), 0);
+    a.put(S.xr, x0.data(), n * sizeof(double), 0);
     SIH26_CUDA(cudaDeviceSynchronize(), SANKHYA_GPU_SYNC_FAILED);
   }
   return L;
@@ -215,6 +231,7 @@ template <class T>
 static int blocks_per_sm() {
   const void* k1[] = {reinterpret_cast<const void*>(iterate_kernel<T>),
                       reinterpret_cast<const void*>(init_ax_kernel<T>),
+                      reinterpret_cast<const void*>(anchor_kernel<T>),
                       reinterpret_cast<const void*>(report_kernel<T>),
                       reinterpret_cast<const void*>(power_kernel<T>)};
   int best = 1 << 20;
@@ -236,9 +253,6 @@ static int blocks_per_sm() {
 }
 
 // Runs (iterate, evaluate) launch pairs until the device reports a final state. With
-// `watch_stall` (the FP32 phase of the mixed mode) it also returns, with *stalled set, once
-// the best KKT error has not moved over two host checks of at least 16 pairs each: the FP32
-// iterate has reached what its precision allows.
 // Event-timed launches of the iteration kernel (profile_kernels).
 struct LaunchTimer {
   bool on = false;
@@ -269,17 +283,23 @@ struct LaunchTimer {
 };
 
 // Runs (iterate, evaluate) launch pairs until the device reports a final state. With
-// `watch_stall` (the FP32 phase of the mixed mode) it also returns, with *stalled set, once
-// the best KKT error has not moved over two host checks of at least 16 pairs each: the FP32
-// iterate has reached what its precision allows.
+// `stall_checks` > 0 (the FP32 phase of the mixed mode) it also returns, with *stalled set,
+// once the best KKT error has not moved over that many host checks of at least 16 pairs each:
+// the FP32 iterate has reached what its precision allows. kAutoStall is the default rule:
+// no 1 % improvement over the last 30 % of the iterations, and over 8 checks at least --
+// wide enough for the long plateaus restarted PDHG goes through on its own.
+constexpr int kAutoStall = -2;
+
 template <class T>
 static Ctrl run_loop(Level<T>& L, int G, cudaStream_t stream, Ctrl* host_ctrl, int verbose,
-                     bool watch_stall, bool* stalled, LaunchTimer& timer) {
+                     int stall_checks, bool* stalled, LaunchTimer& timer) {
   long long max_attempts = 1ll << 40;
   int pairs = 4;
   Ctrl c{};
   double last_best = INFINITY;
   int flat = 0;
+  double mark_best = INFINITY;     // auto rule: best error at the last 1 % improvement
+  long long mark_iteration = 0;    // and the iteration it was seen at
   if (stalled) *stalled = false;
   for (;;) {
     if (timer.on) timer.ensure(pairs);
@@ -303,9 +323,22 @@ static Ctrl run_loop(Level<T>& L, int G, cudaStream_t stream, Ctrl* host_ctrl, i
       std::fflush(stdout);
     }
     if (c.state != kRunning && c.state != kNeedEval) break;
-    if (watch_stall && pairs >= 16) {
+    if (stall_checks > 0 && pairs >= 16) {
       flat = (c.best_worst >= last_best) ? flat + 1 : 0;
-      if (flat >= 2) {
+      if (flat >= stall_checks) {
+        *stalled = true;
+        break;
+      }
+    } else if (stall_checks == kAutoStall) {
+      // no 1 % improvement over the last 30 % of the iterations (and 8 checks at least)
+      if (c.best_worst < 0.99 * mark_best) {
+        mark_best = c.best_worst;
+        mark_iteration = c.iteration;
+        flat = 0;
+      } else if (pairs >= 16) {
+        ++flat;
+      }
+      if (flat >= 8 && c.iteration - mark_iteration > (long long)(0.3 * (double)c.iteration)) {
         *stalled = true;
         break;
       }
@@ -315,6 +348,12 @@ static Ctrl run_loop(Level<T>& L, int G, cudaStream_t stream, Ctrl* host_ctrl, i
   }
   return c;
 }
+
+// Relative KKT error below which the FP32 phase of the mixed mode hands over by default.
+// FP32 deltas about an FP64 anchor keep their accuracy as the restarts close in (a plain FP32
+// iterate stalls near 256 units of FP32 rounding, ~1.5e-5), so this is only a backstop for
+// requests at the edge of FP64 itself; the stall rule catches a level that stops improving.
+constexpr double kFp32Reach = 1e-10;
 
 static int G_max_coresident(const cudaDeviceProp& props, int bpsm) {
   return props.multiProcessorCount * bpsm;
@@ -406,6 +445,11 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
   cm.cu0 = a.upload_same(gather_ptr(prob.col_upper, q.col_perm));
   cm.rl0 = a.upload_same(gather_ptr(prob.row_lower, q.row_perm));
   cm.ru0 = a.upload_same(gather_ptr(prob.row_upper, q.row_perm));
+  cm.c64 = a.upload_same(gather(sc.cost, q.col_perm));
+  cm.cl64 = a.upload_same(gather(sc.cl, q.col_perm));
+  cm.cu64 = a.upload_same(gather(sc.cu, q.col_perm));
+  cm.rl64 = a.upload_same(gather(sc.rl, q.row_perm));
+  cm.ru64 = a.upload_same(gather(sc.ru, q.row_perm));
   cm.pa = upload_part(a, partition(q.a_ptr, G, kWarps, prm.group_size_rows));
   cm.pat = upload_part(a, partition(q.at_ptr, G, kWarps, prm.group_size_cols));
   cm.best_x = a.zeros<double>(n);
@@ -448,7 +492,7 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
   }
   // A x0 for the starting point, with the same phase code as the iteration's A x'
   if (mixed) {
-    init_ax_kernel<float><<<G, kThreads, stream_smem_bytes(), stream>>>(L32.P, L32.S);
+    anchor_kernel<float><<<G, kThreads, stream_smem_bytes(), stream>>>(L32.P, L32.S);
   } else {
     init_ax_kernel<double><<<G, kThreads, stream_smem_bytes(), stream>>>(L64.P, L64.S);
   }
@@ -524,38 +568,37 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
   long long fp32_iterations = 0;
   if (!mixed) {
     a.put(cm.ctrl, &c0, sizeof(Ctrl), stream);
-    fin = run_loop(L64, G, stream, host_ctrl, prm.verbose, false, nullptr, timer);
+    fin = run_loop(L64, G, stream, host_ctrl, prm.verbose, 0, nullptr, timer);
   } else {
-    // FP32 phase: relative KKT to the request (or to the switch tolerance when one is set),
-    // handing over early if the FP32 iterate stalls
-    const double fp32_target = prm.mixed_switch_tolerance > 0.0
-                                   ? std::max(prm.tolerance, prm.mixed_switch_tolerance)
-                                   : prm.tolerance;
+    // FP32 phase: relative KKT to the switch tolerance -- by default the request, but no
+    // finer than kFp32Reach -- handing over early if the FP32 level stalls
+    const double fp32_target =
+        prm.mixed_switch_tolerance > 0.0 ? std::max(prm.tolerance, prm.mixed_switch_tolerance)
+                                         : std::max(prm.tolerance, kFp32Reach);
     Ctrl c32 = c0;
     c32.stop_rule = 1;
     c32.tolerance = fp32_target;
     a.put(cm.ctrl, &c32, sizeof(Ctrl), stream);
     bool stalled = false;
-    fin = run_loop(L32, G, stream, host_ctrl, prm.verbose, true, &stalled, timer);
+    const int stall_checks = prm.mixed_stall_checks > 0 ? prm.mixed_stall_checks
+                           : prm.mixed_stall_checks < 0 ? 0 : kAutoStall;
+    fin = run_loop(L32, G, stream, host_ctrl, prm.verbose, stall_checks, &stalled, timer);
     fp32_iterations = fin.iteration;
     const bool done_in_fp32 = fin.state == kConverged && prm.stop_rule == 1 &&
                               fp32_target <= prm.tolerance;
     const bool limit_hit = fin.state == kIterationLimit || fin.state == kTimeLimit ||
                            fin.state == kDeviceError;
     if (!done_in_fp32 && !limit_hit) {
-      // FP64 polish, warm-started from the FP32 iterate
+      // FP64 polish. The hand-over keeps the whole restart state -- iterate, restart anchor,
+      // running sums and their count, step size, primal weight -- so the FP64 loop goes on
+      // exactly where the FP32 one stopped, only with more digits.
       const int threads = 256, blocks = std::max(1, std::min(4096, (std::max(m, n) + threads - 1) / threads));
-      handover_kernel<<<blocks, threads, 0, stream>>>(L32.S.x[fin.cur], L32.S.y[fin.cur], L64.S.x[0],
-                                                     L64.S.y[0], L64.S.xr, L64.S.yr, L64.S.xsum,
-                                                     L64.S.ysum, m, n);
+      handover_kernel<<<blocks, threads, 0, stream>>>(L32.S, fin.cur, static_cast<double>(fin.averaged),
+                                                     L64.S, m, n);
       SIH26_CUDA(cudaGetLastError(), SANKHYA_GPU_KERNEL_LAUNCH_FAILED);
       ++g_launches;
       Ctrl h = fin;
       h.cur = 0;
-      h.pending = 0;
-      h.averaged = 0;
-      h.last_restart = h.iteration;
-      h.restart_kkt = h.best_worst;
       h.state = kRunning;
       h.converged = 0;
       h.tolerance = prm.tolerance;
@@ -564,7 +607,7 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
       init_ax_kernel<double><<<G, kThreads, stream_smem_bytes(), stream>>>(L64.P, L64.S);
       SIH26_CUDA(cudaGetLastError(), SANKHYA_GPU_KERNEL_LAUNCH_FAILED);
       ++g_launches;
-      fin = run_loop(L64, G, stream, host_ctrl, prm.verbose, false, nullptr, timer);
+      fin = run_loop(L64, G, stream, host_ctrl, prm.verbose, 0, nullptr, timer);
     }
   }
   SIH26_CUDA(cudaEventRecord(ev1, stream), SANKHYA_GPU_INIT_FAILED);

@@ -69,7 +69,8 @@ class _Params(C.Structure):
                 ("verbose", C.c_int32), ("detect_infeasibility", C.c_int32),
                 ("mixed_switch_tolerance", C.c_double), ("group_size_rows", C.c_int32),
                 ("group_size_cols", C.c_int32), ("grid_blocks", C.c_int32),
-                ("profile_kernels", C.c_int32), ("reserved", C.c_int32 * 6)]
+                ("profile_kernels", C.c_int32), ("mixed_stall_checks", C.c_int32),
+                ("reserved", C.c_int32 * 5)]
 
 
 class _Residuals(C.Structure):
@@ -151,6 +152,7 @@ class Options:
         "pdhg_lanes_cols": (int, 0),
         "pdhg_grid_blocks": (int, 0),
         "pdhg_profile_kernels": (bool, False),
+        "pdhg_mixed_stall_checks": (int, 0),
     }
 
     def __init__(self, **values):
@@ -251,24 +253,7 @@ def solve_pdhg(model: LP, options: Optional[Options] = None) -> Solution:
                     cs.ctypes.data_as(_i32p), ri.ctypes.data_as(_i32p),
                     vals.ctypes.data_as(_f64p), *[v.ctypes.data_as(_f64p) for v in vecs],
                     1 if model.maximize else 0, float(model.objective_offset))
-    prm = _Params()
-    lib.sankhya_pdhg_gpu_default_params(C.byref(prm))
-    prm.tolerance = opt.get("pdhg_tolerance")
-    prm.iteration_limit = opt.get("iteration_limit")
-    prm.time_limit = opt.get("time_limit")
-    prm.restart = int(opt.get("pdhg_restart"))
-    prm.stop_at_request = int(opt.get("pdhg_stop_at_request"))
-    prm.random_seed = opt.get("random_seed")
-    prm.precision = PRECISIONS[opt.get("pdhg_precision")]
-    prm.stop_rule = STOP_RULES[opt.get("pdhg_stop_rule")]
-    prm.device = opt.get("gpu_device")
-    prm.verbose = int(opt.get("log_to_console"))
-    prm.detect_infeasibility = int(opt.get("pdhg_detect_infeasibility"))
-    prm.mixed_switch_tolerance = opt.get("pdhg_mixed_switch_tolerance")
-    prm.group_size_rows = opt.get("pdhg_lanes_rows")
-    prm.group_size_cols = opt.get("pdhg_lanes_cols")
-    prm.grid_blocks = opt.get("pdhg_grid_blocks")
-    prm.profile_kernels = int(opt.get("pdhg_profile_kernels"))
+    prm = _params(opt, lib)
     n, m = model.num_cols, model.num_rows
     x = np.zeros(n)
     rd = np.zeros(m)
@@ -349,6 +334,7 @@ def _params(opt: Options, lib) -> _Params:
     prm.group_size_cols = opt.get("pdhg_lanes_cols")
     prm.grid_blocks = opt.get("pdhg_grid_blocks")
     prm.profile_kernels = int(opt.get("pdhg_profile_kernels"))
+    prm.mixed_stall_checks = opt.get("pdhg_mixed_stall_checks")
     return prm
 
 

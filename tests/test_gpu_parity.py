@@ -185,3 +185,29 @@ def test_mixed_precision_against_oracle(rule):
         assert s.iterations > s.fp32_iterations  # the FP64 polish ran
         o = oracle.oracle_solve(lp, tolerance=tol)
         assert np.array_equal(_pattern(lp, s.col_value), _pattern(lp, o.col_value))
+
+
+def test_mixed_hand_over_keeps_the_restart_state():
+    """An early switch hands the FP32 level's whole restart state to FP64: the solve goes on
+    and meets the request."""
+    lp = lpgen.uniform_planted(2000, 5000, 10, seed=0)
+    tol = 1e-6
+    s = P.solve_pdhg(lp, _opts(pdhg_tolerance=tol, pdhg_precision="mixed",
+                               pdhg_stop_rule="relative_kkt", pdhg_mixed_switch_tolerance=1e-3))
+    assert s.status in ("optimal", "feasible"), s.message
+    assert 0 < s.fp32_iterations < s.iterations
+    r = oracle.oracle_evaluate(lp, s.col_value, _y_pdhg_sign(lp, s))
+    assert max(r["primal"], r["dual"], r["gap"]) <= tol
+
+
+def test_mixed_reaches_a_tolerance_below_plain_fp32():
+    """FP32 deltas about an FP64 anchor have no FP32 floor at 1e-8 (plain FP32 iterates stall
+    around 1e-5 to 1e-6 relative KKT); the answer meets the request either way."""
+    lp = lpgen.uniform_planted(2000, 5000, 10, seed=0)
+    tol = 1e-8
+    s = P.solve_pdhg(lp, _opts(pdhg_tolerance=tol, pdhg_precision="mixed",
+                               pdhg_stop_rule="relative_kkt"))
+    assert s.status in ("optimal", "feasible"), s.message
+    r = oracle.oracle_evaluate(lp, s.col_value, _y_pdhg_sign(lp, s))
+    assert max(r["primal"], r["dual"], r["gap"]) <= tol
+    print("fp32 iterations", s.fp32_iterations, "of", s.iterations)
