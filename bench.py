@@ -17,6 +17,19 @@ FP64, unscaled) through the library's C ABI.
           threads, on a bounded sample: setup + 20 iterations, extrapolated to the iteration
           count of this workload
 
+  batched  512 uneven LPs (m log-uniform on [50, 5,000], n = m U(1.5, 3), 5-15 nonzeros per
+          column, 10 % primal-infeasible; lpgen.uneven_batch, seed 3) solved to relative KKT
+          1e-6 by the batched engine in one call (sankhya_pdhg_gpu_batch_solve, host arrays in
+          and out): LPs/s, p50 / p99 / p99.9 submit-to-answer latency, certificates found, and
+          the same LPs solved one at a time by the plain FP64 single-LP path (a sample of every
+          8th LP) for the LPs/s ratio. Under torchrun the 512 LPs are sharded by nonzeros
+          (sih26_b200.shard) and the time is the maximum over ranks.
+  served  Poisson request streams (default 50 and 200 LPs/s for 4 s; LPs drawn from a seeded pool of
+          the served family, m log-uniform on [100, 50,000]) into a resident server that admits
+          requests between launches of its persistent kernels (continuous batching): LPs/s and
+          p50 / p99 / p99.9 arrival-to-answer latency, next to one-at-a-time FP64 solves of
+          the same pool. Rank 0 only.
+
 `--impl reference` times that CPU reference alone on the same workload and prints its line.
 With torchrun (N > 1) every rank solves its own replica of the LP (a single LP does not
 shard); the time is the maximum over ranks.
@@ -143,6 +156,176 @@ def cpu_reference_sample(lp, iterations):
     return kind, threads, setup, per_iteration
 
 
+def _percentiles(values):
+    import numpy as np
+
+    if not values:
+        return {"p50": None, "p99": None, "p99.9": None}
+    v = np.asarray(values, dtype=np.float64)
+    return {"p50": float(np.percentile(v, 50)), "p99": float(np.percentile(v, 99)),
+            "p99.9": float(np.percentile(v, 99.9))}
+
+
+def batched_leg(local, world, rank, dist, torch):
+    """512 uneven LPs through the batched engine (sharded over ranks), and a one-at-a-time
+    FP64 sample on rank 0."""
+    from sih26_b200 import lpgen, pdhg
+    from sih26_b200.shard import gather_by_index, shard_by_nnz
+
+    lps = lpgen.uneven_batch(count=512, m_lo=50, m_hi=5000, infeasible_fraction=0.1, seed=3)
+    mine = shard_by_nnz([lp.num_nonzeros for lp in lps], world)[rank]
+    opts = pdhg.Options(pdhg_tolerance=TOLERANCE, pdhg_stop_rule="relative_kkt",
+                        gpu_device=local)
+
+    def sync():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    pdhg.batch_solve([lps[k] for k in mine[:64]], opts)  # warm-up (module load, first launch)
+    sync()
+    t0 = time.perf_counter()
+    sols = pdhg.batch_solve([lps[k] for k in mine], opts)
+    sync()
+    wall = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([wall], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        wall = float(t.item())
+    local_out = {}
+    for k, s in zip(mine, sols):
+        rel = max(s.residuals["relative_primal"], s.residuals["relative_dual"],
+                  s.residuals["relative_gap"])
+        local_out[k] = (s.status, rel, s.solve_seconds, s.iterations)
+    allres = gather_by_index(local_out, dist)
+    if rank != 0:
+        return None
+    planted_infeasible = sum(lp.farkas_star is not None for lp in lps)
+    statuses = [allres[k][0] for k in range(len(lps))]
+    met = sum(1 for k in range(len(lps)) if lps[k].farkas_star is None
+              and statuses[k] in ("optimal", "feasible") and allres[k][1] <= TOLERANCE)
+    certified = sum(1 for k in range(len(lps)) if lps[k].farkas_star is not None
+                    and statuses[k] == "infeasible")
+    # one at a time, plain FP64, on every 8th LP (its feasible ones, and its infeasible ones
+    # with the certificate test that the single-LP path also runs)
+    sample = list(range(0, len(lps), 8))
+    one_rate = one_at_a_time([lps[k] for k in sample], local)
+    rate = len(lps) / wall
+    return {
+        "workload": "512 uneven LPs, m log-uniform [50, 5000], n = m U(1.5,3), 5-15 nnz/col, "
+                    "10% infeasible, seed 3, relative KKT 1e-6",
+        "lps": len(lps), "nonzeros": int(sum(lp.num_nonzeros for lp in lps)),
+        "value": rate, "unit": "LPs/s", "seconds": wall,
+        "latency_s": _percentiles([allres[k][2] for k in range(len(lps))]),
+        "met_tolerance": met, "feasible_lps": len(lps) - planted_infeasible,
+        "certified_infeasible": certified, "planted_infeasible": planted_infeasible,
+        "precision": "fp64",
+        "one_at_a_time_fp64": {"value": one_rate, "unit": "LPs/s",
+                               "sample": f"every 8th LP ({len(sample)}), once each"},
+        "speedup_vs_one_at_a_time": rate / one_rate,
+        "sharding": f"{world} rank(s), by nonzeros" if world > 1 else "single GPU",
+    }
+
+
+def served_family(count, seed):
+    """The served family: m log-uniform on [100, 50,000], otherwise as the batched one."""
+    import math
+
+    import numpy as np
+
+    from sih26_b200 import lpgen
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        m = int(round(math.exp(rng.uniform(math.log(100), math.log(50000)))))
+        n = int(round(m * rng.uniform(1.5, 3.0)))
+        out.append(lpgen.small_planted(m, n, 5, 15, rng, name=f"served{k}-{m}x{n}"))
+    return out
+
+
+def one_at_a_time(lps, local):
+    """LPs/s of the plain FP64 single-LP path, one LP after another (after one warm-up)."""
+    from sih26_b200 import pdhg
+
+    one = pdhg.Options(pdhg_tolerance=TOLERANCE, pdhg_stop_rule="relative_kkt",
+                       pdhg_precision="fp64", gpu_device=local)
+    pdhg.solve_pdhg(lps[0], one)
+    t0 = time.perf_counter()
+    for lp in lps:
+        pdhg.solve_pdhg(lp, one)
+    return len(lps) / (time.perf_counter() - t0)
+
+
+def served_leg(local, rates, seconds, chunk, pool_size=24, seed=5, drain_cap=90.0):
+    """A Poisson stream at each rate (LPs/s) for `seconds` into a resident server."""
+    import concurrent.futures as cf
+
+    import numpy as np
+
+    from sih26_b200 import pdhg
+
+    pool = served_family(pool_size, seed)
+    base_rate = one_at_a_time(pool, local)
+    opts = pdhg.Options(pdhg_tolerance=TOLERANCE, pdhg_stop_rule="relative_kkt",
+                        gpu_device=local)
+    out = []
+    for rate in rates:
+        rng = np.random.default_rng(seed + 1)
+        arrivals = []
+        t = 0.0
+        while True:
+            t += rng.exponential(1.0 / rate)
+            if t > seconds:
+                break
+            arrivals.append(t)
+        picks = rng.integers(0, pool_size, len(arrivals))
+        latency, statuses = {}, {}
+        with pdhg.Server(device=local, chunk_attempts=chunk) as srv, \
+                cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
+            srv.solve_all([pool[0]], opts)  # warm-up
+            futures, tickets = {}, {}
+            nxt = 0
+            t0 = time.perf_counter()
+            while len(latency) < len(arrivals):
+                now = time.perf_counter() - t0
+                if now > seconds + drain_cap:
+                    break
+                while nxt < len(arrivals) and arrivals[nxt] <= now:
+                    futures[nxt] = ex.submit(srv.submit, pool[picks[nxt]], opts)
+                    nxt += 1
+                for k in [k for k, f in futures.items() if f.done()]:
+                    tickets[k] = futures.pop(k).result()
+                active, waiting, _ = srv.step()
+                done_at = time.perf_counter() - t0
+                for k in list(tickets):
+                    r = srv.result(tickets[k])
+                    if r is not None:
+                        latency[k] = done_at - arrivals[k]
+                        statuses[k] = r.status
+                        del tickets[k]
+                if active == 0 and waiting == 0 and not tickets:
+                    time.sleep(0.0005)
+            span = time.perf_counter() - t0
+        done = len(latency)
+        served_rate = done / span if span > 0 else None
+        out.append({
+            "workload": f"Poisson arrivals at {rate:g} LPs/s for {seconds:g} s, LPs drawn from "
+                        f"a pool of {pool_size} of the served family (m log-uniform [100, "
+                        f"50000], n = m U(1.5,3), 5-15 nnz/col, seed {seed}), relative KKT 1e-6",
+            "offered_rate": rate, "requests": len(arrivals), "completed": done,
+            "optimal_or_feasible": sum(1 for v in statuses.values()
+                                       if v in ("optimal", "feasible")),
+            "value": served_rate, "unit": "LPs/s", "span_s": span,
+            "latency_s": _percentiles(list(latency.values())), "chunk_attempts": chunk,
+            "precision": "fp64",
+            "one_at_a_time_fp64": {"value": base_rate, "unit": "LPs/s",
+                                   "sample": f"the {pool_size} LPs of the pool, once each"},
+            "speedup_vs_one_at_a_time": (served_rate / base_rate) if served_rate else None,
+        })
+    return out
+
+
 def make_workload():
     from sih26_b200 import lpgen
 
@@ -267,6 +450,11 @@ def run_ours(args):
                           f"iterations ({per_it * 1e3:.2f} ms each), extrapolated to the "
                           f"{fp64.iterations} iterations the FP64 GPU leg needed")}
     launches = int(statistics.mean(s.kernel_launches for s in sols))
+    batched = None if args.no_batched else batched_leg(local, world, rank, dist, torch)
+    served = None
+    if rank == 0 and not args.no_served:
+        rates = [float(r) for r in args.served_rates.split(",") if r]
+        served = served_leg(local, rates, args.served_seconds, args.served_chunk)
     if rank == 0:
         line = {
             "metric": "time-to-rel-KKT 1e-6 (s), FP32-mixed", "value": dev, "unit": "s",
@@ -296,6 +484,8 @@ def run_ours(args):
                     "d2h_bytes_per_step": last.d2h_bytes},
             "gpu_launches": launches,
             "clocks": clocks.summary(),
+            "batched": batched,
+            "served": served,
         }
         print(json.dumps(line))
     if dist is not None:
@@ -309,6 +499,14 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-batched", action="store_true", help="skip the 512-LP batched leg")
+    ap.add_argument("--no-served", action="store_true", help="skip the served-stream leg")
+    ap.add_argument("--served-rates", default="50,200",
+                    help="Poisson rates, LPs/s, comma-separated (the served family's full "
+                         "study is 200,1000,5000 for 60 s)")
+    ap.add_argument("--served-seconds", type=float, default=4.0, help="arrival window, s")
+    ap.add_argument("--served-chunk", type=int, default=512,
+                    help="attempts per LP per server launch")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("at least 3 warm-up steps")

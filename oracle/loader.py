@@ -242,6 +242,15 @@ def ref_farkas_check(lp, y) -> tuple[bool, str]:
     return rc == 1, why.value.decode()
 
 
+def ref_ray_check(lp, d) -> tuple[bool, str]:
+    """ray_proves_unbounded (src/core/certificate.cpp:121-218) of the reference build."""
+    pin = _Pinned(lp)
+    d = np.ascontiguousarray(d, dtype=np.float64)
+    why = C.create_string_buffer(512)
+    rc = _ref().ref_ray_check(C.byref(pin.s), _p(d, _f64p), why, 512)
+    return rc == 1, why.value.decode()
+
+
 def ref_read_model(path):
     """Reads an MPS/LP file with the reference reader into an lpgen.LP."""
     from sih26_b200.lpgen import LP

@@ -14,12 +14,10 @@
 // code and summation order whatever else is in the batch: a result is the same alone and in
 // the mix.
 //
-// Primal infeasibility: at every evaluation the dual movement since the last restart,
-// f = -Dr (y - y_r) in original units, is tested as a Farkas certificate in the sense of
-// src/core/certificate.cpp:29-119 (rows aggregate to S = sum f_i * bound chosen by the sign
-// of f_i; the column box allows at most M = max d.x with d = A'f; S > M proves
-// infeasibility). For a feasible LP S <= M for every f, so the test cannot fire on one;
-// the host re-checks every certificate exactly before reporting it.
+// Infeasibility and unboundedness: at every evaluation the dual movement since the last
+// restart is tested as a Farkas certificate and the last primal step as a primal ray (see
+// certificate_test in pdhg_kernels.cuh); the host re-checks every candidate exactly with the
+// reference's rules (src/core/certificate.cpp) before reporting it.
 #pragma once
 
 #include <cooperative_groups.h>
@@ -40,6 +38,7 @@ struct BatchSlot {
   double* red_out;      // report: min-space reduced costs, permuted
   double* y_out;        // report: unscaled y (PDHG sign), permuted
   double* farkas_out;   // certificate f (reference sign, normalised), permuted
+  double* ray_out;      // primal ray r (normalised), permuted
 };
 
 // One block.
@@ -102,42 +101,6 @@ struct ClusterGroup {
   }
 };
 
-// sum_k A'_jk (y - y_r)_k, the column side of the Farkas candidate
-struct DiffGather {
-  const double* y;
-  const double* yr;
-  __device__ __forceinline__ void add(double (&s)[1], double a, int k) const {
-    s[0] += a * (ld(y + k) - ld(yr + k));
-  }
-  __device__ __forceinline__ double product(int, double a, int k) const {
-    return a * (ld(y + k) - ld(yr + k));
-  }
-};
-
-// Column terms of the Farkas test for d = A'f = -(A'_scaled (y - y_r)) / Dc.
-// slots: 0 max |d|, 1 reachable M, 2 max |d| over columns leaning on a missing bound
-struct FarkasCol {
-  const double* dc;
-  const double* cl0;
-  const double* cu0;
-  struct In {
-    double dc, lo, hi;
-  };
-  __device__ __forceinline__ In load(int j) const {
-    return In{__ldg(dc + j), __ldg(cl0 + j), __ldg(cu0 + j)};
-  }
-  __device__ __forceinline__ void apply(int j, const double (&s)[1], const In& v,
-                                        double (&acc)[3]) const {
-    const double d = -s[0] / v.dc;
-    acc[0] = dmax(acc[0], fabs(d));
-    if (d > 0.0) {
-      if (finite_bound(v.hi)) acc[1] += d * v.hi; else acc[2] = dmax(acc[2], d);
-    } else if (d < 0.0) {
-      if (finite_bound(v.lo)) acc[1] += d * v.lo; else acc[2] = dmax(acc[2], -d);
-    }
-  }
-};
-
 // Norm estimate of the LP's scaled matrix (src/la/scaling.cpp:161-194):
 // v = S.xavg holds the random start, u = S.yavg is scratch.
 template <class Grp>
@@ -178,19 +141,27 @@ __device__ __noinline__ void group_evaluate(const BatchSlot& B, Ctrl& c, double*
   const State<double>& S = B.S;
   const int rank = grp.rank();
   const int base = rank * kThreads + threadIdx.x, stride = Grp::kSize * kThreads;
-  const int cur = c.cur;
+  const int cur = c.cur, prev = cur_prev_slot(c);
   const bool has_average = c.averaged > 0;
   const double count = (double)c.averaged;
-  // E1 + Farkas rows. slots: 0 |x-x_r|^2, 1 |y-y_r|^2, 2 S, 3 max|f|, 4 max|f| leaning on a
-  // missing row bound
-  double e1[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  const bool test_cert = c.farkas_cooldown == 0 && (c.evaluations % kCertEvery) == kCertEvery - 1;
+  // E1: running sums and averages, the movement since the last restart (mv) and the
+  // certificates' row / column terms (ec, see certificate_test)
+  double mv[2] = {0.0, 0.0};
+  double ec[kCertSlots];
+#pragma unroll
+  for (int s = 0; s < kCertSlots; ++s) ec[s] = 0.0;
   for (int j = base; j < P.n; j += stride) {
     const double xo = ld(S.x[cur] + j);
     const double xs = S.xsum[j] + (c.pending ? xo : 0.0);
     S.xsum[j] = xs;
     S.xavg[j] = has_average ? xs / count : 0.0;
     const double d = xo - ld(S.xr + j);
-    e1[0] += d * d;
+    mv[0] += d * d;
+    if (test_cert) {
+      const double r = __ldg(P.dc + j) * (xo - ld(S.x[prev] + j));
+      ray_col_terms(r, __ldg(P.cl0 + j), __ldg(P.cu0 + j), __ldg(P.c0 + j), ec);
+    }
   }
   for (int i = base; i < P.m; i += stride) {
     const double yo = ld(S.y[cur] + i);
@@ -198,17 +169,11 @@ __device__ __noinline__ void group_evaluate(const BatchSlot& B, Ctrl& c, double*
     S.ysum[i] = ys;
     S.yavg[i] = has_average ? ys / count : 0.0;
     const double d = yo - ld(S.yr + i);
-    e1[1] += d * d;
-    const double f = -__ldg(P.dr + i) * d;
-    const double lo = __ldg(P.rl0 + i), hi = __ldg(P.ru0 + i);
-    e1[3] = dmax(e1[3], fabs(f));
-    if (f > 0.0) {
-      if (finite_bound(lo)) e1[2] += f * lo; else e1[4] = dmax(e1[4], f);
-    } else if (f < 0.0) {
-      if (finite_bound(hi)) e1[2] += f * hi; else e1[4] = dmax(e1[4], -f);
-    }
+    mv[1] += d * d;
+    if (test_cert) farkas_row_terms(-__ldg(P.dr + i) * d, __ldg(P.rl0 + i), __ldg(P.ru0 + i), ec);
   }
-  grp.template reduce<5, (1u << 3) | (1u << 4)>(e1, sh);
+  grp.template reduce<2, 0u>(mv, sh);
+  if (test_cert) grp.template reduce<kCertSlots, kCertMaxMask>(ec, sh);
   // E2: residual terms of both candidates (FP64 values)
   double acc[kEvalSlots];
 #pragma unroll
@@ -220,39 +185,45 @@ __device__ __noinline__ void group_evaluate(const BatchSlot& B, Ctrl& c, double*
   run_phase<2, kEvalSlots>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pat,
                            Gather2<double, double>{S.y[cur], S.yavg}, ce, acc, stream, rank);
   grp.template reduce<kEvalSlots, kEvalMaxMask>(acc, sh);
-  // Farkas columns
-  double fk[3] = {0.0, 0.0, 0.0};
-  const bool test_farkas = c.farkas_cooldown == 0 && e1[3] > 0.0;
-  if (test_farkas) {
-    run_phase<1, 3>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pat, DiffGather{S.y[cur], S.yr},
+  // the certificates' matrix terms: A'(y - y_r) and A (x_k - x_{k-1})
+  double fk[3] = {0.0, 0.0, 0.0}, rr[2] = {0.0, 0.0};
+  if (test_cert) {
+    run_phase<1, 3>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pat, DiffGather<double, double>{S.y[cur], S.yr},
                     FarkasCol{P.dc, P.cl0, P.cu0}, fk, stream, rank);
-    grp.template reduce<3, (1u << 0) | (1u << 2)>(fk, sh);
+    grp.template reduce<3, kFarkasColMaxMask>(fk, sh);
+    run_phase<1, 2>(P.A.ptr, P.A.idx, P.A.val64, P.pa, DiffGather<double, double>{S.x[cur], S.x[prev]},
+                    RayRow{P.dr, P.rl0, P.ru0}, rr, stream, rank);
+    grp.template reduce<2, 3u>(rr, sh);
   }
   // every block takes the same decisions from the same totals
   if (threadIdx.x == 0) {
-    const double mv[2] = {e1[0], e1[1]};
+    const Ctrl before = c;
     evaluation_decision(c, acc, mv, has_average, flags);
     flags[3] = 0;
     if (c.farkas_cooldown > 0) --c.farkas_cooldown;
-    if (test_farkas && c.state != kConverged) {
-      const double Sn = e1[2] / e1[3], Mn = fk[1] / e1[3];
-      const double margin = Sn - Mn;
-      const bool rows_ok = e1[4] <= 1e-9 * e1[3];
-      const bool cols_ok = fk[2] <= 1e-9 * dmax(fk[0], 1e-300);
-      c.farkas_margin = margin;
-      if (rows_ok && cols_ok && margin > 1e-6 * dmax(1.0, dmax(fabs(Sn), fabs(Mn)))) {
-        c.state = kInfeasible;
-        flags[1] = 0;  // keep the restart anchor: the certificate is read from it
-        flags[3] = 1;
+    if (test_cert && c.state != kConverged) {
+      const int kind = certificate_test(c, ec, fk, rr);
+      if (kind != 0) {
+        // keep the restart anchor and step state: the certificate is read from them, and the
+        // LP resumes from them if the host turns it down
+        const double margin = c.farkas_margin;
+        c = before;
+        ++c.evaluations;
+        c.pending = 0;
+        c.farkas_margin = margin;
+        c.state = kind == 1 ? kInfeasible : kUnbounded;
+        flags[0] = flags[1] = flags[2] = 0;
+        flags[3] = kind;
       }
     }
   }
   __syncthreads();
-  const double fmax = e1[3];
+  const double scale = flags[3] == 1 ? ec[1] : ec[3];
   // E3: certificate, best point, restart reset
   if (flags[0] || flags[1] || flags[3]) {
     for (int j = base; j < P.n; j += stride) {
       const double xo = ld(S.x[cur] + j);
+      if (flags[3] == 2) B.ray_out[j] = __ldg(P.dc + j) * (xo - ld(S.x[prev] + j)) / scale;
       if (flags[0]) S.best_x[j] = flags[2] ? S.xavg[j] : xo;
       if (flags[1]) {
         S.xr[j] = S.x[cur][j];
@@ -261,7 +232,7 @@ __device__ __noinline__ void group_evaluate(const BatchSlot& B, Ctrl& c, double*
     }
     for (int i = base; i < P.m; i += stride) {
       const double yo = ld(S.y[cur] + i);
-      if (flags[3]) B.farkas_out[i] = -__ldg(P.dr + i) * (yo - ld(S.yr + i)) / fmax;
+      if (flags[3] == 1) B.farkas_out[i] = -__ldg(P.dr + i) * (yo - ld(S.yr + i)) / scale;
       if (flags[0]) S.best_y[i] = flags[2] ? S.yavg[i] : yo;
       if (flags[1]) {
         S.yr[i] = S.y[cur][i];
@@ -358,7 +329,7 @@ __device__ inline void run_instance(const BatchSlot& B, Ctrl& c, double* sh, dou
     if (c.state == kNeedEval) group_evaluate(B, c, sh, stream, flags, grp);
   }
   if (c.state == kConverged || c.state == kIterationLimit || c.state == kTimeLimit ||
-      c.state == kInfeasible) {
+      c.state == kInfeasible || c.state == kUnbounded) {
     group_report(B, c, sh, stream, grp);
   }
   if (threadIdx.x == 0 && rank == 0) *S.ctrl = c;

@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -22,6 +23,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "batch_kernels.cuh"
@@ -42,49 +44,6 @@ extern thread_local std::string g_last_error;
 namespace {
 
 using Clock = std::chrono::steady_clock;
-
-// ---- host re-check of a certificate (the test of src/core/certificate.cpp:29-119) -------
-bool farkas_holds(const sankhya_pdhg_problem& p, const std::vector<double>& y) {
-  const int m = p.num_rows, n = p.num_cols;
-  bool any = false;
-  double required = 0.0;
-  for (int i = 0; i < m; ++i) {
-    if (y[i] != 0.0) any = true;
-    if (y[i] > 0.0) {
-      if (!host_finite_bound(p.row_lower[i])) return false;
-      required += y[i] * p.row_lower[i];
-    } else if (y[i] < 0.0) {
-      if (!host_finite_bound(p.row_upper[i])) return false;
-      required += y[i] * p.row_upper[i];
-    }
-  }
-  if (!any) return false;
-  std::vector<double> d(n, 0.0);
-  double scale = 0.0;
-  for (int j = 0; j < n; ++j) {
-    double sum = 0.0;
-    for (int k = p.col_starts[j]; k < p.col_starts[j + 1]; ++k) {
-      const double term = p.values[k] * y[p.row_indices[k]];
-      sum += term;
-      scale = std::max(scale, std::fabs(term));
-    }
-    d[j] = sum;
-  }
-  double reachable = 0.0;
-  for (int j = 0; j < n; ++j) {
-    if (d[j] > 1e-11 * std::max(1.0, scale)) {
-      if (!host_finite_bound(p.col_upper[j])) return false;
-      reachable += d[j] * p.col_upper[j];
-    } else if (d[j] < -1e-11 * std::max(1.0, scale)) {
-      if (!host_finite_bound(p.col_lower[j])) return false;
-      reachable += d[j] * p.col_lower[j];
-    }
-  }
-  const double margin = required - reachable;
-  const double comparison =
-      std::max({1.0, std::fabs(required), std::fabs(reachable), scale});
-  return margin > 1e-7 * comparison;
-}
 
 // Offsets of one LP's arrays inside its device image (bytes, 256-byte aligned).
 struct Layout {
@@ -118,7 +77,7 @@ struct Job {
     PartOff pa, pat;
     size_t c, cl, cu, rl, ru, dr, dc, c0, cl0, cu0, rl0, ru0;
     size_t x0, x1, y0, y1, ax0, ax1, xsum, ysum, xr, yr, xavg, yavg, best_x, best_y;
-    size_t x_out, red_out, y_out, farkas_out;
+    size_t x_out, red_out, y_out, farkas_out, ray_out;
   } off{};
   Ctrl ctrl0{};
   // lifecycle
@@ -133,7 +92,7 @@ struct Job {
   // result
   int status = SANKHYA_PDHG_NOT_SOLVED;
   Ctrl last{};
-  std::vector<double> x, row_dual, col_dual, farkas;
+  std::vector<double> x, row_dual, col_dual, farkas, ray;
 };
 
 template <class T>
@@ -216,7 +175,7 @@ void prepare(Job& J, const sankhya_pdhg_problem& p, const sankhya_pdhg_params& p
   o.pa = part_off(pa);
   o.pat = part_off(pat);
   for (size_t* f : {&o.c, &o.cl, &o.cu, &o.dc, &o.c0, &o.cl0, &o.cu0, &o.x0, &o.x1, &o.xsum,
-                    &o.xr, &o.xavg, &o.best_x, &o.x_out, &o.red_out})
+                    &o.xr, &o.xavg, &o.best_x, &o.x_out, &o.red_out, &o.ray_out})
     *f = L.put(n * 8);
   for (size_t* f : {&o.rl, &o.ru, &o.dr, &o.rl0, &o.ru0, &o.y0, &o.y1, &o.ax0, &o.ax1, &o.ysum,
                     &o.yr, &o.yavg, &o.best_y, &o.y_out, &o.farkas_out})
@@ -415,6 +374,7 @@ BatchSlot relocate(const Job& J, unsigned char* base, Ctrl* ctrl) {
   b.red_out = D(o.red_out);
   b.y_out = D(o.y_out);
   b.farkas_out = D(o.farkas_out);
+  b.ray_out = D(o.ray_out);
   return b;
 }
 
@@ -507,6 +467,8 @@ void finish_job(Server& s, Job& J, const Ctrl& c) {
                         f.gap_as_verified <= 1e-9 && f.complementarity <= 1e-6;
   if (c.state == kInfeasible) {
     J.status = SANKHYA_PDHG_INFEASIBLE;
+  } else if (c.state == kUnbounded) {
+    J.status = SANKHYA_PDHG_UNBOUNDED;
   } else if (c.converged) {
     J.status = standard ? SANKHYA_PDHG_OPTIMAL : SANKHYA_PDHG_FEASIBLE;
   } else {
@@ -518,6 +480,11 @@ void finish_job(Server& s, Job& J, const Ctrl& c) {
                   "primal infeasible: Farkas certificate from the dual movement after %lld "
                   "iterations (normalised margin %.3e), checked on the original model",
                   c.iteration, c.farkas_margin);
+  } else if (J.status == SANKHYA_PDHG_UNBOUNDED) {
+    std::snprintf(msg, sizeof msg,
+                  "unbounded: primal ray from the last step after %lld iterations, checked on "
+                  "the original model",
+                  c.iteration);
   } else {
     std::snprintf(msg, sizeof msg,
                   "%lld iterations and %lld restarts; relative primal %.3e, dual %.3e, gap %.3e",
@@ -582,21 +549,26 @@ static std::vector<int> settle(Server& s, const std::vector<int>& list, const Ct
     Job& J = *s.slot_job[slot];
     if (c.state == kDeviceError) throw Failure{SANKHYA_GPU_DEVICE_TIMEOUT, "batch kernel error"};
     bool done = c.state == kConverged || c.state == kIterationLimit || c.state == kTimeLimit;
-    if (c.state == kInfeasible) {
-      std::vector<double> f(J.m);
-      if (J.m)
-        SIH26_SCUDA(cudaMemcpy(f.data(), s.pool + J.pool_offset + J.off.farkas_out, J.m * 8,
-                               cudaMemcpyDeviceToHost), SANKHYA_GPU_COPY_FAILED);
-      std::vector<double> y(J.m);
-      for (int t = 0; t < J.m; ++t) y[J.row_perm[t]] = f[t];
-      if (farkas_holds(J.view, y)) {
-        J.farkas = y;
+    if (c.state == kInfeasible || c.state == kUnbounded) {
+      const bool rows = c.state == kInfeasible;
+      const int len = rows ? J.m : J.n;
+      std::vector<double> h(len), v(len);
+      if (len)
+        SIH26_SCUDA(cudaMemcpy(h.data(),
+                               s.pool + J.pool_offset + (rows ? J.off.farkas_out : J.off.ray_out),
+                               len * 8, cudaMemcpyDeviceToHost), SANKHYA_GPU_COPY_FAILED);
+      const std::vector<int>& perm = rows ? J.row_perm : J.col_perm;
+      for (int t = 0; t < len; ++t) v[perm[t]] = h[t];
+      bool ok = rows ? farkas_holds(J.view, v) : ray_holds(J.view, v);
+      if (!ok && !rows && repair_ray(J.view, v)) ok = ray_holds(J.view, v);
+      if (ok) {
+        (rows ? J.farkas : J.ray) = v;
         done = true;
       } else {
         // not a proof after all: carry on, and give the test a rest
         Ctrl r = c;
         r.state = kRunning;
-        r.farkas_cooldown = 8;
+        r.farkas_cooldown = kCertCooldown;
         SIH26_SCUDA(cudaMemcpy(s.d_ctrls + slot, &r, sizeof(Ctrl), cudaMemcpyHostToDevice),
                     SANKHYA_GPU_COPY_FAILED);
       }
@@ -851,6 +823,7 @@ int sankhya_pdhg_server_result(sankhya_pdhg_server* server, int64_t ticket,
   if (r->col_dual && !J.col_dual.empty()) std::memcpy(r->col_dual, J.col_dual.data(), J.n * 8);
   if (r->row_dual && !J.row_dual.empty()) std::memcpy(r->row_dual, J.row_dual.data(), J.m * 8);
   if (r->farkas_dual && !J.farkas.empty()) std::memcpy(r->farkas_dual, J.farkas.data(), J.m * 8);
+  if (r->primal_ray && !J.ray.empty()) std::memcpy(r->primal_ray, J.ray.data(), J.n * 8);
   r->setup_seconds = std::max(0.0, J.admit_time - J.submit_time);
   r->solve_seconds = std::max(0.0, J.finish_time - J.admit_time);
   r->total_seconds = std::max(0.0, J.finish_time - J.submit_time);
@@ -876,9 +849,32 @@ int sankhya_pdhg_gpu_batch_solve(const sankhya_pdhg_problem* problems, int32_t c
   sankhya_pdhg_server* server = nullptr;
   int rc = sankhya_pdhg_server_create(&cfg, &server);
   if (rc != SANKHYA_GPU_SUCCESS) return rc;
+  // host preparation (validation, scaling, layout) of the LPs on several threads; submit is
+  // thread-safe and the results do not depend on the order of admission
   std::vector<int64_t> tickets(count);
-  for (int k = 0; k < count && rc == SANKHYA_GPU_SUCCESS; ++k)
-    rc = sankhya_pdhg_server_submit(server, &problems[k], params, &tickets[k]);
+  std::vector<int> codes(count, SANKHYA_GPU_SUCCESS);
+  std::vector<std::string> errors(count);
+  {
+    const int workers = std::max(1, std::min<int>(count, std::min(16u, std::max(1u, std::thread::hardware_concurrency()))));
+    std::atomic<int> next{0};
+    std::vector<std::thread> pool;
+    for (int w = 0; w < workers; ++w) {
+      pool.emplace_back([&] {
+        for (int k = next++; k < count; k = next++) {
+          codes[k] = sankhya_pdhg_server_submit(server, &problems[k], params, &tickets[k]);
+          if (codes[k] != SANKHYA_GPU_SUCCESS) errors[k] = sih26::g_last_error;
+        }
+      });
+    }
+    for (auto& t : pool) t.join();
+  }
+  for (int k = 0; k < count; ++k) {
+    if (codes[k] != SANKHYA_GPU_SUCCESS) {
+      rc = codes[k];
+      sih26::g_last_error = errors[k];
+      break;
+    }
+  }
   int32_t active = 0, waiting = 0, finished = 0;
   while (rc == SANKHYA_GPU_SUCCESS) {
     rc = sankhya_pdhg_server_step(server, &active, &waiting, &finished);

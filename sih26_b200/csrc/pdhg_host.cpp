@@ -12,6 +12,184 @@ namespace sih26 {
 
 bool host_finite_bound(double v) { return !(std::isinf(v) || std::fabs(v) >= 1e30); }
 
+// farkas_proves_infeasible (src/core/certificate.cpp:29-119) on the ABI's problem: every
+// multiplier leans on a bound its row has; d = A'y; the column box reaches at most
+// `reachable`; the rows require `required`; a margin beyond 1e-7 (kPrimalFeasibility) of the
+// comparison scale proves the LP infeasible. Coefficients of d at 1e-11 (kZeroDrop) of the
+// term scale count as zero.
+bool farkas_holds(const sankhya_pdhg_problem& p, const std::vector<double>& y) {
+  const int m = p.num_rows, n = p.num_cols;
+  bool any = false;
+  double required = 0.0;
+  for (int i = 0; i < m; ++i) {
+    if (y[i] != 0.0) any = true;
+    if (y[i] > 0.0) {
+      if (!host_finite_bound(p.row_lower[i])) return false;
+      required += y[i] * p.row_lower[i];
+    } else if (y[i] < 0.0) {
+      if (!host_finite_bound(p.row_upper[i])) return false;
+      required += y[i] * p.row_upper[i];
+    }
+  }
+  if (!any) return false;
+  std::vector<double> d(n, 0.0);
+  double scale = 0.0;
+  for (int j = 0; j < n; ++j) {
+    double sum = 0.0;
+    for (int k = p.col_starts[j]; k < p.col_starts[j + 1]; ++k) {
+      const double term = p.values[k] * y[p.row_indices[k]];
+      sum += term;
+      scale = std::max(scale, std::fabs(term));
+    }
+    d[j] = sum;
+  }
+  double reachable = 0.0;
+  for (int j = 0; j < n; ++j) {
+    if (d[j] > 1e-11 * std::max(1.0, scale)) {
+      if (!host_finite_bound(p.col_upper[j])) return false;
+      reachable += d[j] * p.col_upper[j];
+    } else if (d[j] < -1e-11 * std::max(1.0, scale)) {
+      if (!host_finite_bound(p.col_lower[j])) return false;
+      reachable += d[j] * p.col_lower[j];
+    }
+  }
+  const double margin = required - reachable;
+  const double comparison = std::max({1.0, std::fabs(required), std::fabs(reachable), scale});
+  return margin > 1e-7 * comparison;
+}
+
+// ray_proves_unbounded (src/core/certificate.cpp:121-218) for an LP: the direction moves no
+// column against a bound it has (beyond 1e-7 of its largest entry), moves no row activity
+// against a bound it has (beyond 1e-7 of the term scale), and improves the min-space cost by
+// more than 1e-7 of the cost-term scale per unit step.
+bool ray_holds(const sankhya_pdhg_problem& p, const std::vector<double>& d) {
+  const int m = p.num_rows, n = p.num_cols;
+  double magnitude = 0.0;
+  for (int j = 0; j < n; ++j) magnitude = std::max(magnitude, std::fabs(d[j]));
+  if (magnitude == 0.0) return false;
+  const double moving = 1e-7 * magnitude;
+  for (int j = 0; j < n; ++j) {
+    if (d[j] > moving && host_finite_bound(p.col_upper[j])) return false;
+    if (d[j] < -moving && host_finite_bound(p.col_lower[j])) return false;
+  }
+  std::vector<double> activity(m, 0.0);
+  double scale = 0.0;
+  for (int j = 0; j < n; ++j) {
+    if (d[j] == 0.0) continue;
+    for (int k = p.col_starts[j]; k < p.col_starts[j + 1]; ++k) {
+      const double term = p.values[k] * d[j];
+      activity[p.row_indices[k]] += term;
+      scale = std::max(scale, std::fabs(term));
+    }
+  }
+  const double row_moving = 1e-7 * std::max(1.0, scale);
+  for (int i = 0; i < m; ++i) {
+    if (activity[i] > row_moving && host_finite_bound(p.row_upper[i])) return false;
+    if (activity[i] < -row_moving && host_finite_bound(p.row_lower[i])) return false;
+  }
+  const double sense = p.maximize ? -1.0 : 1.0;
+  double improvement = 0.0, cost_scale = 0.0;
+  for (int j = 0; j < n; ++j) {
+    const double term = sense * p.cost[j] * d[j];
+    improvement += term;
+    cost_scale = std::max(cost_scale, std::fabs(term));
+  }
+  return improvement < -1e-7 * std::max(1.0, cost_scale);
+}
+
+// Repairs a primal-ray candidate before the exact check. Restarted PDHG on an unbounded LP
+// drives the primal weight to its floor, so the dual settles slowly and the last step still
+// carries a small movement of the bounded part (a few 1e-6 of the ray) -- above the checker's
+// 1e-7. The repair keeps the columns that move by more than 1e-4 of the largest move, drops
+// the rest, and projects the kept part onto the null space of the rows it would push against
+// a finite bound (modified Gram-Schmidt over those rows), so those activities stay put. Any
+// vector that passes ray_holds proves unboundedness, so the repair cannot produce a false
+// proof; it returns false when the support is larger than kMaxSupport columns.
+bool repair_ray(const sankhya_pdhg_problem& p, std::vector<double>& d) {
+  constexpr int kMaxSupport = 256;
+  const int n = p.num_cols;
+  double mag = 0.0;
+  for (int j = 0; j < n; ++j) mag = std::max(mag, std::fabs(d[j]));
+  if (mag == 0.0) return false;
+  std::vector<int> S;
+  for (int j = 0; j < n; ++j) {
+    if (std::fabs(d[j]) > 1e-4 * mag) S.push_back(j);
+    if (static_cast<int>(S.size()) > kMaxSupport) return false;
+  }
+  const int k = static_cast<int>(S.size());
+  // the rows the support touches, their activity along d, and, as dense rows over the
+  // support, those whose activity must stay put: a finite bound on the side the activity moves
+  // towards (or either side, for a move at rounding size)
+  std::vector<int> row_slot(p.num_rows, -1);
+  std::vector<int> touched;
+  std::vector<double> act;
+  for (int s = 0; s < k; ++s) {
+    const int j = S[s];
+    for (int t = p.col_starts[j]; t < p.col_starts[j + 1]; ++t) {
+      const int i = p.row_indices[t];
+      if (row_slot[i] < 0) {
+        row_slot[i] = static_cast<int>(touched.size());
+        touched.push_back(i);
+        act.push_back(0.0);
+      }
+      act[row_slot[i]] += p.values[t] * d[j];
+    }
+  }
+  double act_max = 0.0;
+  for (double v : act) act_max = std::max(act_max, std::fabs(v));
+  const double thr = 1e-6 * act_max;
+  std::vector<int> keep_slot(touched.size(), -1);
+  std::vector<std::vector<double>> rows;
+  for (size_t r = 0; r < touched.size(); ++r) {
+    const int i = touched[r];
+    const bool up_blocked = host_finite_bound(p.row_upper[i]) && act[r] >= -thr;
+    const bool down_blocked = host_finite_bound(p.row_lower[i]) && act[r] <= thr;
+    if (up_blocked || down_blocked) {
+      keep_slot[r] = static_cast<int>(rows.size());
+      rows.emplace_back(k, 0.0);
+    }
+  }
+  for (int s = 0; s < k; ++s) {
+    const int j = S[s];
+    for (int t = p.col_starts[j]; t < p.col_starts[j + 1]; ++t) {
+      const int slot = keep_slot[row_slot[p.row_indices[t]]];
+      if (slot >= 0) rows[slot][s] = p.values[t];
+    }
+  }
+  // orthonormal basis of the rows' span (modified Gram-Schmidt, rank-revealing threshold)
+  std::vector<std::vector<double>> basis;
+  for (auto& r : rows) {
+    double n0 = 0.0;
+    for (double v : r) n0 += v * v;
+    n0 = std::sqrt(n0);
+    if (n0 == 0.0) continue;
+    for (const auto& q : basis) {
+      double dot = 0.0;
+      for (int s = 0; s < k; ++s) dot += q[s] * r[s];
+      for (int s = 0; s < k; ++s) r[s] -= dot * q[s];
+    }
+    double n1 = 0.0;
+    for (double v : r) n1 += v * v;
+    n1 = std::sqrt(n1);
+    if (n1 <= 1e-10 * n0) continue;
+    for (double& v : r) v /= n1;
+    basis.push_back(std::move(r));
+    if (static_cast<int>(basis.size()) == k) return false;  // no null space left
+  }
+  std::vector<double> ds(k);
+  for (int s = 0; s < k; ++s) ds[s] = d[S[s]];
+  for (int pass = 0; pass < 2; ++pass) {  // twice, for the rounding of the first pass
+    for (const auto& q : basis) {
+      double dot = 0.0;
+      for (int s = 0; s < k; ++s) dot += q[s] * ds[s];
+      for (int s = 0; s < k; ++s) ds[s] -= dot * q[s];
+    }
+  }
+  std::fill(d.begin(), d.end(), 0.0);
+  for (int s = 0; s < k; ++s) d[S[s]] = ds[s];
+  return true;
+}
+
 static std::string fmtd(const char* f, long long a, long long b = 0) {
   char buf[256];
   std::snprintf(buf, sizeof buf, f, a, b);

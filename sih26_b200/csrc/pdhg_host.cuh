@@ -20,6 +20,14 @@ struct Failure {
 
 bool host_finite_bound(double v);
 
+// The reference's certificate checks (src/core/certificate.cpp:29-119 and :121-218) on the
+// original problem: every certificate is re-checked with these before it is reported.
+bool farkas_holds(const sankhya_pdhg_problem& p, const std::vector<double>& y);
+bool ray_holds(const sankhya_pdhg_problem& p, const std::vector<double>& d);
+// Cleans a primal-ray candidate taken from PDHG iterates (see pdhg_host.cpp); false when it
+// cannot. The result still has to pass ray_holds.
+bool repair_ray(const sankhya_pdhg_problem& p, std::vector<double>& d);
+
 // Structural checks of the C-ABI input (sizes, pointers, CSC well-formedness). Throws Failure
 // with SANKHYA_GPU_INVALID_ARGUMENT; these are inputs the reference's frozen SparseMatrix can
 // never hold.

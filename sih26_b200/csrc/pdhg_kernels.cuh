@@ -46,7 +46,8 @@ enum : int {
   kTimeLimit = 4,
   kDeviceError = 5,
   kSetup = 6,       // batched LPs: norm estimate and A x0 still to do
-  kInfeasible = 7   // batched LPs: a Farkas certificate passed the device test
+  kInfeasible = 7,  // a Farkas certificate passed the device test (the host re-checks it)
+  kUnbounded = 8    // a primal ray passed the device test (the host re-checks it)
 };
 
 struct Residuals {
@@ -157,12 +158,14 @@ struct State {
   double* yavg;
   double* best_x;  // scaled, FP64
   double* best_y;
+  double* cert_row;  // [m] Farkas candidate (reference sign, max-normalised), permuted
+  double* cert_col;  // [n] primal-ray candidate (max-normalised), permuted
   double* partials;  // [2][G][kPartSlots]
   Ctrl* ctrl;
   GridBarrier bar;
 };
 
-constexpr int kPartSlots = 20;
+constexpr int kPartSlots = 32;
 constexpr int kEvalSlots = 16;
 // complementarity slots of the evaluation are max-reductions
 constexpr unsigned kEvalMaxMask = (1u << 6) | (1u << 7) | (1u << 12) | (1u << 13);
@@ -544,6 +547,138 @@ struct AnchorCol {
     du[j] = finite_bound(v.hi) ? static_cast<float>(v.hi - v.xr) : INFINITY;
   }
 };
+
+// ---- infeasibility and unboundedness certificates ------------------------------------------
+//
+// At an evaluation the iterate differences are tested as certificates in the sense of
+// src/core/certificate.cpp (the reference's own checkers; its CPU PDHG never produces one):
+//
+//  * Farkas (primal infeasibility, certificate.cpp:29-119): f = -Dr (y - y_r), the dual
+//    movement since the last restart in original units and the reference's row_dual sign.
+//    Rows aggregate to S = sum_i f_i * (row_lower if f_i > 0, row_upper if f_i < 0); the
+//    column box allows at most M = max over the box of d.x with d = A'f. S > M proves the LP
+//    infeasible. For a feasible LP S <= M for every f, so the test cannot fire on one.
+//  * primal ray (dual infeasibility, certificate.cpp:121-218): r = Dc (x_k - x_{k-1}), the
+//    last accepted step in original units. It must move no column against a finite bound,
+//    keep A r off every finite row bound it would cross, and improve the min-space cost.
+//
+// The device test is a filter with the reference's structure (with a margin for the Farkas
+// test, and loose enough for a near-ray that the host can repair); the host re-checks every
+// candidate exactly with the reference's rules before it reports one.
+
+// Slots of the row/column terms gathered in the evaluation's first pass. Max-reduced: 1-4, 6.
+//   0 S, 1 max|f|, 2 max|f| leaning on a missing row bound,
+//   3 max|r|, 4 max|r| against a finite column bound, 5 c'r (min space), 6 max|c_j r_j|
+constexpr int kCertSlots = 7;
+constexpr unsigned kCertMaxMask = (1u << 1) | (1u << 2) | (1u << 3) | (1u << 4) | (1u << 6);
+
+__device__ __forceinline__ void farkas_row_terms(double f, double lo, double hi,
+                                                 double (&e)[kCertSlots]) {
+  e[1] = dmax(e[1], fabs(f));
+  if (f > 0.0) {
+    if (finite_bound(lo)) e[0] += f * lo; else e[2] = dmax(e[2], f);
+  } else if (f < 0.0) {
+    if (finite_bound(hi)) e[0] += f * hi; else e[2] = dmax(e[2], -f);
+  }
+}
+
+__device__ __forceinline__ void ray_col_terms(double r, double lo, double hi, double c,
+                                              double (&e)[kCertSlots]) {
+  e[3] = dmax(e[3], fabs(r));
+  if (r > 0.0 && finite_bound(hi)) e[4] = dmax(e[4], r);
+  if (r < 0.0 && finite_bound(lo)) e[4] = dmax(e[4], -r);
+  e[5] += c * r;
+  e[6] = dmax(e[6], fabs(c * r));
+}
+
+// sum_k M_ik (u - v)_k: a matrix times the difference of two vectors
+template <class U, class V>
+struct DiffGather {
+  const U* u;
+  const V* v;
+  __device__ __forceinline__ void add(double (&s)[1], double a, int k) const {
+    s[0] += a * (ld(u + k) - ld(v + k));
+  }
+  __device__ __forceinline__ double product(int, double a, int k) const {
+    return a * (ld(u + k) - ld(v + k));
+  }
+};
+
+// Column terms of the Farkas test for d = A'f = -(A'_scaled (y - y_r)) / Dc.
+// slots: 0 max |d|, 1 reachable M, 2 max |d| over columns leaning on a missing bound
+constexpr unsigned kFarkasColMaxMask = (1u << 0) | (1u << 2);
+struct FarkasCol {
+  const double* dc;
+  const double* cl0;
+  const double* cu0;
+  struct In {
+    double dc, lo, hi;
+  };
+  __device__ __forceinline__ In load(int j) const {
+    return In{__ldg(dc + j), __ldg(cl0 + j), __ldg(cu0 + j)};
+  }
+  __device__ __forceinline__ void apply(int j, const double (&s)[1], const In& v,
+                                        double (&acc)[3]) const {
+    const double d = -s[0] / v.dc;
+    acc[0] = dmax(acc[0], fabs(d));
+    if (d > 0.0) {
+      if (finite_bound(v.hi)) acc[1] += d * v.hi; else acc[2] = dmax(acc[2], d);
+    } else if (d < 0.0) {
+      if (finite_bound(v.lo)) acc[1] += d * v.lo; else acc[2] = dmax(acc[2], -d);
+    }
+  }
+};
+
+// Row terms of the ray test for A r = (A_scaled (x_k - x_{k-1})) / Dr.
+// slots: 0 max |(A r)_i| against a finite row bound, 1 max |(A r)_i|
+struct RayRow {
+  const double* dr;
+  const double* rl0;
+  const double* ru0;
+  struct In {
+    double dr, lo, hi;
+  };
+  __device__ __forceinline__ In load(int i) const {
+    return In{__ldg(dr + i), __ldg(rl0 + i), __ldg(ru0 + i)};
+  }
+  __device__ __forceinline__ void apply(int i, const double (&s)[1], const In& v,
+                                        double (&acc)[2]) const {
+    const double act = s[0] / v.dr;
+    if (act > 0.0 && finite_bound(v.hi)) acc[0] = dmax(acc[0], act);
+    if (act < 0.0 && finite_bound(v.lo)) acc[0] = dmax(acc[0], -act);
+    acc[1] = dmax(acc[1], fabs(act));
+  }
+};
+
+// The device filter: 1 = Farkas candidate, 2 = ray candidate, 0 = neither. Sets
+// c.farkas_margin to the normalised Farkas margin S - M when that test ran.
+__device__ __forceinline__ int certificate_test(Ctrl& c, const double (&e)[kCertSlots],
+                                                const double (&fk)[3], const double (&rr)[2]) {
+  if (e[1] > 0.0) {
+    const double Sn = e[0] / e[1], Mn = fk[1] / e[1];
+    const double margin = Sn - Mn;
+    c.farkas_margin = margin;
+    const bool rows_ok = e[2] <= 1e-9 * e[1];
+    const bool cols_ok = fk[2] <= 1e-9 * dmax(fk[0], 1e-300);
+    if (rows_ok && cols_ok && margin > 1e-6 * dmax(1.0, dmax(fabs(Sn), fabs(Mn)))) return 1;
+  }
+  if (e[3] > 0.0) {
+    // looser than the checker: the host repairs a near-ray before its exact check
+    const double improvement = e[5] / e[3];
+    const bool cols_ok = e[4] <= 1e-3 * e[3];
+    const bool rows_ok = rr[0] <= 1e-3 * dmax(e[3], rr[1]);
+    if (cols_ok && rows_ok && improvement < -1e-6 * dmax(1.0, e[6] / e[3])) return 2;
+  }
+  return 0;
+}
+
+// The slot of the previous accepted iterate at an evaluation: an evaluation follows an
+// accepted step (pdhg.cpp:502-503), which flipped `cur`.
+__device__ __forceinline__ int cur_prev_slot(const Ctrl& c) { return c.cur ^ 1; }
+
+// Evaluations between two certificate tests, and after a candidate the host turned down.
+constexpr int kCertEvery = 4;
+constexpr int kCertCooldown = 8;
 
 // Sum (or max) of kPartSlots-wide block partials over all blocks, in block order. Every
 // block calls it after a barrier and gets identical totals.
@@ -937,11 +1072,15 @@ template <class T>
 __global__ void __launch_bounds__(kThreads, 2) evaluate_kernel(Prob<T> P, State<T> S) {
   __shared__ Ctrl c;
   __shared__ double sh[kWarps * kEvalSlots];
-  __shared__ int flags[3];  // best updated, restart, chosen average
+  __shared__ int flags[4];  // best updated, restart, chosen average, certificate kind
   double* stream = warp_stream();
   if (threadIdx.x == 0) c = *S.ctrl;
   __syncthreads();
   if (c.state != kNeedEval) return;
+  // every kCertEvery-th evaluation tests the iterate differences as certificates
+  const bool test_cert = c.farkas_cooldown == 0 && (c.evaluations % kCertEvery) == kCertEvery - 1;
+  const int prev = cur_prev_slot(c);
+  double cert_scale = 1.0;  // max|f| or max|r| of a candidate, once one is found
   const int G = gridDim.x;
   const int cur = c.cur;
   const int stride = G * kThreads;
@@ -955,6 +1094,9 @@ __global__ void __launch_bounds__(kThreads, 2) evaluate_kernel(Prob<T> P, State<
   // On the FP32 level the iterates and sums are deltas from the anchor: the movement is the
   // delta itself, and the full FP64 iterate goes to xfull / yfull for the passes below.
   double acc1[2] = {0.0, 0.0};
+  double ec[kCertSlots];
+#pragma unroll
+  for (int s = 0; s < kCertSlots; ++s) ec[s] = 0.0;
   for (int j = gt; j < P.n; j += stride) {
     const double xo = ld(S.x[cur] + j);
     const double xs = S.xsum[j] + (c.pending ? xo : 0.0);
@@ -970,6 +1112,10 @@ __global__ void __launch_bounds__(kThreads, 2) evaluate_kernel(Prob<T> P, State<
       d = xo - ld(S.xr + j);
     }
     acc1[0] += d * d;
+    if (test_cert) {
+      const double r = __ldg(P.dc + j) * (xo - ld(S.x[prev] + j));
+      ray_col_terms(r, __ldg(P.cl0 + j), __ldg(P.cu0 + j), __ldg(P.c0 + j), ec);
+    }
   }
   for (int i = gt; i < P.m; i += stride) {
     const double yo = ld(S.y[cur] + i);
@@ -986,9 +1132,14 @@ __global__ void __launch_bounds__(kThreads, 2) evaluate_kernel(Prob<T> P, State<
       d = yo - ld(S.yr + i);
     }
     acc1[1] += d * d;
+    if (test_cert) farkas_row_terms(-__ldg(P.dr + i) * d, __ldg(P.rl0 + i), __ldg(P.ru0 + i), ec);
   }
   block_reduce<2, 0u>(acc1, sh);
   write_partials(part, 0, acc1, 2);
+  if (test_cert) {
+    block_reduce<kCertSlots, kCertMaxMask>(ec, sh);
+    write_partials(part, 18, ec, kCertSlots);
+  }
   if (!grid_barrier(S.bar)) goto device_error;
 
   {
@@ -1013,6 +1164,25 @@ __global__ void __launch_bounds__(kThreads, 2) evaluate_kernel(Prob<T> P, State<
     }
     block_reduce<kEvalSlots, kEvalMaxMask>(acc, sh);
     write_partials(part, 2, acc, kEvalSlots);
+    if (test_cert) {
+      // the certificates' matrix terms: A'(y - y_r) for the Farkas test, A (x_k - x_{k-1})
+      // for the ray test
+      double fk[3] = {0.0, 0.0, 0.0};
+      if constexpr (kDelta<T>) {
+        run_phase<1, 3>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pat, Gather1<T>{S.y[cur]},
+                        FarkasCol{P.dc, P.cl0, P.cu0}, fk, stream);
+      } else {
+        run_phase<1, 3>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pat, DiffGather<T, double>{S.y[cur], S.yr},
+                        FarkasCol{P.dc, P.cl0, P.cu0}, fk, stream);
+      }
+      block_reduce<3, kFarkasColMaxMask>(fk, sh);
+      write_partials(part, 25, fk, 3);
+      double rr[2] = {0.0, 0.0};
+      run_phase<1, 2>(P.A.ptr, P.A.idx, P.A.val64, P.pa, DiffGather<T, T>{S.x[cur], S.x[prev]},
+                      RayRow{P.dr, P.rl0, P.ru0}, rr, stream);
+      block_reduce<2, 3u>(rr, sh);
+      write_partials(part, 28, rr, 2);
+    }
   }
   if (!grid_barrier(S.bar)) goto device_error;
 
@@ -1021,8 +1191,45 @@ __global__ void __launch_bounds__(kThreads, 2) evaluate_kernel(Prob<T> P, State<
     reduce_partials<2, 0u>(part, 0, mv, sh);
     double t[kEvalSlots];
     reduce_partials<kEvalSlots, kEvalMaxMask>(part, 2, t, sh);
-    if (threadIdx.x == 0) evaluation_decision(c, t, mv, has_average, flags);
+    double ect[kCertSlots] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, fkt[3] = {0.0, 0.0, 0.0},
+           rrt[2] = {0.0, 0.0};
+    if (test_cert) {
+      reduce_partials<kCertSlots, kCertMaxMask>(part, 18, ect, sh);
+      reduce_partials<3, kFarkasColMaxMask>(part, 25, fkt, sh);
+      reduce_partials<2, 3u>(part, 28, rrt, sh);
+    }
+    if (threadIdx.x == 0) {
+      const Ctrl before = c;
+      evaluation_decision(c, t, mv, has_average, flags);
+      flags[3] = 0;
+      if (c.farkas_cooldown > 0) --c.farkas_cooldown;
+      if (test_cert && c.state != kConverged) {
+        const int kind = certificate_test(c, ect, fkt, rrt);
+        if (kind != 0) {
+          // keep the restart anchor and the step state as they were: the certificate is read
+          // from them, and the loop resumes from them if the host turns it down
+          const double margin = c.farkas_margin;
+          c = before;
+          ++c.evaluations;
+          c.pending = 0;
+          c.farkas_margin = margin;
+          c.state = kind == 1 ? kInfeasible : kUnbounded;
+          flags[0] = flags[1] = flags[2] = 0;
+          flags[3] = kind;
+        }
+      }
+    }
     __syncthreads();
+    if (flags[3] != 0) cert_scale = flags[3] == 1 ? ect[1] : ect[3];
+  }
+  if (flags[3] == 1) {
+    for (int i = gt; i < P.m; i += stride) {
+      const double d = kDelta<T> ? ld(S.y[cur] + i) : ld(S.y[cur] + i) - ld(S.yr + i);
+      S.cert_row[i] = -__ldg(P.dr + i) * d / cert_scale;
+    }
+  } else if (flags[3] == 2) {
+    for (int j = gt; j < P.n; j += stride)
+      S.cert_col[j] = __ldg(P.dc + j) * (ld(S.x[cur] + j) - ld(S.x[prev] + j)) / cert_scale;
   }
 
   // E3: keep the best point (scaled, FP64) and reset the average at a restart.

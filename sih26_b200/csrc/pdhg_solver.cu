@@ -144,7 +144,7 @@ struct Common {
   const double *dr, *dc, *c0, *cl0, *cu0, *rl0, *ru0;
   const double *c64, *cl64, *cu64, *rl64, *ru64;  // scaled, FP64
   Part pa, pat;
-  double *best_x, *best_y, *partials;
+  double *best_x, *best_y, *cert_row, *cert_col, *partials;
   Ctrl* ctrl;
   GridBarrier bar;
 };
@@ -213,6 +213,8 @@ static Level<T> make_level(Arena& a, const Common& cm, const PermutedLp& q, cons
   }
   S.best_x = cm.best_x;
   S.best_y = cm.best_y;
+  S.cert_row = cm.cert_row;
+  S.cert_col = cm.cert_col;
   S.partials = cm.partials;
   S.ctrl = cm.ctrl;
   S.bar = cm.bar;
@@ -349,6 +351,52 @@ static Ctrl run_loop(Level<T>& L, int G, cudaStream_t stream, Ctrl* host_ctrl, i
   return c;
 }
 
+// A certificate the device found, checked on the host against the original problem.
+struct Certificate {
+  int kind = 0;               // 0 none, kInfeasible or kUnbounded
+  std::vector<double> value;  // original order: Farkas multipliers [m] or a primal ray [n]
+  int rejected = 0;           // candidates the exact check turned down
+};
+
+// run_loop, plus the host half of infeasibility detection: when the device stops on a
+// certificate candidate, the candidate is copied back, un-permuted and checked with the
+// reference's exact rules (farkas_holds / ray_holds). A proof ends the solve; anything else
+// resumes the loop from the same state with the test paused for kCertCooldown evaluations.
+template <class T>
+static Ctrl run_loop_checked(Level<T>& L, int G, cudaStream_t stream, Ctrl* host_ctrl,
+                             int verbose, int stall_checks, bool* stalled, LaunchTimer& timer,
+                             const sankhya_pdhg_problem& prob, const PermutedLp& q, Arena& a,
+                             const double* cert_row, const double* cert_col, Certificate& cert) {
+  for (;;) {
+    Ctrl c = run_loop(L, G, stream, host_ctrl, verbose, stall_checks, stalled, timer);
+    if (c.state != kInfeasible && c.state != kUnbounded) return c;
+    const bool rows = c.state == kInfeasible;
+    const int len = rows ? q.m : q.n;
+    std::vector<double> h(len), v(len);
+    a.get(h.data(), rows ? cert_row : cert_col, len * sizeof(double), stream);
+    SIH26_CUDA(cudaStreamSynchronize(stream), SANKHYA_GPU_SYNC_FAILED);
+    const std::vector<int>& perm = rows ? q.row_perm : q.col_perm;
+    for (int t = 0; t < len; ++t) v[perm[t]] = h[t];
+    bool ok = rows ? farkas_holds(prob, v) : ray_holds(prob, v);
+    if (!ok && !rows && repair_ray(prob, v)) ok = ray_holds(prob, v);
+    if (ok) {
+      cert.kind = c.state;
+      cert.value = std::move(v);
+      return c;
+    }
+    ++cert.rejected;
+    c.state = kRunning;
+    c.farkas_cooldown = kCertCooldown;
+    a.put(L.S.ctrl, &c, sizeof(Ctrl), stream);
+    if (kDelta<T> && !rows && stalled) {
+      // the FP32 level sees a ray it cannot resolve to the checker's 1e-7: the FP64 level
+      // takes over from here (the mixed mode's hand-over) and certifies it
+      *stalled = true;
+      return c;
+    }
+  }
+}
+
 // Relative KKT error below which the FP32 phase of the mixed mode hands over by default.
 // FP32 deltas about an FP64 anchor keep their accuracy as the restarts close in (a plain FP32
 // iterate stalls near 256 units of FP32 rounding, ~1.5e-5), so this is only a backstop for
@@ -454,6 +502,8 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
   cm.pat = upload_part(a, partition(q.at_ptr, G, kWarps, prm.group_size_cols));
   cm.best_x = a.zeros<double>(n);
   cm.best_y = a.zeros<double>(m);
+  cm.cert_row = a.zeros<double>(m);
+  cm.cert_col = a.zeros<double>(n);
   cm.partials = a.zeros<double>(2ull * G * kPartSlots);
   cm.ctrl = a.zeros<Ctrl>(1);
   unsigned* bar_words = a.zeros<unsigned>(2);
@@ -520,6 +570,7 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
   c0.use_restarts = prm.restart ? 1 : 0;
   c0.stop_at_request = prm.stop_at_request ? 1 : 0;
   c0.stop_rule = prm.stop_rule;
+  c0.farkas_cooldown = prm.detect_infeasibility ? 0 : (1 << 30);
 
   // the time limit counts from the start of the call, like the reference's Timer
   const double setup_seconds = seconds_since(t_start);
@@ -565,10 +616,12 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
   timer.on = prm.profile_kernels != 0;
   SIH26_CUDA(cudaEventRecord(ev0, stream), SANKHYA_GPU_INIT_FAILED);
   Ctrl fin{};
+  Certificate cert;
   long long fp32_iterations = 0;
   if (!mixed) {
     a.put(cm.ctrl, &c0, sizeof(Ctrl), stream);
-    fin = run_loop(L64, G, stream, host_ctrl, prm.verbose, 0, nullptr, timer);
+    fin = run_loop_checked(L64, G, stream, host_ctrl, prm.verbose, 0, nullptr, timer, prob, q, a,
+                           cm.cert_row, cm.cert_col, cert);
   } else {
     // FP32 phase: relative KKT to the switch tolerance -- by default the request, but no
     // finer than kFp32Reach -- handing over early if the FP32 level stalls
@@ -582,12 +635,13 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
     bool stalled = false;
     const int stall_checks = prm.mixed_stall_checks > 0 ? prm.mixed_stall_checks
                            : prm.mixed_stall_checks < 0 ? 0 : kAutoStall;
-    fin = run_loop(L32, G, stream, host_ctrl, prm.verbose, stall_checks, &stalled, timer);
+    fin = run_loop_checked(L32, G, stream, host_ctrl, prm.verbose, stall_checks, &stalled, timer,
+                           prob, q, a, cm.cert_row, cm.cert_col, cert);
     fp32_iterations = fin.iteration;
     const bool done_in_fp32 = fin.state == kConverged && prm.stop_rule == 1 &&
                               fp32_target <= prm.tolerance;
     const bool limit_hit = fin.state == kIterationLimit || fin.state == kTimeLimit ||
-                           fin.state == kDeviceError;
+                           fin.state == kDeviceError || cert.kind != 0;
     if (!done_in_fp32 && !limit_hit) {
       // FP64 polish. The hand-over keeps the whole restart state -- iterate, restart anchor,
       // running sums and their count, step size, primal weight -- so the FP64 loop goes on
@@ -607,7 +661,8 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
       init_ax_kernel<double><<<G, kThreads, stream_smem_bytes(), stream>>>(L64.P, L64.S);
       SIH26_CUDA(cudaGetLastError(), SANKHYA_GPU_KERNEL_LAUNCH_FAILED);
       ++g_launches;
-      fin = run_loop(L64, G, stream, host_ctrl, prm.verbose, 0, nullptr, timer);
+      fin = run_loop_checked(L64, G, stream, host_ctrl, prm.verbose, 0, nullptr, timer, prob, q,
+                             a, cm.cert_row, cm.cert_col, cert);
     }
   }
   SIH26_CUDA(cudaEventRecord(ev1, stream), SANKHYA_GPU_INIT_FAILED);
@@ -667,7 +722,21 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
                                 f.gap_as_verified <= 1e-9 && f.complementarity <= 1e-6;
   const bool verifiable = fin.converged && project_standard;
   char msg[512];
-  if (verifiable) {
+  if (cert.kind == kInfeasible) {
+    res->status = SANKHYA_PDHG_INFEASIBLE;
+    if (res->farkas_dual) std::memcpy(res->farkas_dual, cert.value.data(), m * sizeof(double));
+    std::snprintf(msg, sizeof msg,
+                  "primal infeasible: Farkas certificate from the dual movement after %lld "
+                  "iterations (normalised margin %.3e), checked on the original model",
+                  fin.iteration, fin.farkas_margin);
+  } else if (cert.kind == kUnbounded) {
+    res->status = SANKHYA_PDHG_UNBOUNDED;
+    if (res->primal_ray) std::memcpy(res->primal_ray, cert.value.data(), n * sizeof(double));
+    std::snprintf(msg, sizeof msg,
+                  "unbounded: primal ray from the last step after %lld iterations, checked on "
+                  "the original model",
+                  fin.iteration);
+  } else if (verifiable) {
     res->status = SANKHYA_PDHG_OPTIMAL;
     std::snprintf(msg, sizeof msg,
                   "converged after %lld iterations and %lld restarts; absolute primal %.3e, dual "
@@ -693,7 +762,7 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
                   f.primal, f.dual, f.gap, fin.iteration, fin.restarts, prm.tolerance);
   }
   fill_message(res, msg);
-  res->dual_bound = verifiable ? sense * f.dual_objective + prob.objective_offset
+  res->dual_bound = (verifiable && cert.kind == 0) ? sense * f.dual_objective + prob.objective_offset
                                : (prob.maximize ? INFINITY : -INFINITY);
   res->setup_seconds = setup_seconds;
   res->h2d_bytes = a.h2d_bytes;

@@ -54,6 +54,8 @@ class LP:
     optimal_objective: Optional[float] = None
     # a Farkas ray when the instance was made infeasible on purpose
     farkas_star: Optional[np.ndarray] = None
+    # a primal ray when the instance was made unbounded on purpose
+    ray_star: Optional[np.ndarray] = None
 
     @property
     def num_nonzeros(self) -> int:
@@ -251,6 +253,35 @@ def make_infeasible(lp: LP, rng: np.random.Generator, margin: float = 0.1) -> LP
                               row_dual_star=None, optimal_objective=None,
                               name=lp.name + "-infeasible")
     out.farkas_star = y_hat
+    return out
+
+
+def make_unbounded(lp: LP, rng: np.random.Generator) -> LP:
+    """Append two columns with no upper bound whose matrix columns cancel (a and -a, a the
+    column of a random existing column) and whose costs sum to a negative number: moving both
+    up together keeps every row activity and lowers the cost without limit, so a primal ray
+    (0, ..., 0, 1, 1) exists by construction and the LP is unbounded."""
+    j = int(rng.integers(0, lp.num_cols))
+    b, e = int(lp.col_starts[j]), int(lp.col_starts[j + 1])
+    rows = lp.row_indices[b:e]
+    vals = lp.values[b:e]
+    nnz = lp.num_nonzeros
+    cs = np.concatenate([lp.col_starts, [nnz + rows.size, nnz + 2 * rows.size]]).astype(np.int32)
+    ri = np.concatenate([lp.row_indices, rows, rows]).astype(np.int32)
+    v = np.concatenate([lp.values, vals, -vals])
+    c1 = -float(rng.uniform(0.5, 1.5))
+    c2 = float(rng.uniform(0.0, 0.4))
+    n = lp.num_cols + 2
+    ray = np.zeros(n)
+    ray[-2:] = 1.0
+    out = dataclasses.replace(
+        lp, num_cols=n, col_starts=cs, row_indices=ri, values=v,
+        cost=np.concatenate([lp.cost, [c1, c2]]),
+        col_lower=np.concatenate([lp.col_lower, [0.0, 0.0]]),
+        col_upper=np.concatenate([lp.col_upper, [INF, INF]]), x_star=None, row_dual_star=None,
+        optimal_objective=None, name=lp.name + "-unbounded")
+    out.ray_star = ray
+    out.check()
     return out
 
 

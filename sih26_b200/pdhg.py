@@ -285,7 +285,7 @@ def solve_pdhg(model: LP, options: Optional[Options] = None) -> Solution:
         h2d_bytes=res.h2d_bytes, d2h_bytes=res.d2h_bytes,
         iterate_kernel_seconds=res.iterate_kernel_seconds, iterate_launches=res.iterate_launches,
         kernel_launches=res.kernel_launches)
-    if status != "model_error":
+    if status not in ("model_error", "infeasible", "unbounded"):
         sol.primal_infeasibility = _primal_infeasibility(model, x)
     return sol
 
@@ -375,12 +375,13 @@ class _Outputs:
             solve_seconds=res.total_seconds, algorithm="pdhg-gpu-batch",
             message=res.message.decode(errors="replace"),
             farkas_dual=self.fk if status == "infeasible" else None,
+            primal_ray=self.ray if status == "unbounded" else None,
             attempts=res.attempts, restarts=res.restarts, evaluations=res.evaluations,
             spectral_norm=res.spectral_norm,
             residuals={k: getattr(r, k) for k, _ in _Residuals._fields_},
             setup_seconds=res.setup_seconds, device_seconds=res.solve_seconds,
             kernel_launches=res.kernel_launches)
-        if status not in ("model_error", "infeasible"):
+        if status not in ("model_error", "infeasible", "unbounded"):
             sol.primal_infeasibility = _primal_infeasibility(model, self.x)
         return sol
 
