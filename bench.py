@@ -7,7 +7,9 @@ seed 1). A step is one solve to relative KKT 1e-6 (max of relative primal, dual 
 FP64, unscaled) through the library's C ABI.
 
   value   device seconds of the iteration loop (CUDA events on the solve's stream; the LP
-          was uploaded, scaled and its norm estimated before the timed region), FP32-mixed
+          was uploaded, scaled and its norm estimated before the timed region), FP32-mixed,
+          with the iteration operator of --algorithm (default: the Halpern operator; the
+          reference's operator is timed once in each precision beside it)
   e2e     the same solve measured around the public call with host arrays: validation,
           host scaling, H2D of the problem, the loop, D2H of x / y / reduced costs
   fp64    the same metric on the plain FP64 path
@@ -74,13 +76,24 @@ def _peaks():
     return 6650.0, "fallback"
 
 
-def algorithmic_bytes(m, n, nnz, value_bytes):
-    """Bytes one PDHG attempt must move (A and A' once, the vectors once): matrix values and
-    int32 indices of both orientations, both row-pointer arrays, per column x, c, l, u, the
-    gathered operand and the written x' and xbar at the iterate width plus the FP64 running
-    sum, per row y, row bounds, the gathered operand and y' plus the FP64 running sum."""
+def algorithmic_bytes(m, n, nnz, value_bytes, algorithm="reference"):
+    """Bytes one PDHG attempt must move (A and A' once, the vectors once).
+
+    reference operator: matrix values and int32 indices of both orientations, both
+    row-pointer arrays, per column x, c, l, u, the gathered operand and the written x' and
+    xbar at the iterate width plus the FP64 running sum, per row y, row bounds, the gathered
+    operand and y' plus the FP64 running sum.
+    Halpern operator, FP32 level (value_bytes 4): the same matrix terms; per column the delta
+    x, c + A'y_r (FP64), the two FP32 relative bounds, the gathered operand, written T(z)_x
+    and x_{k+1} (32 B); per row the delta y, y_r, A x_r, both FP64 bounds, the gathered
+    operand, written T(z)_y, y_{k+1} and the FP64 A x_{k+1} (56 B). FP64 level: per column x,
+    c, l, u, x_0, the gathered operand, T(z)_x, x_{k+1} (64 B); per row y, both bounds, y_0,
+    A x_0, the gathered operand, T(z)_y, y_{k+1}, A x_{k+1} (72 B)."""
     s = value_bytes
-    return 2 * nnz * (s + 4) + 4 * (m + n + 2) + n * (7 * s + 16) + m * (5 * s + 16)
+    matrix = 2 * nnz * (s + 4) + 4 * (m + n + 2)
+    if algorithm == "halpern":
+        return matrix + (n * 32 + m * 56 if s == 4 else n * 64 + m * 72)
+    return matrix + n * (7 * s + 16) + m * (5 * s + 16)
 
 
 class ClockSampler:
@@ -384,30 +397,34 @@ def run_ours(args):
     m, n, nnz = lp.num_rows, lp.num_cols, lp.num_nonzeros
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
 
-    def opts(precision, profile=False):
+    def opts(precision, algorithm, profile=False):
         return pdhg.Options(pdhg_tolerance=TOLERANCE, pdhg_stop_rule="relative_kkt",
-                            pdhg_precision=precision, gpu_device=local,
-                            pdhg_profile_kernels=profile)
+                            pdhg_precision=precision, pdhg_algorithm=algorithm,
+                            gpu_device=local, pdhg_profile_kernels=profile)
 
     def sync():
         torch.cuda.synchronize()
         if dist is not None:
             dist.barrier()
 
-    def step(precision, profile=False):
+    def step(precision, algorithm, profile=False):
         flush.random_(0, 255)  # L2 flush between steps
         sync()
-        s = pdhg.solve_pdhg(lp, opts(precision, profile))
+        s = pdhg.solve_pdhg(lp, opts(precision, algorithm, profile))
         sync()
         return s
 
+    algo = args.algorithm
+    other = "reference" if algo == "halpern" else "halpern"
     for _ in range(args.warmup):
-        step("mixed")
+        step("mixed", algo)
     sols = []
     with ClockSampler(local) as clocks:
         for _ in range(args.steps):
-            sols.append(step("mixed", profile=True))
-    fp64 = step("fp64")
+            sols.append(step("mixed", algo, profile=True))
+    fp64 = step("fp64", algo)
+    alt_mixed = step("mixed", other)
+    alt_fp64 = step("fp64", other)
 
     def max_over_ranks(v):
         if dist is None:
@@ -419,6 +436,9 @@ def run_ours(args):
     dev = max_over_ranks(statistics.mean(s.device_seconds for s in sols))
     e2e = max_over_ranks(statistics.mean(s.solve_seconds for s in sols))
     fp64_dev = max_over_ranks(fp64.device_seconds)
+    alt = {k: {"value": max_over_ranks(v.device_seconds), "unit": "s",
+               "iterations": v.iterations, "status": v.status}
+           for k, v in (("mixed", alt_mixed), ("fp64", alt_fp64))}
     last = sols[-1]
     for s in sols:
         if s.status not in ("optimal", "feasible"):
@@ -431,8 +451,8 @@ def run_ours(args):
     attempts = sum(s.attempts for s in sols)
     kern = sum(s.iterate_kernel_seconds for s in sols)
     fp32_share = sum(s.fp32_iterations for s in sols) / max(1, sum(s.iterations for s in sols))
-    bytes_attempt = (fp32_share * algorithmic_bytes(m, n, nnz, 4)
-                     + (1 - fp32_share) * algorithmic_bytes(m, n, nnz, 8))
+    bytes_attempt = (fp32_share * algorithmic_bytes(m, n, nnz, 4, algo)
+                     + (1 - fp32_share) * algorithmic_bytes(m, n, nnz, 8, algo))
     achieved = bytes_attempt * attempts / kern / 1e9 if kern > 0 else None
     peak, peak_kind = _peaks()
     traffic = None
@@ -463,7 +483,7 @@ def run_ours(args):
             "vs_baseline": None, "dtype": "f32 iterates, f64 reductions",
             "data": "synthetic (seeded planted-optimum LP)",
             "config": {"workload": WORKLOAD, "tolerance": TOLERANCE,
-                       "stop_rule": "relative_kkt", "precision": "mixed",
+                       "stop_rule": "relative_kkt", "precision": "mixed", "algorithm": algo,
                        "l2": "inputs larger than L2 (A, A' and vectors ~0.3 GB resident) and a "
                              "256 MB L2 flush before every step",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
@@ -473,6 +493,8 @@ def run_ours(args):
             / abs(lp.optimal_objective),
             "fp64": {"value": fp64_dev, "unit": "s", "iterations": fp64.iterations,
                      "status": fp64.status},
+            "algorithm": algo,
+            f"{other}_operator": alt,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None,
                          "traffic": traffic, "peak_kind": peak_kind,
@@ -493,12 +515,36 @@ def run_ours(args):
     return 0
 
 
+def profile_run(kind):
+    """Bounded runs for ncu captures (no timing, no JSON): `single` runs the 5M-nonzero LP for
+    200 iterations in FP32-mixed and again in FP64; `batch` solves the first 64 LPs of the
+    batched family in one batched call."""
+    from sih26_b200 import lpgen, pdhg
+
+    if kind == "single":
+        lp = make_workload()
+        for precision in ("mixed", "fp64"):
+            s = pdhg.solve_pdhg(lp, pdhg.Options(pdhg_tolerance=TOLERANCE, iteration_limit=200,
+                                                 pdhg_stop_rule="relative_kkt",
+                                                 pdhg_precision=precision))
+            print(precision, s.status, s.iterations, s.kernel_launches)
+    else:
+        lps = lpgen.uneven_batch(count=512, m_lo=50, m_hi=5000, infeasible_fraction=0.1, seed=3)
+        sols = pdhg.batch_solve(lps[:64], pdhg.Options(pdhg_tolerance=TOLERANCE,
+                                                       pdhg_stop_rule="relative_kkt"))
+        print("batch", sum(s.status in ("optimal", "feasible", "infeasible") for s in sols))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--algorithm", choices=["halpern", "reference"], default="halpern",
+                    help="iteration operator of the timed solves (the other one is timed once "
+                         "in each precision for comparison)")
     ap.add_argument("--no-batched", action="store_true", help="skip the 512-LP batched leg")
     ap.add_argument("--no-served", action="store_true", help="skip the served-stream leg")
     ap.add_argument("--served-rates", default="50,200",
@@ -507,7 +553,11 @@ def main():
     ap.add_argument("--served-seconds", type=float, default=4.0, help="arrival window, s")
     ap.add_argument("--served-chunk", type=int, default=512,
                     help="attempts per LP per server launch")
+    ap.add_argument("--profile-run", choices=["single", "batch"], default=None,
+                    help="a bounded run for an ncu capture (prints no bench line)")
     args = ap.parse_args()
+    if args.profile_run:
+        return profile_run(args.profile_run)
     if args.warmup < 3:
         raise SystemExit("at least 3 warm-up steps")
     if args.impl == "reference":

@@ -83,6 +83,20 @@ enum {
   SANKHYA_PDHG_STOP_RELATIVE_KKT = 1
 };
 
+/* Iteration operator (single-LP path). */
+enum {
+  /* src/pdhg/pdhg.cpp:383-644: adaptive step size with acceptance test, running average,
+   * restarts on the KKT error (sufficient 0.2, artificial 0.36 of the iterations), primal
+   * weight smoothing 0.5. */
+  SANKHYA_PDHG_ALGORITHM_REFERENCE = 0,
+  /* Reflected restarted Halpern PDHG (Lu & Yang, "Restarted Halpern PDHG for linear
+   * programming", 2024): z_{k+1} = (k+1)/(k+2) (2 T(z_k) - z_k) + 1/(k+2) z_0 with T one PDHG
+   * step at the constant step size 0.998/||A||_2 and z_0 the last restart point. The
+   * candidates, restart rules, primal weight, stopping test and status rules stay the
+   * reference's; the PDHG output T(z_k) takes the place of the running average. */
+  SANKHYA_PDHG_ALGORITHM_HALPERN = 1
+};
+
 /* One LP as the reference's Model holds it (include/sankhya/model.hpp:131-225). */
 typedef struct sankhya_pdhg_problem {
   int32_t num_rows;
@@ -127,7 +141,8 @@ typedef struct sankhya_pdhg_params {
   int32_t mixed_stall_checks; /* MIXED: host checks (about 2,600 iterations each) without a
                                  better KKT error before the FP32 phase hands over; 0 = auto
                                  (no 1% gain over the last 30% of the iterations), -1 = never */
-  int32_t reserved[5];
+  int32_t algorithm;        /* SANKHYA_PDHG_ALGORITHM_REFERENCE (default) or _HALPERN */
+  int32_t reserved[4];
 } sankhya_pdhg_params;
 
 /* Unscaled residual block of the reported point (src/pdhg/pdhg.cpp:81-110). */

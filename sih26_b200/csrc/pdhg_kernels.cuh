@@ -62,7 +62,7 @@ struct Ctrl {
   double eta, omega, restart_kkt, best_worst;
   long long iteration, attempts, averaged, last_restart, restarts, evaluations;
   int cur, pending, state, converged;
-  int chosen_average, best_is_set, pad0, pad1;
+  int chosen_average, best_is_set, pad0, halpern;  // halpern: the Halpern operator
   Residuals best, current, average;  // best so far; last evaluation's two candidates
   // constants of the solve
   double spectral_norm, eta_ceiling, tolerance, bound_norm, cost_norm;
@@ -151,7 +151,9 @@ struct State {
   double* cg;     // [n] c + A'yr (scaled)
   float* dl;      // [n] lower bound - xr, rounded to FP32
   float* du;      // [n] upper bound - xr
-  double* axr;    // [m] A xr
+  double* axr;    // [m] A xr (the Halpern operator needs it on the FP64 level too)
+  T* xt;          // Halpern: the PDHG output T(z_k), primal part (a delta on the FP32 level)
+  T* yt;          // and dual part
   double* xfull;  // [n] evaluation scratch: xr + dx
   double* yfull;  // [m] yr + dy
   double* xavg;
@@ -548,6 +550,131 @@ struct AnchorCol {
   }
 };
 
+// ---- the Halpern operator ------------------------------------------------------------------
+//
+// Reflected Halpern PDHG: with T one PDHG step (pdhg.cpp:392-408 at a constant step size),
+// z_{k+1} = w (2 T(z_k) - z_k) + (1 - w) z_0, w = (k+1)/(k+2), k the steps since the last
+// restart and z_0 the restart point. Phase P forms x' = T(z_k)_x and x_{k+1}; phase D gathers
+// x_{k+1}, so a_{k+1} = A x_{k+1} is exact for the stored iterate as in the reference mode,
+// and recovers A xbar = A (2x' - x_k) = (a_{k+1} - (1 - w) A x_0) / w for the dual step. On the
+// FP32 level everything is a delta from the restart point, where x_0 and A x_0 are zero.
+
+template <class T>
+struct PrimalStepHalpern {
+  const T* x;
+  T* xn;
+  T* xt;
+  const T* c;
+  const T* cl;
+  const T* cu;
+  const double* x0;
+  double tau, w;
+  struct In {
+    double xo, c, lo, hi, x0;
+  };
+  __device__ __forceinline__ In load(int j) const {
+    return In{ld(x + j), ro(c + j), ro(cl + j), ro(cu + j), __ldcg(x0 + j)};
+  }
+  __device__ __forceinline__ void apply(int j, const double (&s)[1], const In& v,
+                                        double (&)[3]) const {
+    const T xp = static_cast<T>(project(v.xo - tau * (v.c + s[0]), v.lo, v.hi));
+    xt[j] = xp;
+    xn[j] = static_cast<T>(w * (2.0 * static_cast<double>(xp) - v.xo) + (1.0 - w) * v.x0);
+  }
+};
+
+template <class T>
+struct PrimalStepHalpernDelta {
+  const T* x;
+  T* xn;
+  T* xt;
+  const double* cg;
+  const float* dl;
+  const float* du;
+  double tau, w;
+  struct In {
+    double xo, c, lo, hi;
+  };
+  __device__ __forceinline__ In load(int j) const {
+    return In{ld(x + j), ro(cg + j), ro(dl + j), ro(du + j)};
+  }
+  __device__ __forceinline__ void apply(int j, const double (&s)[1], const In& v,
+                                        double (&)[3]) const {
+    const T xp = static_cast<T>(project(v.xo - tau * (v.c + s[0]), v.lo, v.hi));
+    xt[j] = xp;
+    xn[j] = static_cast<T>(w * (2.0 * static_cast<double>(xp) - v.xo));
+  }
+};
+
+template <class T>
+struct DualStepHalpern {
+  const T* y;
+  T* yn;
+  T* yt;
+  double* axn;
+  const T* rl;
+  const T* ru;
+  const double* y0;
+  const double* ax0;
+  double sigma, w;
+  struct In {
+    double yo, lo, hi, y0, a0;
+  };
+  __device__ __forceinline__ In load(int i) const {
+    return In{ld(y + i), ro(rl + i), ro(ru + i), __ldcg(y0 + i), __ldcg(ax0 + i)};
+  }
+  __device__ __forceinline__ void apply(int i, const double (&s)[1], const In& v,
+                                        double (&)[3]) const {
+    const double anew = s[0];
+    const double axbar = (anew - (1.0 - w) * v.a0) / w;
+    const double u = v.yo + sigma * axbar;
+    const T yp = static_cast<T>(u - sigma * project(u / sigma, v.lo, v.hi));
+    yt[i] = yp;
+    yn[i] = static_cast<T>(w * (2.0 * static_cast<double>(yp) - v.yo) + (1.0 - w) * v.y0);
+    axn[i] = anew;
+  }
+};
+
+template <class T>
+struct DualStepHalpernDelta {
+  const T* y;
+  T* yn;
+  T* yt;
+  double* axn;
+  const double* yr;
+  const double* axr;
+  const double* rl;
+  const double* ru;
+  double sigma, w;
+  struct In {
+    double yo, yr, axr, lo, hi;
+  };
+  __device__ __forceinline__ In load(int i) const {
+    return In{ld(y + i), ro(yr + i), ro(axr + i), ro(rl + i), ro(ru + i)};
+  }
+  __device__ __forceinline__ void apply(int i, const double (&s)[1], const In& v,
+                                        double (&)[3]) const {
+    const double anew = s[0];
+    const double u = (v.yr + v.yo) + sigma * (v.axr + anew / w);
+    const double yp = u - sigma * project(u / sigma, v.lo, v.hi);
+    const T dyp = static_cast<T>(yp - v.yr);
+    yt[i] = dyp;
+    yn[i] = static_cast<T>(w * (2.0 * static_cast<double>(dyp) - v.yo));
+    axn[i] = anew;
+  }
+};
+
+// One Halpern step is always taken: no acceptance test, no step-size change (the constant
+// step 0.998 / ||A||_2 keeps tau sigma ||A||^2 < 1); an evaluation every 40 steps.
+__device__ __forceinline__ void halpern_control(Ctrl& c) {
+  c.cur ^= 1;
+  ++c.averaged;  // k, the steps since the last restart
+  ++c.iteration;
+  ++c.attempts;
+  c.pending = 0;
+  if (c.iteration % 40 == 0) c.state = kNeedEval;
+}
+
 // ---- infeasibility and unboundedness certificates ------------------------------------------
 //
 // At an evaluation the iterate differences are tested as certificates in the sense of
@@ -792,6 +919,33 @@ __global__ void __launch_bounds__(kThreads, 2) iterate_kernel(Prob<T> P, State<T
     double* part = S.partials + (size_t)(c.attempts & 1) * G * kPartSlots;
     double acc[3] = {0.0, 0.0, 0.0};
     SIH26_MARK_START();
+    if (c.halpern) {
+      const double w = (double)(c.averaged + 1) / (double)(c.averaged + 2);
+      if constexpr (kDelta<T>) {
+        PrimalStepHalpernDelta<T> ps{S.x[cur], S.x[nxt], S.xt, S.cg, S.dl, S.du, tau, w};
+        run_phase<1, 3>(P.AT.ptr, P.AT.idx, P.AT.val, P.pat, Gather1<T>{S.y[cur]}, ps, acc, stream);
+      } else {
+        PrimalStepHalpern<T> ps{S.x[cur], S.x[nxt], S.xt, P.c, P.cl, P.cu, S.xr, tau, w};
+        run_phase<1, 3>(P.AT.ptr, P.AT.idx, P.AT.val, P.pat, Gather1<T>{S.y[cur]}, ps, acc, stream);
+      }
+      if (!grid_barrier(S.bar)) goto device_error;
+      if constexpr (kDelta<T>) {
+        DualStepHalpernDelta<T> ds{S.y[cur], S.y[nxt], S.yt, S.ax[nxt], S.yr, S.axr, P.rl64,
+                                   P.ru64, sigma, w};
+        run_phase<1, 3>(P.A.ptr, P.A.idx, P.A.val, P.pa, Gather1<T>{S.x[nxt]}, ds, acc, stream);
+      } else {
+        DualStepHalpern<T> ds{S.y[cur], S.y[nxt], S.yt, S.ax[nxt], P.rl, P.ru, S.yr, S.axr, sigma, w};
+        run_phase<1, 3>(P.A.ptr, P.A.idx, P.A.val, P.pa, Gather1<T>{S.x[nxt]}, ds, acc, stream);
+      }
+      if (!grid_barrier(S.bar)) goto device_error;
+      if (threadIdx.x == 0) {
+        halpern_control(c);
+        c.time_up = *((volatile int*)S.bar.time_up);
+      }
+      __syncthreads();
+      if (c.state != kRunning) break;
+      continue;
+    }
     if constexpr (kDelta<T>) {
       PrimalStepDelta<T> ps{S.x[cur], S.x[nxt], S.cg, S.dl, S.du, S.xsum, tau, c.pending};
       run_phase<1, 3>(P.AT.ptr, P.AT.idx, P.AT.val, P.pat, Gather1<T>{S.y[cur]}, ps, acc, stream);
@@ -1097,6 +1251,9 @@ __global__ void __launch_bounds__(kThreads, 2) evaluate_kernel(Prob<T> P, State<
   double ec[kCertSlots];
 #pragma unroll
   for (int s = 0; s < kCertSlots; ++s) ec[s] = 0.0;
+  // the Halpern operator's second candidate is the PDHG output T(z_k), not an average
+  const bool halpern = c.halpern != 0;
+  const T* ray_from = halpern ? S.xt : S.x[cur];
   for (int j = gt; j < P.n; j += stride) {
     const double xo = ld(S.x[cur] + j);
     const double xs = S.xsum[j] + (c.pending ? xo : 0.0);
@@ -1105,15 +1262,15 @@ __global__ void __launch_bounds__(kThreads, 2) evaluate_kernel(Prob<T> P, State<
     if constexpr (kDelta<T>) {
       const double r = S.xr[j];
       S.xfull[j] = r + xo;
-      S.xavg[j] = has_average ? r + xs / count : 0.0;
+      S.xavg[j] = has_average ? r + (halpern ? ld(S.xt + j) : xs / count) : 0.0;
       d = xo;
     } else {
-      S.xavg[j] = has_average ? xs / count : 0.0;
+      S.xavg[j] = has_average ? (halpern ? ld(S.xt + j) : xs / count) : 0.0;
       d = xo - ld(S.xr + j);
     }
     acc1[0] += d * d;
     if (test_cert) {
-      const double r = __ldg(P.dc + j) * (xo - ld(S.x[prev] + j));
+      const double r = __ldg(P.dc + j) * (ld(ray_from + j) - ld(S.x[prev] + j));
       ray_col_terms(r, __ldg(P.cl0 + j), __ldg(P.cu0 + j), __ldg(P.c0 + j), ec);
     }
   }
@@ -1125,10 +1282,10 @@ __global__ void __launch_bounds__(kThreads, 2) evaluate_kernel(Prob<T> P, State<
     if constexpr (kDelta<T>) {
       const double r = S.yr[i];
       S.yfull[i] = r + yo;
-      S.yavg[i] = has_average ? r + ys / count : 0.0;
+      S.yavg[i] = has_average ? r + (halpern ? ld(S.yt + i) : ys / count) : 0.0;
       d = yo;
     } else {
-      S.yavg[i] = has_average ? ys / count : 0.0;
+      S.yavg[i] = has_average ? (halpern ? ld(S.yt + i) : ys / count) : 0.0;
       d = yo - ld(S.yr + i);
     }
     acc1[1] += d * d;
@@ -1178,7 +1335,7 @@ __global__ void __launch_bounds__(kThreads, 2) evaluate_kernel(Prob<T> P, State<
       block_reduce<3, kFarkasColMaxMask>(fk, sh);
       write_partials(part, 25, fk, 3);
       double rr[2] = {0.0, 0.0};
-      run_phase<1, 2>(P.A.ptr, P.A.idx, P.A.val64, P.pa, DiffGather<T, T>{S.x[cur], S.x[prev]},
+      run_phase<1, 2>(P.A.ptr, P.A.idx, P.A.val64, P.pa, DiffGather<T, T>{ray_from, S.x[prev]},
                       RayRow{P.dr, P.rl0, P.ru0}, rr, stream);
       block_reduce<2, 3u>(rr, sh);
       write_partials(part, 28, rr, 2);
@@ -1229,7 +1386,7 @@ __global__ void __launch_bounds__(kThreads, 2) evaluate_kernel(Prob<T> P, State<
     }
   } else if (flags[3] == 2) {
     for (int j = gt; j < P.n; j += stride)
-      S.cert_col[j] = __ldg(P.dc + j) * (ld(S.x[cur] + j) - ld(S.x[prev] + j)) / cert_scale;
+      S.cert_col[j] = __ldg(P.dc + j) * (ld(ray_from + j) - ld(S.x[prev] + j)) / cert_scale;
   }
 
   // E3: keep the best point (scaled, FP64) and reset the average at a restart.
@@ -1252,6 +1409,8 @@ __global__ void __launch_bounds__(kThreads, 2) evaluate_kernel(Prob<T> P, State<
         if constexpr (kDelta<T>) {
           S.y[cur][i] = T(0);
           S.ax[cur][i] = 0.0;
+        } else {
+          if (halpern) S.axr[i] = S.ax[cur][i];  // A x_0 of the new restart point
         }
       }
     }
@@ -1300,21 +1459,24 @@ __global__ void __launch_bounds__(kThreads, 2) report_kernel(Prob<T> P, State<T>
 
 // FP32 -> FP64 hand-over of the mixed-precision mode: the FP32 level's restart state into
 // the FP64 level -- iterate (into slot 0), restart anchor and running sums, the deltas added
-// back to the anchor (`count` iterates are summed).
+// back to the anchor (`count` iterates are summed). With `restart` (the Halpern operator) the
+// FP64 level restarts at the hand-over point instead: the anchor is the iterate itself.
 static __global__ void handover_kernel(State<float> from, int cur, double count, State<double> to,
-                                       int m, int n) {
+                                       int m, int n, int restart) {
   const int stride = gridDim.x * blockDim.x;
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
     const double r = from.xr[j];
-    to.x[0][j] = r + static_cast<double>(from.x[cur][j]);
-    to.xr[j] = r;
-    to.xsum[j] = count * r + from.xsum[j];
+    const double x = r + static_cast<double>(from.x[cur][j]);
+    to.x[0][j] = x;
+    to.xr[j] = restart ? x : r;
+    to.xsum[j] = restart ? 0.0 : count * r + from.xsum[j];
   }
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
     const double r = from.yr[i];
-    to.y[0][i] = r + static_cast<double>(from.y[cur][i]);
-    to.yr[i] = r;
-    to.ysum[i] = count * r + from.ysum[i];
+    const double y = r + static_cast<double>(from.y[cur][i]);
+    to.y[0][i] = y;
+    to.yr[i] = restart ? y : r;
+    to.ysum[i] = restart ? 0.0 : count * r + from.ysum[i];
   }
 }
 

@@ -203,11 +203,13 @@ static Level<T> make_level(Arena& a, const Common& cm, const PermutedLp& q, cons
   S.yr = a.zeros<double>(m);
   S.xavg = a.zeros<double>(n);
   S.yavg = a.zeros<double>(m);
+  S.axr = a.zeros<double>(m);
+  S.xt = a.zeros<T>(n);
+  S.yt = a.zeros<T>(m);
   if constexpr (kDelta<T>) {
     S.cg = a.zeros<double>(n);
     S.dl = a.zeros<float>(n);
     S.du = a.zeros<float>(n);
-    S.axr = a.zeros<double>(m);
     S.xfull = a.zeros<double>(n);
     S.yfull = a.zeros<double>(m);
   }
@@ -419,6 +421,9 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
   if (!(prm.tolerance > 0.0)) throw Failure{SANKHYA_GPU_INVALID_ARGUMENT, "tolerance must be > 0"};
   if (prm.precision != SANKHYA_PDHG_FP64 && prm.precision != SANKHYA_PDHG_MIXED)
     throw Failure{SANKHYA_GPU_INVALID_ARGUMENT, "unknown precision"};
+  if (prm.algorithm != SANKHYA_PDHG_ALGORITHM_REFERENCE &&
+      prm.algorithm != SANKHYA_PDHG_ALGORITHM_HALPERN)
+    throw Failure{SANKHYA_GPU_INVALID_ARGUMENT, "unknown algorithm"};
   const int m = prob.num_rows, n = prob.num_cols;
   res->status = SANKHYA_PDHG_NOT_SOLVED;
   res->converged = 0;
@@ -541,10 +546,15 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
                SANKHYA_GPU_COPY_FAILED);
   }
   // A x0 for the starting point, with the same phase code as the iteration's A x'
+  const bool halpern = prm.algorithm == SANKHYA_PDHG_ALGORITHM_HALPERN;
   if (mixed) {
     anchor_kernel<float><<<G, kThreads, stream_smem_bytes(), stream>>>(L32.P, L32.S);
   } else {
     init_ax_kernel<double><<<G, kThreads, stream_smem_bytes(), stream>>>(L64.P, L64.S);
+    // the Halpern operator's A x_0 for the starting point (x_0 = x0)
+    if (halpern)
+      SIH26_CUDA(cudaMemcpyAsync(L64.S.axr, L64.S.ax[0], m * sizeof(double),
+                                 cudaMemcpyDeviceToDevice, stream), SANKHYA_GPU_COPY_FAILED);
   }
   SIH26_CUDA(cudaGetLastError(), SANKHYA_GPU_KERNEL_LAUNCH_FAILED);
   ++g_launches;
@@ -571,6 +581,10 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
   c0.stop_at_request = prm.stop_at_request ? 1 : 0;
   c0.stop_rule = prm.stop_rule;
   c0.farkas_cooldown = prm.detect_infeasibility ? 0 : (1 << 30);
+  if (halpern) {
+    c0.halpern = 1;
+    c0.eta = 0.998 / std::max(spectral_norm, 1e-12);  // constant: tau sigma ||A||^2 < 1
+  }
 
   // the time limit counts from the start of the call, like the reference's Timer
   const double setup_seconds = seconds_since(t_start);
@@ -648,7 +662,7 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
       // exactly where the FP32 one stopped, only with more digits.
       const int threads = 256, blocks = std::max(1, std::min(4096, (std::max(m, n) + threads - 1) / threads));
       handover_kernel<<<blocks, threads, 0, stream>>>(L32.S, fin.cur, static_cast<double>(fin.averaged),
-                                                     L64.S, m, n);
+                                                     L64.S, m, n, halpern ? 1 : 0);
       SIH26_CUDA(cudaGetLastError(), SANKHYA_GPU_KERNEL_LAUNCH_FAILED);
       ++g_launches;
       Ctrl h = fin;
@@ -657,10 +671,18 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
       h.converged = 0;
       h.tolerance = prm.tolerance;
       h.stop_rule = prm.stop_rule;
+      if (halpern) {
+        // the Halpern sequence restarts at the hand-over point
+        h.averaged = 0;
+        h.last_restart = h.iteration;
+      }
       a.put(cm.ctrl, &h, sizeof(Ctrl), stream);
       init_ax_kernel<double><<<G, kThreads, stream_smem_bytes(), stream>>>(L64.P, L64.S);
       SIH26_CUDA(cudaGetLastError(), SANKHYA_GPU_KERNEL_LAUNCH_FAILED);
       ++g_launches;
+      if (halpern)
+        SIH26_CUDA(cudaMemcpyAsync(L64.S.axr, L64.S.ax[0], m * sizeof(double),
+                                   cudaMemcpyDeviceToDevice, stream), SANKHYA_GPU_COPY_FAILED);
       fin = run_loop_checked(L64, G, stream, host_ctrl, prm.verbose, 0, nullptr, timer, prob, q,
                              a, cm.cert_row, cm.cert_col, cert);
     }

@@ -38,6 +38,7 @@ SOLVE_STATUS = {0: "not_solved", 1: "optimal", 2: "feasible", 3: "infeasible", 4
                 9: "model_error", 10: "infeasible_or_unbounded"}
 
 PRECISIONS = {"fp64": 0, "mixed": 1}
+ALGORITHMS = {"reference": 0, "halpern": 1}
 STOP_RULES = {"reference": 0, "relative_kkt": 1}
 
 
@@ -70,7 +71,7 @@ class _Params(C.Structure):
                 ("mixed_switch_tolerance", C.c_double), ("group_size_rows", C.c_int32),
                 ("group_size_cols", C.c_int32), ("grid_blocks", C.c_int32),
                 ("profile_kernels", C.c_int32), ("mixed_stall_checks", C.c_int32),
-                ("reserved", C.c_int32 * 5)]
+                ("algorithm", C.c_int32), ("reserved", C.c_int32 * 4)]
 
 
 class _Residuals(C.Structure):
@@ -153,6 +154,7 @@ class Options:
         "pdhg_grid_blocks": (int, 0),
         "pdhg_profile_kernels": (bool, False),
         "pdhg_mixed_stall_checks": (int, 0),
+        "pdhg_algorithm": (str, "reference"),
     }
 
     def __init__(self, **values):
@@ -167,7 +169,8 @@ class Options:
         if typ is bool and isinstance(value, str):
             value = value.lower() in ("1", "true", "on", "yes")
         if typ is str:
-            allowed = {"pdhg_precision": PRECISIONS, "pdhg_stop_rule": STOP_RULES}.get(name)
+            allowed = {"pdhg_precision": PRECISIONS, "pdhg_stop_rule": STOP_RULES,
+                       "pdhg_algorithm": ALGORITHMS}.get(name)
             if allowed is not None and value not in allowed:
                 raise ValueError(f"{name} must be one of {sorted(allowed)}")
         self._v[name] = typ(value)
@@ -335,6 +338,7 @@ def _params(opt: Options, lib) -> _Params:
     prm.grid_blocks = opt.get("pdhg_grid_blocks")
     prm.profile_kernels = int(opt.get("pdhg_profile_kernels"))
     prm.mixed_stall_checks = opt.get("pdhg_mixed_stall_checks")
+    prm.algorithm = ALGORITHMS[opt.get("pdhg_algorithm")]
     return prm
 
 
