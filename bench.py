@@ -179,7 +179,7 @@ def _percentiles(values):
             "p99.9": float(np.percentile(v, 99.9))}
 
 
-def batched_leg(local, world, rank, dist, torch):
+def batched_leg(local, world, rank, dist, torch, algorithm="halpern"):
     """512 uneven LPs through the batched engine (sharded over ranks), and a one-at-a-time
     FP64 sample on rank 0."""
     from sih26_b200 import lpgen, pdhg
@@ -188,7 +188,7 @@ def batched_leg(local, world, rank, dist, torch):
     lps = lpgen.uneven_batch(count=512, m_lo=50, m_hi=5000, infeasible_fraction=0.1, seed=3)
     mine = shard_by_nnz([lp.num_nonzeros for lp in lps], world)[rank]
     opts = pdhg.Options(pdhg_tolerance=TOLERANCE, pdhg_stop_rule="relative_kkt",
-                        gpu_device=local)
+                        gpu_device=local, pdhg_algorithm=algorithm)
 
     def sync():
         torch.cuda.synchronize()
@@ -222,7 +222,13 @@ def batched_leg(local, world, rank, dist, torch):
     # one at a time, plain FP64, on every 8th LP (its feasible ones, and its infeasible ones
     # with the certificate test that the single-LP path also runs)
     sample = list(range(0, len(lps), 8))
-    one_rate = one_at_a_time([lps[k] for k in sample], local)
+    one_rate = one_at_a_time([lps[k] for k in sample], local, algorithm)
+    # the reference operator on the same batch, for comparison
+    other = "reference" if algorithm == "halpern" else "halpern"
+    t0 = time.perf_counter()
+    pdhg.batch_solve(lps, pdhg.Options(pdhg_tolerance=TOLERANCE, pdhg_stop_rule="relative_kkt",
+                                       gpu_device=local, pdhg_algorithm=other))
+    other_rate = len(lps) / (time.perf_counter() - t0)
     rate = len(lps) / wall
     return {
         "workload": "512 uneven LPs, m log-uniform [50, 5000], n = m U(1.5,3), 5-15 nnz/col, "
@@ -232,8 +238,9 @@ def batched_leg(local, world, rank, dist, torch):
         "latency_s": _percentiles([allres[k][2] for k in range(len(lps))]),
         "met_tolerance": met, "feasible_lps": len(lps) - planted_infeasible,
         "certified_infeasible": certified, "planted_infeasible": planted_infeasible,
-        "precision": "fp64",
-        "one_at_a_time_fp64": {"value": one_rate, "unit": "LPs/s",
+        "precision": "fp64", "algorithm": algorithm,
+        f"{other}_operator": {"value": other_rate, "unit": "LPs/s"},
+        "one_at_a_time_fp64": {"value": one_rate, "unit": "LPs/s", "algorithm": algorithm,
                                "sample": f"every 8th LP ({len(sample)}), once each"},
         "speedup_vs_one_at_a_time": rate / one_rate,
         "sharding": f"{world} rank(s), by nonzeros" if world > 1 else "single GPU",
@@ -257,12 +264,12 @@ def served_family(count, seed):
     return out
 
 
-def one_at_a_time(lps, local):
+def one_at_a_time(lps, local, algorithm):
     """LPs/s of the plain FP64 single-LP path, one LP after another (after one warm-up)."""
     from sih26_b200 import pdhg
 
     one = pdhg.Options(pdhg_tolerance=TOLERANCE, pdhg_stop_rule="relative_kkt",
-                       pdhg_precision="fp64", gpu_device=local)
+                       pdhg_precision="fp64", gpu_device=local, pdhg_algorithm=algorithm)
     pdhg.solve_pdhg(lps[0], one)
     t0 = time.perf_counter()
     for lp in lps:
@@ -270,7 +277,8 @@ def one_at_a_time(lps, local):
     return len(lps) / (time.perf_counter() - t0)
 
 
-def served_leg(local, rates, seconds, chunk, pool_size=24, seed=5, drain_cap=90.0):
+def served_leg(local, rates, seconds, chunk, algorithm="halpern", pool_size=24, seed=5,
+               drain_cap=90.0):
     """A Poisson stream at each rate (LPs/s) for `seconds` into a resident server."""
     import concurrent.futures as cf
 
@@ -279,9 +287,9 @@ def served_leg(local, rates, seconds, chunk, pool_size=24, seed=5, drain_cap=90.
     from sih26_b200 import pdhg
 
     pool = served_family(pool_size, seed)
-    base_rate = one_at_a_time(pool, local)
+    base_rate = one_at_a_time(pool, local, algorithm)
     opts = pdhg.Options(pdhg_tolerance=TOLERANCE, pdhg_stop_rule="relative_kkt",
-                        gpu_device=local)
+                        gpu_device=local, pdhg_algorithm=algorithm)
     out = []
     for rate in rates:
         rng = np.random.default_rng(seed + 1)
@@ -331,7 +339,7 @@ def served_leg(local, rates, seconds, chunk, pool_size=24, seed=5, drain_cap=90.
                                        if v in ("optimal", "feasible")),
             "value": served_rate, "unit": "LPs/s", "span_s": span,
             "latency_s": _percentiles(list(latency.values())), "chunk_attempts": chunk,
-            "precision": "fp64",
+            "precision": "fp64", "algorithm": algorithm,
             "one_at_a_time_fp64": {"value": base_rate, "unit": "LPs/s",
                                    "sample": f"the {pool_size} LPs of the pool, once each"},
             "speedup_vs_one_at_a_time": (served_rate / base_rate) if served_rate else None,
@@ -470,11 +478,13 @@ def run_ours(args):
                           f"iterations ({per_it * 1e3:.2f} ms each), extrapolated to the "
                           f"{fp64.iterations} iterations the FP64 GPU leg needed")}
     launches = int(statistics.mean(s.kernel_launches for s in sols))
-    batched = None if args.no_batched else batched_leg(local, world, rank, dist, torch)
+    batched = (None if args.no_batched
+               else batched_leg(local, world, rank, dist, torch, args.algorithm))
     served = None
     if rank == 0 and not args.no_served:
         rates = [float(r) for r in args.served_rates.split(",") if r]
-        served = served_leg(local, rates, args.served_seconds, args.served_chunk)
+        served = served_leg(local, rates, args.served_seconds, args.served_chunk,
+                            args.algorithm)
     if rank == 0:
         line = {
             "metric": "time-to-rel-KKT 1e-6 (s), FP32-mixed", "value": dev, "unit": "s",

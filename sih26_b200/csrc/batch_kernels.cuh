@@ -145,6 +145,9 @@ __device__ __noinline__ void group_evaluate(const BatchSlot& B, Ctrl& c, double*
   const bool has_average = c.averaged > 0;
   const double count = (double)c.averaged;
   const bool test_cert = c.farkas_cooldown == 0 && (c.evaluations % kCertEvery) == kCertEvery - 1;
+  // the Halpern operator's second candidate is the PDHG output T(z_k), not an average
+  const bool halpern = c.halpern != 0;
+  const double* ray_from = halpern ? S.xt : S.x[cur];
   // E1: running sums and averages, the movement since the last restart (mv) and the
   // certificates' row / column terms (ec, see certificate_test)
   double mv[2] = {0.0, 0.0};
@@ -155,11 +158,11 @@ __device__ __noinline__ void group_evaluate(const BatchSlot& B, Ctrl& c, double*
     const double xo = ld(S.x[cur] + j);
     const double xs = S.xsum[j] + (c.pending ? xo : 0.0);
     S.xsum[j] = xs;
-    S.xavg[j] = has_average ? xs / count : 0.0;
+    S.xavg[j] = has_average ? (halpern ? S.xt[j] : xs / count) : 0.0;
     const double d = xo - ld(S.xr + j);
     mv[0] += d * d;
     if (test_cert) {
-      const double r = __ldg(P.dc + j) * (xo - ld(S.x[prev] + j));
+      const double r = __ldg(P.dc + j) * (ld(ray_from + j) - ld(S.x[prev] + j));
       ray_col_terms(r, __ldg(P.cl0 + j), __ldg(P.cu0 + j), __ldg(P.c0 + j), ec);
     }
   }
@@ -167,7 +170,7 @@ __device__ __noinline__ void group_evaluate(const BatchSlot& B, Ctrl& c, double*
     const double yo = ld(S.y[cur] + i);
     const double ys = S.ysum[i] + (c.pending ? yo : 0.0);
     S.ysum[i] = ys;
-    S.yavg[i] = has_average ? ys / count : 0.0;
+    S.yavg[i] = has_average ? (halpern ? S.yt[i] : ys / count) : 0.0;
     const double d = yo - ld(S.yr + i);
     mv[1] += d * d;
     if (test_cert) farkas_row_terms(-__ldg(P.dr + i) * d, __ldg(P.rl0 + i), __ldg(P.ru0 + i), ec);
@@ -191,7 +194,7 @@ __device__ __noinline__ void group_evaluate(const BatchSlot& B, Ctrl& c, double*
     run_phase<1, 3>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pat, DiffGather<double, double>{S.y[cur], S.yr},
                     FarkasCol{P.dc, P.cl0, P.cu0}, fk, stream, rank);
     grp.template reduce<3, kFarkasColMaxMask>(fk, sh);
-    run_phase<1, 2>(P.A.ptr, P.A.idx, P.A.val64, P.pa, DiffGather<double, double>{S.x[cur], S.x[prev]},
+    run_phase<1, 2>(P.A.ptr, P.A.idx, P.A.val64, P.pa, DiffGather<double, double>{ray_from, S.x[prev]},
                     RayRow{P.dr, P.rl0, P.ru0}, rr, stream, rank);
     grp.template reduce<2, 3u>(rr, sh);
   }
@@ -223,7 +226,7 @@ __device__ __noinline__ void group_evaluate(const BatchSlot& B, Ctrl& c, double*
   if (flags[0] || flags[1] || flags[3]) {
     for (int j = base; j < P.n; j += stride) {
       const double xo = ld(S.x[cur] + j);
-      if (flags[3] == 2) B.ray_out[j] = __ldg(P.dc + j) * (xo - ld(S.x[prev] + j)) / scale;
+      if (flags[3] == 2) B.ray_out[j] = __ldg(P.dc + j) * (ld(ray_from + j) - ld(S.x[prev] + j)) / scale;
       if (flags[0]) S.best_x[j] = flags[2] ? S.xavg[j] : xo;
       if (flags[1]) {
         S.xr[j] = S.x[cur][j];
@@ -237,6 +240,7 @@ __device__ __noinline__ void group_evaluate(const BatchSlot& B, Ctrl& c, double*
       if (flags[1]) {
         S.yr[i] = S.y[cur][i];
         S.ysum[i] = 0.0;
+        if (halpern) S.axr[i] = S.ax[cur][i];  // A x_0 of the new restart point
       }
     }
   }
@@ -279,6 +283,7 @@ __device__ inline void run_instance(const BatchSlot& B, Ctrl& c, double* sh, dou
     if (threadIdx.x == 0) {
       c.spectral_norm = norm;
       c.eta = norm > 0.0 ? 1.0 / norm : 1.0;
+      if (c.halpern) c.eta = 0.998 / dmax(norm, 1e-12);  // constant: tau sigma ||A||^2 < 1
       c.eta_ceiling = 1.0e3 / dmax(norm, 1e-12);
       c.state = kRunning;
     }
@@ -286,6 +291,11 @@ __device__ inline void run_instance(const BatchSlot& B, Ctrl& c, double* sh, dou
     run_phase<1, 1>(P.A.ptr, P.A.idx, P.A.val, P.pa, Gather1<double>{S.x[0]},
                     StoreRow<1>{S.ax[0], -1}, dummy, stream, rank);
     grp.sync();
+    if (c.halpern) {  // A x_0 of the starting point
+      const int base = rank * kThreads + threadIdx.x, stride = Grp::kSize * kThreads;
+      for (int i = base; i < P.m; i += stride) S.axr[i] = S.ax[0][i];
+      grp.sync();
+    }
   }
   long long a = 0;
   while (c.state == kRunning) {
@@ -311,6 +321,24 @@ __device__ inline void run_instance(const BatchSlot& B, Ctrl& c, double* sh, dou
     const double tau = c.eta / c.omega;
     const double sigma = c.eta * c.omega;
     double acc[3] = {0.0, 0.0, 0.0};
+    if (c.halpern) {
+      // the Halpern operator (see PrimalStepHalpern in pdhg_kernels.cuh)
+      const double w = (double)(c.averaged + 1) / (double)(c.averaged + 2);
+      run_phase<1, 3>(P.AT.ptr, P.AT.idx, P.AT.val, P.pat, Gather1<double>{S.y[cur]},
+                      PrimalStepHalpern<double>{S.x[cur], S.x[nxt], S.xt, P.c, P.cl, P.cu, S.xr,
+                                                tau, w},
+                      acc, stream, rank);
+      grp.sync();
+      run_phase<1, 3>(P.A.ptr, P.A.idx, P.A.val, P.pa, Gather1<double>{S.x[nxt]},
+                      DualStepHalpern<double>{S.y[cur], S.y[nxt], S.yt, S.ax[nxt], P.rl, P.ru,
+                                              S.yr, S.axr, sigma, w},
+                      acc, stream, rank);
+      grp.sync();
+      if (threadIdx.x == 0) halpern_control(c);
+      __syncthreads();
+      if (c.state == kNeedEval) group_evaluate(B, c, sh, stream, flags, grp);
+      continue;
+    }
     {
       PrimalStep<double> ps{S.x[cur], S.x[nxt], P.c, P.cl, P.cu, S.xsum, tau, c.pending};
       run_phase<1, 3>(P.AT.ptr, P.AT.idx, P.AT.val, P.pat, Gather1<double>{S.y[cur]}, ps, acc,

@@ -77,6 +77,7 @@ struct Job {
     PartOff pa, pat;
     size_t c, cl, cu, rl, ru, dr, dc, c0, cl0, cu0, rl0, ru0;
     size_t x0, x1, y0, y1, ax0, ax1, xsum, ysum, xr, yr, xavg, yavg, best_x, best_y;
+    size_t xt, yt, axr;  // the Halpern operator's T(z) and A x_0
     size_t x_out, red_out, y_out, farkas_out, ray_out;
   } off{};
   Ctrl ctrl0{};
@@ -175,10 +176,10 @@ void prepare(Job& J, const sankhya_pdhg_problem& p, const sankhya_pdhg_params& p
   o.pa = part_off(pa);
   o.pat = part_off(pat);
   for (size_t* f : {&o.c, &o.cl, &o.cu, &o.dc, &o.c0, &o.cl0, &o.cu0, &o.x0, &o.x1, &o.xsum,
-                    &o.xr, &o.xavg, &o.best_x, &o.x_out, &o.red_out, &o.ray_out})
+                    &o.xr, &o.xavg, &o.best_x, &o.x_out, &o.red_out, &o.ray_out, &o.xt})
     *f = L.put(n * 8);
   for (size_t* f : {&o.rl, &o.ru, &o.dr, &o.rl0, &o.ru0, &o.y0, &o.y1, &o.ax0, &o.ax1, &o.ysum,
-                    &o.yr, &o.yavg, &o.best_y, &o.y_out, &o.farkas_out})
+                    &o.yr, &o.yavg, &o.best_y, &o.y_out, &o.farkas_out, &o.yt, &o.axr})
     *f = L.put(m * 8);
   J.image.assign(L.bytes, 0);
   auto& img = J.image;
@@ -242,6 +243,7 @@ void prepare(Job& J, const sankhya_pdhg_problem& p, const sankhya_pdhg_params& p
   c.stop_at_request = prm.stop_at_request ? 1 : 0;
   c.stop_rule = prm.stop_rule;
   c.farkas_cooldown = prm.detect_infeasibility ? 0 : (1 << 30);
+  c.halpern = prm.algorithm == SANKHYA_PDHG_ALGORITHM_HALPERN ? 1 : 0;
 }
 
 // First-fit allocator over the pool, coalescing on free.
@@ -368,6 +370,9 @@ BatchSlot relocate(const Job& J, unsigned char* base, Ctrl* ctrl) {
   S.yavg = D(o.yavg);
   S.best_x = D(o.best_x);
   S.best_y = D(o.best_y);
+  S.xt = D(o.xt);
+  S.yt = D(o.yt);
+  S.axr = D(o.axr);
   S.partials = nullptr;
   S.ctrl = ctrl;
   b.x_out = D(o.x_out);

@@ -99,3 +99,32 @@ def test_certificates():
     s = P.solve_pdhg(unb, _opts(pdhg_tolerance=1e-6, iteration_limit=200000))
     assert s.status == "unbounded", s.message
     assert ray_ok(unb, s.primal_ray)[0]
+
+
+def test_batched_engine_with_the_halpern_operator():
+    """Batched: every feasible LP meets the request, certificates pass the reference's
+    checkers, and each answer is the same alone, in the mix and when served in chunks."""
+    rng = np.random.default_rng(9)
+    lps = lpgen.uneven_batch(count=24, m_lo=50, m_hi=600, infeasible_fraction=0.2, seed=13)
+    lps.append(lpgen.make_unbounded(lpgen.uniform_planted(80, 200, 4, seed=3), rng))
+    opts = _opts(pdhg_tolerance=1e-6, pdhg_stop_rule="relative_kkt", iteration_limit=200000)
+    sols = P.batch_solve(lps, opts)
+    for lp, s in zip(lps, sols):
+        if lp.farkas_star is not None:
+            assert s.status == "infeasible", (lp.name, s.status, s.message)
+            assert farkas_ok(lp, s.farkas_dual)[0], lp.name
+        elif lp.ray_star is not None:
+            assert s.status == "unbounded", (lp.name, s.status, s.message)
+            assert ray_ok(lp, s.primal_ray)[0], lp.name
+        else:
+            assert s.status in ("optimal", "feasible"), (lp.name, s.status, s.message)
+            r = oracle.oracle_evaluate(lp, s.col_value, -s.row_dual)
+            assert max(r["primal"], r["dual"], r["gap"]) <= 1e-6, (lp.name, r)
+    alone = P.batch_solve([lps[5]], opts)[0]
+    assert alone.iterations == sols[5].iterations
+    assert np.array_equal(alone.col_value, sols[5].col_value)
+    with P.Server(chunk_attempts=100) as srv:
+        chunked = srv.solve_all(lps[:8], opts)
+    for a, b in zip(chunked, sols[:8]):
+        assert a.status == b.status and a.iterations == b.iterations
+        assert np.array_equal(a.col_value, b.col_value)
