@@ -525,10 +525,10 @@ def run_ours(args):
     return 0
 
 
-def profile_run(kind):
+def profile_run(kind, algorithm):
     """Bounded runs for ncu captures (no timing, no JSON): `single` runs the 5M-nonzero LP for
     200 iterations in FP32-mixed and again in FP64; `batch` solves the first 64 LPs of the
-    batched family in one batched call."""
+    batched family in one batched call; both with the operator of --algorithm."""
     from sih26_b200 import lpgen, pdhg
 
     if kind == "single":
@@ -536,12 +536,14 @@ def profile_run(kind):
         for precision in ("mixed", "fp64"):
             s = pdhg.solve_pdhg(lp, pdhg.Options(pdhg_tolerance=TOLERANCE, iteration_limit=200,
                                                  pdhg_stop_rule="relative_kkt",
-                                                 pdhg_precision=precision))
+                                                 pdhg_precision=precision,
+                                                 pdhg_algorithm=algorithm))
             print(precision, s.status, s.iterations, s.kernel_launches)
     else:
         lps = lpgen.uneven_batch(count=512, m_lo=50, m_hi=5000, infeasible_fraction=0.1, seed=3)
         sols = pdhg.batch_solve(lps[:64], pdhg.Options(pdhg_tolerance=TOLERANCE,
-                                                       pdhg_stop_rule="relative_kkt"))
+                                                       pdhg_stop_rule="relative_kkt",
+                                                       pdhg_algorithm=algorithm))
         print("batch", sum(s.status in ("optimal", "feasible", "infeasible") for s in sols))
     return 0
 
@@ -567,7 +569,7 @@ def main():
                     help="a bounded run for an ncu capture (prints no bench line)")
     args = ap.parse_args()
     if args.profile_run:
-        return profile_run(args.profile_run)
+        return profile_run(args.profile_run, args.algorithm)
     if args.warmup < 3:
         raise SystemExit("at least 3 warm-up steps")
     if args.impl == "reference":

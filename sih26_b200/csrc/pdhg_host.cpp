@@ -7,10 +7,30 @@
 #include <numeric>
 #include <queue>
 #include <string>
+#include <thread>
 
 namespace sih26 {
 
 bool host_finite_bound(double v) { return !(std::isinf(v) || std::fabs(v) >= 1e30); }
+
+// Runs fn(part, parts) on `parts` host threads (the calling thread takes part 0). The host
+// preparation below splits work so that every output element is written by one thread and
+// every floating-point sum keeps the reference's order: results do not depend on `parts`.
+static int host_parts(long long work) {
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const long long by_work = std::max(1ll, work / 200000);
+  return static_cast<int>(std::min<long long>(std::min(hw, 32u), by_work));
+}
+template <class F>
+static void parallel_parts(int parts, F fn) {
+  std::vector<std::thread> pool;
+  for (int t = 1; t < parts; ++t) pool.emplace_back(fn, t, parts);
+  fn(0, parts);
+  for (auto& th : pool) th.join();
+}
+static inline int split(int count, int part, int parts) {
+  return static_cast<int>(static_cast<long long>(count) * part / parts);
+}
 
 // farkas_proves_infeasible (src/core/certificate.cpp:29-119) on the ABI's problem: every
 // multiplier leans on a bound its row has; d = A'y; the column box reaches at most
@@ -266,55 +286,105 @@ std::string validate_model(const sankhya_pdhg_problem& p) {
 
 // apply_pass (src/la/scaling.cpp:14-40): the reference rebuilds the matrix through
 // add_entry + finalize(0.0), which keeps pattern and order, i.e. value * row_pass * col_pass.
-static void apply_pass(const sankhya_pdhg_problem& p, Scaling& s, const std::vector<double>& rp,
-                       const std::vector<double>& cp) {
-  for (int j = 0; j < p.num_cols; ++j) {
-    const double cj = cp[j];
-    for (int k = p.col_starts[j]; k < p.col_starts[j + 1]; ++k) {
-      s.values[k] = s.values[k] * rp[p.row_indices[k]] * cj;
+// A row-major copy of the matrix values (each row's entries in ascending column order), kept
+// in step with the column-major values: every pass multiplies both copies by the same factors
+// in the same order, so they hold the same bits.
+struct RowView {
+  std::vector<int> ptr, col;
+  std::vector<double> val;
+};
+static RowView row_view(const sankhya_pdhg_problem& p, int parts) {
+  RowView r;
+  const int m = p.num_rows;
+  r.ptr.assign(m + 1, 0);
+  for (long long k = 0; k < p.num_nonzeros; ++k) ++r.ptr[p.row_indices[k] + 1];
+  for (int i = 0; i < m; ++i) r.ptr[i + 1] += r.ptr[i];
+  r.col.resize(p.num_nonzeros);
+  r.val.resize(p.num_nonzeros);
+  // a thread owns a range of rows and places only their entries
+  parallel_parts(parts, [&](int part, int np) {
+    const int r0 = split(m, part, np), r1 = split(m, part + 1, np);
+    std::vector<int> next(r.ptr.begin() + r0, r.ptr.begin() + r1);
+    for (int j = 0; j < p.num_cols; ++j) {
+      for (int k = p.col_starts[j]; k < p.col_starts[j + 1]; ++k) {
+        const int i = p.row_indices[k];
+        if (i < r0 || i >= r1) continue;
+        const int t = next[i - r0]++;
+        r.col[t] = j;
+        r.val[t] = p.values[k];
+      }
     }
-  }
+  });
+  return r;
+}
+
+static void apply_pass(const sankhya_pdhg_problem& p, Scaling& s, RowView& rv,
+                       const std::vector<double>& rp, const std::vector<double>& cp, int parts) {
+  parallel_parts(parts, [&](int part, int np) {
+    for (int j = split(p.num_cols, part, np); j < split(p.num_cols, part + 1, np); ++j) {
+      const double cj = cp[j];
+      for (int k = p.col_starts[j]; k < p.col_starts[j + 1]; ++k) {
+        s.values[k] = s.values[k] * rp[p.row_indices[k]] * cj;
+      }
+    }
+    for (int i = split(p.num_rows, part, np); i < split(p.num_rows, part + 1, np); ++i) {
+      const double ri = rp[i];
+      for (int t = rv.ptr[i]; t < rv.ptr[i + 1]; ++t) rv.val[t] = rv.val[t] * ri * cp[rv.col[t]];
+    }
+  });
   for (int i = 0; i < p.num_rows; ++i) s.dr[i] *= rp[i];
   for (int j = 0; j < p.num_cols; ++j) s.dc[j] *= cp[j];
+}
+
+// Per-row and per-column max |a| (Ruiz) or sum |a| (Pock-Chambolle) of the current values.
+// Each row and each column is reduced by one thread in ascending order of the other index,
+// which is the order the reference accumulates in (column by column, scaling.cpp:44-100), so
+// the sums are bit-identical to it whatever the thread count.
+static void row_col_norms(const sankhya_pdhg_problem& p, const RowView& rv, const Scaling& s,
+                          bool sum, std::vector<double>& ra, std::vector<double>& ca, int parts) {
+  const int m = p.num_rows, n = p.num_cols;
+  parallel_parts(parts, [&](int part, int np) {
+    for (int j = split(n, part, np); j < split(n, part + 1, np); ++j) {
+      double acc = 0.0;
+      for (int k = p.col_starts[j]; k < p.col_starts[j + 1]; ++k) {
+        const double mag = std::fabs(s.values[k]);
+        acc = sum ? acc + mag : std::max(acc, mag);
+      }
+      ca[j] = acc;
+    }
+    for (int i = split(m, part, np); i < split(m, part + 1, np); ++i) {
+      double acc = 0.0;
+      for (int t = rv.ptr[i]; t < rv.ptr[i + 1]; ++t) {
+        const double mag = std::fabs(rv.val[t]);
+        acc = sum ? acc + mag : std::max(acc, mag);
+      }
+      ra[i] = acc;
+    }
+  });
 }
 
 Scaling build_scaling(const sankhya_pdhg_problem& p, const std::vector<double>& min_cost,
                       int ruiz_rounds) {
   const int m = p.num_rows, n = p.num_cols;
+  const int parts = host_parts(p.num_nonzeros);
   Scaling s;
   s.dr.assign(m, 1.0);
   s.dc.assign(n, 1.0);
   s.values.assign(p.values, p.values + p.num_nonzeros);
   std::vector<double> ra(m), ca(n), rp(m), cp(n);
+  RowView rv = row_view(p, parts);
   // ruiz_round (scaling.cpp:44-72): 1/sqrt(max |a|) per row and column
   for (int round = 0; round < ruiz_rounds; ++round) {
-    std::fill(ra.begin(), ra.end(), 0.0);
-    std::fill(ca.begin(), ca.end(), 0.0);
-    for (int j = 0; j < n; ++j) {
-      for (int k = p.col_starts[j]; k < p.col_starts[j + 1]; ++k) {
-        const double mag = std::fabs(s.values[k]);
-        double& r = ra[p.row_indices[k]];
-        r = std::max(r, mag);
-        ca[j] = std::max(ca[j], mag);
-      }
-    }
+    row_col_norms(p, rv, s, false, ra, ca, parts);
     for (int i = 0; i < m; ++i) rp[i] = ra[i] > 0.0 ? 1.0 / std::sqrt(ra[i]) : 1.0;
     for (int j = 0; j < n; ++j) cp[j] = ca[j] > 0.0 ? 1.0 / std::sqrt(ca[j]) : 1.0;
-    apply_pass(p, s, rp, cp);
+    apply_pass(p, s, rv, rp, cp, parts);
   }
   // pock_chambolle_round (scaling.cpp:76-100), alpha = 1: 1/sqrt(sum |a|)
-  std::fill(ra.begin(), ra.end(), 0.0);
-  std::fill(ca.begin(), ca.end(), 0.0);
-  for (int j = 0; j < n; ++j) {
-    for (int k = p.col_starts[j]; k < p.col_starts[j + 1]; ++k) {
-      const double mag = std::fabs(s.values[k]);
-      ra[p.row_indices[k]] += mag;
-      ca[j] += mag;
-    }
-  }
+  row_col_norms(p, rv, s, true, ra, ca, parts);
   for (int i = 0; i < m; ++i) rp[i] = ra[i] > 0.0 ? 1.0 / std::sqrt(ra[i]) : 1.0;
   for (int j = 0; j < n; ++j) cp[j] = ca[j] > 0.0 ? 1.0 / std::sqrt(ca[j]) : 1.0;
-  apply_pass(p, s, rp, cp);
+  apply_pass(p, s, rv, rp, cp, parts);
   // vectors (scaling.cpp:124-145); scale_bound multiplies by 1/dc, it does not divide
   s.cost.resize(n);
   s.cl.resize(n);
@@ -335,17 +405,22 @@ Scaling build_scaling(const sankhya_pdhg_problem& p, const std::vector<double>& 
   return s;
 }
 
+// Positions sorted by count, largest first, ties in index order (a stable counting sort).
 static std::vector<int> order_by_count_desc(const std::vector<int>& count) {
+  int top = 0;
+  for (int c : count) top = std::max(top, c);
+  std::vector<int> start(static_cast<size_t>(top) + 2, 0);
+  for (int c : count) ++start[top - c + 1];
+  for (int b = 1; b <= top + 1; ++b) start[b] += start[b - 1];
   std::vector<int> order(count.size());
-  std::iota(order.begin(), order.end(), 0);
-  std::stable_sort(order.begin(), order.end(),
-                   [&](int a, int b) { return count[a] > count[b]; });
+  for (int i = 0; i < static_cast<int>(count.size()); ++i) order[start[top - count[i]]++] = i;
   return order;
 }
 
 PermutedLp permute(const sankhya_pdhg_problem& p, const std::vector<double>& v) {
   PermutedLp q;
   const int m = p.num_rows, n = p.num_cols;
+  const int parts = host_parts(p.num_nonzeros);
   q.m = m;
   q.n = n;
   q.nnz = p.num_nonzeros;
@@ -357,33 +432,44 @@ PermutedLp permute(const sankhya_pdhg_problem& p, const std::vector<double>& v) 
   std::vector<int> row_pos(m), col_pos(n);
   for (int t = 0; t < m; ++t) row_pos[q.row_perm[t]] = t;
   for (int t = 0; t < n; ++t) col_pos[q.col_perm[t]] = t;
-  // A: rows in permuted order; walking permuted columns in order keeps each row ascending
+  // A: rows in permuted order; walking permuted columns in order keeps each row ascending.
+  // A thread owns a range of permuted rows and places only their entries.
   q.a_ptr.assign(m + 1, 0);
   for (int t = 0; t < m; ++t) q.a_ptr[t + 1] = q.a_ptr[t] + rc[q.row_perm[t]];
   q.a_idx.resize(q.nnz);
   q.a_val.resize(q.nnz);
-  std::vector<int> next(q.a_ptr.begin(), q.a_ptr.end() - 1);
-  for (int t = 0; t < n; ++t) {
-    const int j = q.col_perm[t];
-    for (int k = p.col_starts[j]; k < p.col_starts[j + 1]; ++k) {
-      const int slot = next[row_pos[p.row_indices[k]]]++;
-      q.a_idx[slot] = t;
-      q.a_val[slot] = v[k];
+  parallel_parts(parts, [&](int part, int np) {
+    const int r0 = split(m, part, np), r1 = split(m, part + 1, np);
+    std::vector<int> next(q.a_ptr.begin() + r0, q.a_ptr.begin() + r1);
+    for (int t = 0; t < n; ++t) {
+      const int j = q.col_perm[t];
+      for (int k = p.col_starts[j]; k < p.col_starts[j + 1]; ++k) {
+        const int r = row_pos[p.row_indices[k]];
+        if (r < r0 || r >= r1) continue;
+        const int slot = next[r - r0]++;
+        q.a_idx[slot] = t;
+        q.a_val[slot] = v[k];
+      }
     }
-  }
+  });
   // A': rows are permuted columns; walking permuted rows in order keeps each ascending
   q.at_ptr.assign(n + 1, 0);
   for (int t = 0; t < n; ++t) q.at_ptr[t + 1] = q.at_ptr[t] + cc[q.col_perm[t]];
   q.at_idx.resize(q.nnz);
   q.at_val.resize(q.nnz);
-  next.assign(q.at_ptr.begin(), q.at_ptr.end() - 1);
-  for (int t = 0; t < m; ++t) {
-    for (int k = q.a_ptr[t]; k < q.a_ptr[t + 1]; ++k) {
-      const int slot = next[q.a_idx[k]]++;
-      q.at_idx[slot] = t;
-      q.at_val[slot] = q.a_val[k];
+  parallel_parts(parts, [&](int part, int np) {
+    const int c0 = split(n, part, np), c1 = split(n, part + 1, np);
+    std::vector<int> next(q.at_ptr.begin() + c0, q.at_ptr.begin() + c1);
+    for (int t = 0; t < m; ++t) {
+      for (int k = q.a_ptr[t]; k < q.a_ptr[t + 1]; ++k) {
+        const int c = q.a_idx[k];
+        if (c < c0 || c >= c1) continue;
+        const int slot = next[c - c0]++;
+        q.at_idx[slot] = t;
+        q.at_val[slot] = q.a_val[k];
+      }
     }
-  }
+  });
   return q;
 }
 
