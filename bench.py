@@ -406,9 +406,11 @@ def run_ours(args):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
 
     def opts(precision, algorithm, profile=False):
+        # the autotuner measures the schedules in the first warm-up solve and caches them
         return pdhg.Options(pdhg_tolerance=TOLERANCE, pdhg_stop_rule="relative_kkt",
                             pdhg_precision=precision, pdhg_algorithm=algorithm,
-                            gpu_device=local, pdhg_profile_kernels=profile)
+                            gpu_device=local, pdhg_profile_kernels=profile,
+                            pdhg_autotune=True)
 
     def sync():
         torch.cuda.synchronize()
@@ -498,6 +500,10 @@ def run_ours(args):
                              "256 MB L2 flush before every step",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
             "iterations": last.iterations, "fp32_iterations": last.fp32_iterations,
+            "schedule": {"autotuned": last.autotuned, "stream_row_max_A": last.schedule[0],
+                         "nnz_per_lane_A": last.schedule[1],
+                         "stream_row_max_AT": last.schedule[2],
+                         "nnz_per_lane_AT": last.schedule[3]},
             "attempts": last.attempts, "restarts": last.restarts,
             "objective_rel_error": abs(last.objective - lp.optimal_objective)
             / abs(lp.optimal_objective),

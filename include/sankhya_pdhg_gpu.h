@@ -142,7 +142,12 @@ typedef struct sankhya_pdhg_params {
                                  better KKT error before the FP32 phase hands over; 0 = auto
                                  (no 1% gain over the last 30% of the iterations), -1 = never */
   int32_t algorithm;        /* SANKHYA_PDHG_ALGORITHM_REFERENCE (default) or _HALPERN */
-  int32_t reserved[4];
+  int32_t autotune;         /* 1: pick the SpMV schedule of A and A' (rows per stream item,
+                               nonzeros per lane) by timing candidates on this LP, keyed on its
+                               row-length statistics and cached on disk
+                               (SANKHYA_PDHG_AUTOTUNE_CACHE, else ~/.cache/sih26_b200/
+                               autotune.tsv); 0 (default): the fixed rule */
+  int32_t reserved[3];
 } sankhya_pdhg_params;
 
 /* Unscaled residual block of the reported point (src/pdhg/pdhg.cpp:81-110). */
@@ -186,6 +191,8 @@ typedef struct sankhya_pdhg_result {
   int64_t iterate_launches;      /* profile_kernels: how many were timed */
   int64_t kernel_launches;       /* every kernel this call launched */
   sankhya_pdhg_residuals residuals;
+  int32_t autotuned;    /* 0 fixed rule, 1 schedule measured by this call, 2 read from cache */
+  int32_t schedule[4];  /* stream-row limit and nonzeros per lane of A, then of A' */
   char message[512];
 } sankhya_pdhg_result;
 

@@ -8,6 +8,9 @@
 #include <queue>
 #include <string>
 #include <thread>
+#include <cstdio>
+#include <cstdlib>
+#include <sys/stat.h>
 
 namespace sih26 {
 
@@ -473,10 +476,10 @@ PermutedLp permute(const sankhya_pdhg_problem& p, const std::vector<double>& v) 
   return q;
 }
 
-static int lanes_for(int len) {
-  // smallest power of two with at most sixteen nonzeros per lane, capped at a warp
+static int lanes_for(int len, int nnz_per_lane) {
+  // smallest power of two with at most nnz_per_lane nonzeros per lane, capped at a warp
   int lanes = 1;
-  while (lanes < 32 && lanes * 16 < len) lanes *= 2;
+  while (lanes < 32 && lanes * nnz_per_lane < len) lanes *= 2;
   return lanes;
 }
 
@@ -485,10 +488,13 @@ static int lanes_for(int len) {
 // item or segment, plus a small term for its nonzeros.
 static double unit_cost(int nnz) { return 1.0 + nnz / 2048.0; }
 
-HostPart partition(const std::vector<int>& ptr, int G, int warps_per_block, int lanes_override) {
+HostPart partition(const std::vector<int>& ptr, int G, int warps_per_block, int lanes_override,
+                   Schedule sched) {
   constexpr int kSeg = 512;        // == kSegment in pdhg_kernels.cuh
   constexpr int kItem = 512;       // == kItemNnz
-  constexpr int kStreamRow = 32;   // == kStreamRowMax
+  // rows up to this length go to stream items (at most kStreamRowMax = 32 rows per item)
+  const int kStreamRow = std::max(1, std::min(sched.stream_row_max, 32));
+  const int npl = std::max(1, sched.nnz_per_lane);
   (void)warps_per_block;
   const int rows = static_cast<int>(ptr.size()) - 1;
   const auto len = [&](int r) { return ptr[r + 1] - ptr[r]; };
@@ -501,12 +507,12 @@ HostPart partition(const std::vector<int>& ptr, int G, int warps_per_block, int 
   std::vector<double> item_cost;
   for (int r = L; r < rows;) {
     if (lanes_override > 0 || len(r) > kStreamRow) {
-      const int lanes = lanes_override > 0 ? lanes_override : lanes_for(len(r));
+      const int lanes = lanes_override > 0 ? lanes_override : lanes_for(len(r), npl);
       const int per = 32 / lanes;
       const int begin = r;
       int nnz = 0;
       while (r < rows && r - begin < per &&
-             (lanes_override > 0 || (len(r) > kStreamRow && lanes_for(len(r)) == lanes))) {
+             (lanes_override > 0 || (len(r) > kStreamRow && lanes_for(len(r), npl) == lanes))) {
         nnz += len(r);
         ++r;
       }
@@ -586,6 +592,92 @@ HostPart partition(const std::vector<int>& ptr, int G, int warps_per_block, int 
   (void)target;
   hp.items = std::move(items);
   return hp;
+}
+
+// ---- autotuner key and cache --------------------------------------------------------------
+
+static std::string sig2(double v) {  // two significant digits
+  char b[32];
+  std::snprintf(b, sizeof b, "%.2g", v);
+  return b;
+}
+
+static std::string length_stats(const std::vector<int>& ptr) {
+  const int rows = static_cast<int>(ptr.size()) - 1;
+  if (rows <= 0) return "empty";
+  double sum = 0.0, sq = 0.0, nnz_long = 0.0, nnz_mid = 0.0;
+  int mx = 0;
+  for (int r = 0; r < rows; ++r) {
+    const int len = ptr[r + 1] - ptr[r];
+    sum += len;
+    sq += static_cast<double>(len) * len;
+    mx = std::max(mx, len);
+    if (len > 512) nnz_long += len;
+    else if (len > 32) nnz_mid += len;
+  }
+  const double mean = sum / rows;
+  const double cv = mean > 0.0 ? std::sqrt(std::max(0.0, sq / rows - mean * mean)) / mean : 0.0;
+  const double tot = std::max(1.0, sum);
+  // fractions of the nonzeros in 33-512 and >512 nonzero rows, in steps of 0.05
+  const auto step = [](double f) { return sig2(std::round(f * 20.0) / 20.0); };
+  return "mean" + sig2(mean) + ",max" + sig2(mx) + ",cv" + sig2(cv) + ",mid" + step(nnz_mid / tot) +
+         ",long" + step(nnz_long / tot);
+}
+
+std::string autotune_key(const PermutedLp& q, int G, int sms, int value_bytes) {
+  const auto log2b = [](long long v) {
+    int b = 0;
+    while ((1ll << b) < v) ++b;
+    return std::to_string(b);
+  };
+  return "sm" + std::to_string(sms) + "|G" + std::to_string(G) + "|v" + std::to_string(value_bytes) +
+         "|m2^" + log2b(q.m) + "|n2^" + log2b(q.n) + "|nnz2^" + log2b(q.nnz) + "|rows:" +
+         length_stats(q.a_ptr) + "|cols:" + length_stats(q.at_ptr);
+}
+
+std::string autotune_cache_path() {
+  if (const char* e = std::getenv("SANKHYA_PDHG_AUTOTUNE_CACHE")) return e;
+  if (const char* x = std::getenv("XDG_CACHE_HOME")) return std::string(x) + "/sih26_b200/autotune.tsv";
+  if (const char* h = std::getenv("HOME")) return std::string(h) + "/.cache/sih26_b200/autotune.tsv";
+  return "sih26_b200_autotune.tsv";
+}
+
+// One line per key: key, then stream_row_max and nnz_per_lane for A and for A'. The last line
+// of a key wins.
+bool autotune_lookup(const std::string& path, const std::string& key, Schedule* a, Schedule* at) {
+  std::FILE* f = std::fopen(path.c_str(), "r");
+  if (!f) return false;
+  bool found = false;
+  char line[1024];
+  while (std::fgets(line, sizeof line, f)) {
+    char* tab = std::strchr(line, '\t');
+    if (!tab) continue;
+    if (std::string(line, tab - line) != key) continue;
+    Schedule x, y;
+    if (std::sscanf(tab + 1, "%d\t%d\t%d\t%d", &x.stream_row_max, &x.nnz_per_lane,
+                    &y.stream_row_max, &y.nnz_per_lane) == 4 &&
+        x.stream_row_max > 0 && x.nnz_per_lane > 0 && y.stream_row_max > 0 && y.nnz_per_lane > 0) {
+      *a = x;
+      *at = y;
+      found = true;
+    }
+  }
+  std::fclose(f);
+  return found;
+}
+
+void autotune_store(const std::string& path, const std::string& key, const Schedule& a,
+                    const Schedule& at, double us_a, double us_at) {
+  const size_t slash = path.find_last_of('/');
+  if (slash != std::string::npos) {  // create the directory chain (best effort)
+    for (size_t k = path.find('/', 1); k != std::string::npos && k <= slash; k = path.find('/', k + 1))
+      ::mkdir(path.substr(0, k).c_str(), 0755);
+  }
+  std::FILE* f = std::fopen(path.c_str(), "a");
+  if (!f) return;
+  std::fprintf(f, "%s\t%d\t%d\t%d\t%d\t%.2f\t%.2f\n", key.c_str(), a.stream_row_max,
+               a.nnz_per_lane, at.stream_row_max, at.nnz_per_lane, us_a, us_at);
+  std::fclose(f);
 }
 
 // mt19937 (Matsumoto & Nishimura) and libstdc++'s generate_canonical<double, 53> for a

@@ -55,12 +55,29 @@ struct PermutedLp {
 };
 PermutedLp permute(const sankhya_pdhg_problem& p, const std::vector<double>& scaled_values);
 
-// Work partition of one CSR matrix over G blocks (see Part in pdhg_kernels.cuh).
+// Work partition of one CSR matrix over G blocks (see Part in pdhg_kernels.cuh). The schedule
+// knobs: rows of at most stream_row_max nonzeros go to stream items (a warp loads a whole item
+// at once, lane r sums row r); longer rows up to 512 nonzeros get a power-of-two lane group
+// with at most nnz_per_lane nonzeros per lane.
+struct Schedule {
+  int stream_row_max = 32;
+  int nnz_per_lane = 16;
+};
 struct HostPart {
   std::vector<int> blk_seg_begin, blk_long_begin, blk_item_begin;
   std::vector<int4> segs, longs, items;
 };
-HostPart partition(const std::vector<int>& ptr, int G, int warps_per_block, int lanes_override);
+HostPart partition(const std::vector<int>& ptr, int G, int warps_per_block, int lanes_override,
+                   Schedule sched = Schedule{});
+
+// The autotuner's cache (one line per key, see pdhg_host.cpp). The key is built from the
+// row-length statistics of A and A' (mean, max, coefficient of variation, share of nonzeros
+// in 33-512 and >512 nonzero rows), power-of-two size buckets, the grid and the value width.
+std::string autotune_key(const PermutedLp& q, int G, int sms, int value_bytes);
+std::string autotune_cache_path();
+bool autotune_lookup(const std::string& path, const std::string& key, Schedule* a, Schedule* at);
+void autotune_store(const std::string& path, const std::string& key, const Schedule& a,
+                    const Schedule& at, double us_a, double us_at);
 
 // mt19937 + uniform_real_distribution<double>(lo, hi) as libstdc++ draws it: the random start
 // of estimate_spectral_norm (src/la/scaling.cpp:168-171).

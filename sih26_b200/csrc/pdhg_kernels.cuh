@@ -928,7 +928,9 @@ __global__ void __launch_bounds__(kThreads, 2) iterate_kernel(Prob<T> P, State<T
         PrimalStepHalpern<T> ps{S.x[cur], S.x[nxt], S.xt, P.c, P.cl, P.cu, S.xr, tau, w};
         run_phase<1, 3>(P.AT.ptr, P.AT.idx, P.AT.val, P.pat, Gather1<T>{S.y[cur]}, ps, acc, stream);
       }
+      SIH26_MARK(0);
       if (!grid_barrier(S.bar)) goto device_error;
+      SIH26_MARK(1);
       if constexpr (kDelta<T>) {
         DualStepHalpernDelta<T> ds{S.y[cur], S.y[nxt], S.yt, S.ax[nxt], S.yr, S.axr, P.rl64,
                                    P.ru64, sigma, w};
@@ -937,12 +939,15 @@ __global__ void __launch_bounds__(kThreads, 2) iterate_kernel(Prob<T> P, State<T
         DualStepHalpern<T> ds{S.y[cur], S.y[nxt], S.yt, S.ax[nxt], P.rl, P.ru, S.yr, S.axr, sigma, w};
         run_phase<1, 3>(P.A.ptr, P.A.idx, P.A.val, P.pa, Gather1<T>{S.x[nxt]}, ds, acc, stream);
       }
+      SIH26_MARK(2);
       if (!grid_barrier(S.bar)) goto device_error;
+      SIH26_MARK(3);
       if (threadIdx.x == 0) {
         halpern_control(c);
         c.time_up = *((volatile int*)S.bar.time_up);
       }
       __syncthreads();
+      SIH26_MARK(4);
       if (c.state != kRunning) break;
       continue;
     }
@@ -999,6 +1004,17 @@ __global__ void __launch_bounds__(kThreads, 2) init_ax_kernel(Prob<T> P, State<T
   const int cur = S.ctrl->cur;
   run_phase<1, 1>(P.A.ptr, P.A.idx, P.A.val, P.pa, Gather1<T>{S.x[cur]},
                   StoreRow<1>{S.ax[cur], -1}, dummy, stream);
+}
+
+// out = M v over one partition with nothing fused: the autotuner times candidate schedules
+// with it.
+template <class T>
+__global__ void __launch_bounds__(kThreads, 2) probe_kernel(const int* ptr, const int* idx,
+                                                            const T* val, Part part, const T* v,
+                                                            double* out) {
+  double* stream = warp_stream();
+  double dummy[1] = {0.0};
+  run_phase<1, 1>(ptr, idx, val, part, Gather1<T>{v}, StoreRow<1>{out, -1}, dummy, stream);
 }
 
 // The FP32 level's anchor terms from (xr, yr), FP64 values: axr = A xr, cg = c + A'yr, the

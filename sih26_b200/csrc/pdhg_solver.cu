@@ -237,7 +237,8 @@ static int blocks_per_sm() {
                       reinterpret_cast<const void*>(init_ax_kernel<T>),
                       reinterpret_cast<const void*>(anchor_kernel<T>),
                       reinterpret_cast<const void*>(report_kernel<T>),
-                      reinterpret_cast<const void*>(power_kernel<T>)};
+                      reinterpret_cast<const void*>(power_kernel<T>),
+                      reinterpret_cast<const void*>(probe_kernel<T>)};
   int best = 1 << 20;
   for (const void* f : k1) {
     SIH26_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -409,6 +410,63 @@ static int G_max_coresident(const cudaDeviceProp& props, int bpsm) {
   return props.multiProcessorCount * bpsm;
 }
 
+// Mean microseconds of one probe SpMV over `part` (after one warm-up launch).
+template <class T>
+static double time_probe(const int* ptr, const int* idx, const T* val, const Part& part,
+                         const T* v, double* out, int G, cudaStream_t stream, cudaEvent_t e0,
+                         cudaEvent_t e1) {
+  constexpr int kReps = 5;
+  probe_kernel<T><<<G, kThreads, stream_smem_bytes(), stream>>>(ptr, idx, val, part, v, out);
+  SIH26_CUDA(cudaEventRecord(e0, stream), SANKHYA_GPU_INIT_FAILED);
+  for (int r = 0; r < kReps; ++r)
+    probe_kernel<T><<<G, kThreads, stream_smem_bytes(), stream>>>(ptr, idx, val, part, v, out);
+  SIH26_CUDA(cudaEventRecord(e1, stream), SANKHYA_GPU_INIT_FAILED);
+  SIH26_CUDA(cudaGetLastError(), SANKHYA_GPU_KERNEL_LAUNCH_FAILED);
+  g_launches += kReps + 1;
+  SIH26_CUDA(cudaEventSynchronize(e1), SANKHYA_GPU_SYNC_FAILED);
+  float ms = 0.f;
+  SIH26_CUDA(cudaEventElapsedTime(&ms, e0, e1), SANKHYA_GPU_SYNC_FAILED);
+  return ms * 1e3 / kReps;
+}
+
+// The autotuner: for each orientation, the schedule (stream-row limit, nonzeros per lane)
+// whose plain SpMV over this LP's matrix is fastest among a few candidates, at the level the
+// iteration runs in. Results are keyed on row-length statistics and cached on disk, so LPs of
+// the same shape family are tuned once.
+template <class T>
+static int autotune_schedules(Arena& a, const PermutedLp& q, const Level<T>& L, int G, int sms,
+                              cudaStream_t stream, Schedule* sa, Schedule* sat) {
+  const std::string key = autotune_key(q, G, sms, static_cast<int>(sizeof(T)));
+  const std::string path = autotune_cache_path();
+  if (autotune_lookup(path, key, sa, sat)) return 2;
+  static const Schedule kCandidates[] = {{32, 16}, {16, 16}, {32, 8}, {32, 32}, {8, 16}, {16, 8}};
+  double* out = a.zeros<double>(static_cast<size_t>(std::max(q.m, q.n)));
+  cudaEvent_t e0, e1;
+  SIH26_CUDA(cudaEventCreate(&e0), SANKHYA_GPU_INIT_FAILED);
+  SIH26_CUDA(cudaEventCreate(&e1), SANKHYA_GPU_INIT_FAILED);
+  struct EvFree {
+    cudaEvent_t a, b;
+    ~EvFree() { cudaEventDestroy(a); cudaEventDestroy(b); }
+  } ef{e0, e1};
+  double best_a = INFINITY, best_at = INFINITY;
+  for (const Schedule& c : kCandidates) {
+    const Part pa = upload_part(a, partition(q.a_ptr, G, kWarps, 0, c));
+    const double ta = time_probe<T>(L.P.A.ptr, L.P.A.idx, L.P.A.val, pa, L.S.xt, out, G, stream, e0, e1);
+    if (ta < best_a) {
+      best_a = ta;
+      *sa = c;
+    }
+    const Part pat = upload_part(a, partition(q.at_ptr, G, kWarps, 0, c));
+    const double tat = time_probe<T>(L.P.AT.ptr, L.P.AT.idx, L.P.AT.val, pat, L.S.yt, out, G, stream, e0, e1);
+    if (tat < best_at) {
+      best_at = tat;
+      *sat = c;
+    }
+  }
+  autotune_store(path, key, *sa, *sat, best_a, best_at);
+  return 1;
+}
+
 static void fill_message(sankhya_pdhg_result* r, const char* text) {
   std::snprintf(r->message, sizeof r->message, "%s", text);
 }
@@ -531,6 +589,20 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
   Level<float> L32{};
   const bool mixed = prm.precision == SANKHYA_PDHG_MIXED;
   if (mixed) L32 = make_level<float>(a, cm, q, sc, x0);
+
+  // SpMV schedules: the fixed rule, or the autotuner's pick at the level the loop starts in
+  Schedule sched_a, sched_at;
+  int autotuned = 0;
+  if (prm.autotune && prm.group_size_rows <= 0 && prm.group_size_cols <= 0 && q.nnz > 0) {
+    autotuned = mixed ? autotune_schedules(a, q, L32, G, props.multiProcessorCount, stream,
+                                           &sched_a, &sched_at)
+                      : autotune_schedules(a, q, L64, G, props.multiProcessorCount, stream,
+                                           &sched_a, &sched_at);
+    cm.pa = upload_part(a, partition(q.a_ptr, G, kWarps, 0, sched_a));
+    cm.pat = upload_part(a, partition(q.at_ptr, G, kWarps, 0, sched_at));
+    L64.P.pa = L32.P.pa = cm.pa;
+    L64.P.pat = L32.P.pat = cm.pat;
+  }
 
   // ||A||_2 by power iteration (scaling.cpp:161-194), seed random_seed + 1
   double spectral_norm = 1.0;
@@ -792,6 +864,11 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
   res->iterate_kernel_seconds = timer.seconds;
   res->iterate_launches = timer.launches;
   res->kernel_launches = g_launches;
+  res->autotuned = autotuned;
+  res->schedule[0] = sched_a.stream_row_max;
+  res->schedule[1] = sched_a.nnz_per_lane;
+  res->schedule[2] = sched_at.stream_row_max;
+  res->schedule[3] = sched_at.nnz_per_lane;
   res->solve_seconds = ms * 1e-3;
   res->total_seconds = seconds_since(t_start);
   return SANKHYA_GPU_SUCCESS;

@@ -71,7 +71,7 @@ class _Params(C.Structure):
                 ("mixed_switch_tolerance", C.c_double), ("group_size_rows", C.c_int32),
                 ("group_size_cols", C.c_int32), ("grid_blocks", C.c_int32),
                 ("profile_kernels", C.c_int32), ("mixed_stall_checks", C.c_int32),
-                ("algorithm", C.c_int32), ("reserved", C.c_int32 * 4)]
+                ("algorithm", C.c_int32), ("autotune", C.c_int32), ("reserved", C.c_int32 * 3)]
 
 
 class _Residuals(C.Structure):
@@ -92,7 +92,8 @@ class _Result(C.Structure):
                 ("total_seconds", C.c_double), ("h2d_bytes", C.c_int64),
                 ("d2h_bytes", C.c_int64), ("iterate_kernel_seconds", C.c_double),
                 ("iterate_launches", C.c_int64), ("kernel_launches", C.c_int64),
-                ("residuals", _Residuals),
+                ("residuals", _Residuals), ("autotuned", C.c_int32),
+                ("schedule", C.c_int32 * 4),
                 ("message", C.c_char * 512)]
 
 
@@ -155,6 +156,7 @@ class Options:
         "pdhg_profile_kernels": (bool, False),
         "pdhg_mixed_stall_checks": (int, 0),
         "pdhg_algorithm": (str, "reference"),
+        "pdhg_autotune": (bool, False),
     }
 
     def __init__(self, **values):
@@ -218,6 +220,8 @@ class Solution:
     iterate_kernel_seconds: float = 0.0
     iterate_launches: int = 0
     kernel_launches: int = 0
+    autotuned: int = 0
+    schedule: tuple = ()
 
     def has_primal_values(self) -> bool:
         return self.status in ("optimal", "feasible")
@@ -287,7 +291,8 @@ def solve_pdhg(model: LP, options: Optional[Options] = None) -> Solution:
         setup_seconds=res.setup_seconds, device_seconds=res.solve_seconds,
         h2d_bytes=res.h2d_bytes, d2h_bytes=res.d2h_bytes,
         iterate_kernel_seconds=res.iterate_kernel_seconds, iterate_launches=res.iterate_launches,
-        kernel_launches=res.kernel_launches)
+        kernel_launches=res.kernel_launches, autotuned=res.autotuned,
+        schedule=tuple(res.schedule))
     if status not in ("model_error", "infeasible", "unbounded"):
         sol.primal_infeasibility = _primal_infeasibility(model, x)
     return sol
@@ -339,6 +344,7 @@ def _params(opt: Options, lib) -> _Params:
     prm.profile_kernels = int(opt.get("pdhg_profile_kernels"))
     prm.mixed_stall_checks = opt.get("pdhg_mixed_stall_checks")
     prm.algorithm = ALGORITHMS[opt.get("pdhg_algorithm")]
+    prm.autotune = int(opt.get("pdhg_autotune"))
     return prm
 
 

@@ -211,3 +211,26 @@ def test_mixed_reaches_a_tolerance_below_plain_fp32():
     r = oracle.oracle_evaluate(lp, s.col_value, _y_pdhg_sign(lp, s))
     assert max(r["primal"], r["dual"], r["gap"]) <= tol
     print("fp32 iterations", s.fp32_iterations, "of", s.iterations)
+
+
+@pytest.mark.slow
+def test_block_angular_full_size_mixed_to_1e6():
+    """The blending-style block-angular LP at full size (64 blocks of 4,000 x 10,000 plus 2,000
+    linking rows touching 2 % of all columns: 258,000 x 640,000, ~30.7M nonzeros, 30 % '<='
+    rows), FP32-mixed with the FP64 polish when needed, to relative KKT 1e-6. The oracle is too
+    slow at this size, so the checks are the size-independent ones: the residuals recomputed
+    by the oracle's evaluate from the returned point meet the request, and the objective
+    matches the planted optimum to the accuracy such a point carries."""
+    lp = lpgen.block_angular_planted(seed=2)
+    assert lp.num_rows == 258_000 and lp.num_cols == 640_000
+    for algorithm in ("halpern", "reference"):
+        s = P.solve_pdhg(lp, _opts(pdhg_tolerance=1e-6, pdhg_stop_rule="relative_kkt",
+                                   pdhg_precision="mixed", pdhg_algorithm=algorithm,
+                                   iteration_limit=400000))
+        assert s.status in ("optimal", "feasible"), (algorithm, s.message)
+        r = oracle.oracle_evaluate(lp, s.col_value, _y_pdhg_sign(lp, s))
+        assert max(r["primal"], r["dual"], r["gap"]) <= 1e-6, (algorithm, r)
+        scale = max(1.0, abs(lp.optimal_objective))
+        assert abs(s.objective - lp.optimal_objective) <= 1e-5 * scale, algorithm
+        print(f"{algorithm}: {s.iterations} iterations ({s.fp32_iterations} FP32), "
+              f"{s.device_seconds:.2f} s on the device")
