@@ -519,7 +519,8 @@ def run_ours(args):
                          "us_per_attempt": kern / attempts * 1e6 if attempts else None},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": last.h2d_bytes,
-                    "d2h_bytes_per_step": last.d2h_bytes},
+                    "d2h_bytes_per_step": last.d2h_bytes,
+                    "setup_s": statistics.mean(s.setup_seconds for s in sols)},
             "gpu_launches": launches,
             "clocks": clocks.summary(),
             "batched": batched,
