@@ -147,7 +147,9 @@ typedef struct sankhya_pdhg_params {
                                row-length statistics and cached on disk
                                (SANKHYA_PDHG_AUTOTUNE_CACHE, else ~/.cache/sih26_b200/
                                autotune.tsv); 0 (default): the fixed rule */
-  int32_t reserved[3];
+  int32_t host_prep;        /* 1: scale and permute the LP on the host (build_scaling, permute);
+                               0 (default): on the device. Both give identical bits. */
+  int32_t reserved[2];
 } sankhya_pdhg_params;
 
 /* Unscaled residual block of the reported point (src/pdhg/pdhg.cpp:81-110). */

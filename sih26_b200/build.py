@@ -16,7 +16,8 @@ LIBNAME = "libsankhya_pdhg_gpu.so"
 LIBPATH = os.path.join(LIBDIR, LIBNAME)
 
 SOURCES = ["pdhg_solver.cu", "pdhg_host.cpp", "residuals_noalloc.cu", "batch_server.cu"]
-HEADERS = ["device_common.cuh", "pdhg_kernels.cuh", "pdhg_host.cuh", "batch_kernels.cuh"]
+HEADERS = ["device_common.cuh", "pdhg_kernels.cuh", "pdhg_host.cuh", "batch_kernels.cuh",
+           "prep_kernels.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

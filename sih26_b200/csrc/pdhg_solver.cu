@@ -15,8 +15,12 @@
 #include <string>
 #include <vector>
 
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+
 #include "pdhg_host.cuh"
 #include "pdhg_kernels.cuh"
+#include "prep_kernels.cuh"
 #include "sankhya_pdhg_gpu.h"
 
 namespace sih26 {
@@ -150,7 +154,7 @@ struct Common {
 };
 
 template <class T>
-static Level<T> make_level(Arena& a, const Common& cm, const PermutedLp& q, const Scaling& s,
+static Level<T> make_level(Arena& a, const Common& cm, const PermutedLp& q,
                            const std::vector<double>& x0) {
   Level<T> L{};
   const int m = q.m, n = q.n;
@@ -167,8 +171,16 @@ static Level<T> make_level(Arena& a, const Common& cm, const PermutedLp& q, cons
     P.A.val = cm.a_val64;
     P.AT.val = cm.at_val64;
   } else {
-    P.A.val = a.upload<T>(q.a_val);
-    P.AT.val = a.upload<T>(q.at_val);
+    // FP32 copies of the scaled values, rounded on the device
+    T* av = a.alloc<T>(q.nnz);
+    T* atv = a.alloc<T>(q.nnz);
+    const dim3 grid(static_cast<unsigned>(std::max<long long>(1, std::min<long long>((q.nnz + 255) / 256, 148 * 16))));
+    prep::to_float<<<grid, 256>>>(cm.a_val64, q.nnz, av);
+    prep::to_float<<<grid, 256>>>(cm.at_val64, q.nnz, atv);
+    SIH26_CUDA(cudaGetLastError(), SANKHYA_GPU_KERNEL_LAUNCH_FAILED);
+    SIH26_CUDA(cudaDeviceSynchronize(), SANKHYA_GPU_SYNC_FAILED);
+    P.A.val = av;
+    P.AT.val = atv;
   }
   P.pa = cm.pa;
   P.pat = cm.pat;
@@ -410,6 +422,206 @@ static int G_max_coresident(const cudaDeviceProp& props, int bpsm) {
   return props.multiProcessorCount * bpsm;
 }
 
+// ---- preparation on the device (prep_kernels.cuh) --------------------------------------
+
+static int bits_for(long long count) {  // bits that hold 0 .. count-1
+  int b = 1;
+  while ((1ll << b) < count) ++b;
+  return b;
+}
+
+static dim3 prep_grid(long long work) {
+  return dim3(static_cast<unsigned>(std::max<long long>(1, std::min<long long>((work + 255) / 256, 148 * 16))));
+}
+
+template <class K, class V>
+static void radix_sort_pairs(Arena& a, const K* kin, K* kout, const V* vin, V* vout, long long count,
+                             int end_bit, cudaStream_t stream) {
+  size_t bytes = 0;
+  SIH26_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, kin, kout, vin, vout, count, 0, end_bit,
+                                             stream), SANKHYA_GPU_KERNEL_LAUNCH_FAILED);
+  void* tmp = a.alloc<unsigned char>(bytes);
+  SIH26_CUDA(cub::DeviceRadixSort::SortPairs(tmp, bytes, kin, kout, vin, vout, count, 0, end_bit,
+                                             stream), SANKHYA_GPU_KERNEL_LAUNCH_FAILED);
+  g_launches += 1;
+}
+
+// ptr[0] = 0, ptr[i+1] = ptr[i] + len[i]
+static void lengths_to_ptr(Arena& a, const int* len, int count, int* ptr, cudaStream_t stream) {
+  SIH26_CUDA(cudaMemsetAsync(ptr, 0, sizeof(int), stream), SANKHYA_GPU_COPY_FAILED);
+  if (count == 0) return;
+  size_t bytes = 0;
+  SIH26_CUDA(cub::DeviceScan::InclusiveSum(nullptr, bytes, len, ptr + 1, count, stream),
+             SANKHYA_GPU_KERNEL_LAUNCH_FAILED);
+  void* tmp = a.alloc<unsigned char>(bytes);
+  SIH26_CUDA(cub::DeviceScan::InclusiveSum(tmp, bytes, len, ptr + 1, count, stream),
+             SANKHYA_GPU_KERNEL_LAUNCH_FAILED);
+  g_launches += 1;
+}
+
+// build_scaling + permute on the device: fills the device arrays of `cm` (matrix, scaling and
+// vectors, permuted) and, on the host, q's sizes, permutations and row pointers (the work
+// partition and the output un-permutation are built from them) and the starting point x0.
+static void prepare_on_device(Arena& a, const sankhya_pdhg_problem& prob,
+                              const std::vector<double>& cmin, int ruiz_rounds,
+                              cudaStream_t stream, Common& cm, PermutedLp& q,
+                              std::vector<double>& x0) {
+  using namespace prep;
+  const int m = prob.num_rows, n = prob.num_cols;
+  const long long nnz = prob.num_nonzeros;
+  q.m = m;
+  q.n = n;
+  q.nnz = nnz;
+  const auto put_i = [&](const int* h, size_t count) {
+    int* d = a.alloc<int>(count);
+    a.put(d, h, count * sizeof(int), stream);
+    return d;
+  };
+  const auto put_d = [&](const double* h, size_t count) {
+    double* d = a.alloc<double>(count);
+    a.put(d, h, count * sizeof(double), stream);
+    return d;
+  };
+  const dim3 B(256);
+  // the problem as given (CSC) and the entries' columns
+  int* cs = put_i(prob.col_starts, n + 1);
+  int* ri = put_i(prob.row_indices, nnz);
+  double* v = put_d(prob.values, nnz);
+  double* cmin_d = put_d(cmin.data(), n);
+  double* cl = put_d(prob.col_lower, n);
+  double* cu = put_d(prob.col_upper, n);
+  double* rl = put_d(prob.row_lower, m);
+  double* ru = put_d(prob.row_upper, m);
+  int* col = a.alloc<int>(nnz);
+  column_of_entry<<<prep_grid(n), B, 0, stream>>>(cs, n, col);
+  // row-major copy: a stable sort of the entries by row keeps each row in column order
+  int* rcount = a.zeros<int>(m);
+  count_by<<<prep_grid(nnz), B, 0, stream>>>(ri, nnz, rcount);
+  int* rptr = a.alloc<int>(m + 1);
+  lengths_to_ptr(a, rcount, m, rptr, stream);
+  int* entry = a.alloc<int>(nnz);
+  int* entry_rm = a.alloc<int>(nnz);
+  unsigned* rkey_in = a.alloc<unsigned>(nnz);
+  unsigned* rkey_out = a.alloc<unsigned>(nnz);
+  SIH26_CUDA(cudaMemcpyAsync(rkey_in, ri, nnz * sizeof(int), cudaMemcpyDeviceToDevice, stream),
+             SANKHYA_GPU_COPY_FAILED);
+  identity<<<prep_grid(nnz), B, 0, stream>>>(entry, nnz);
+  radix_sort_pairs(a, rkey_in, rkey_out, entry, entry_rm, nnz, bits_for(m), stream);
+  double* vr = a.alloc<double>(nnz);
+  int* cr = a.alloc<int>(nnz);
+  int* rr = a.alloc<int>(nnz);
+  gather<double><<<prep_grid(nnz), B, 0, stream>>>(entry_rm, v, nnz, vr);
+  gather<int><<<prep_grid(nnz), B, 0, stream>>>(entry_rm, col, nnz, cr);
+  row_of_entry<<<prep_grid(m), B, 0, stream>>>(rptr, m, rr);
+  // scaling rounds: 10 Ruiz (max) and one Pock-Chambolle (sum), scaling.cpp:44-100
+  double* ra = a.alloc<double>(m);
+  double* ca = a.alloc<double>(n);
+  double* rp = a.alloc<double>(m);
+  double* cp = a.alloc<double>(n);
+  double* dr = a.alloc<double>(m);
+  double* dc = a.alloc<double>(n);
+  fill<<<prep_grid(m), B, 0, stream>>>(dr, m, 1.0);
+  fill<<<prep_grid(n), B, 0, stream>>>(dc, n, 1.0);
+  for (int round = 0; round <= ruiz_rounds; ++round) {
+    const int sum = round == ruiz_rounds ? 1 : 0;
+    segment_norms<<<prep_grid(n), B, 0, stream>>>(cs, v, n, sum, ca);
+    segment_norms<<<prep_grid(m), B, 0, stream>>>(rptr, vr, m, sum, ra);
+    pass_factors<<<prep_grid(m), B, 0, stream>>>(ra, m, rp, dr);
+    pass_factors<<<prep_grid(n), B, 0, stream>>>(ca, n, cp, dc);
+    apply_pass<<<prep_grid(nnz), B, 0, stream>>>(ri, col, rp, cp, nnz, v);
+    apply_pass<<<prep_grid(nnz), B, 0, stream>>>(rr, cr, rp, cp, nnz, vr);
+    g_launches += 6;
+  }
+  // scaled vectors, original order
+  double* c_s = a.alloc<double>(n);
+  double* cl_s = a.alloc<double>(n);
+  double* cu_s = a.alloc<double>(n);
+  double* rl_s = a.alloc<double>(m);
+  double* ru_s = a.alloc<double>(m);
+  scaled_columns<<<prep_grid(n), B, 0, stream>>>(cmin_d, cl, cu, dc, n, c_s, cl_s, cu_s);
+  scaled_rows<<<prep_grid(m), B, 0, stream>>>(rl, ru, dr, m, rl_s, ru_s);
+  // permutations: longest first, ties by index
+  int* row_perm = a.alloc<int>(m);
+  int* col_perm = a.alloc<int>(n);
+  {
+    unsigned* k_in = a.alloc<unsigned>(std::max(m, n));
+    unsigned* k_out = a.alloc<unsigned>(std::max(m, n));
+    int* idx = a.alloc<int>(std::max(m, n));
+    count_keys<<<prep_grid(m), B, 0, stream>>>(rptr, m, k_in, idx);
+    radix_sort_pairs(a, k_in, k_out, idx, row_perm, m, 32, stream);
+    count_keys<<<prep_grid(n), B, 0, stream>>>(cs, n, k_in, idx);
+    radix_sort_pairs(a, k_in, k_out, idx, col_perm, n, 32, stream);
+  }
+  int* row_pos = a.alloc<int>(m);
+  int* col_pos = a.alloc<int>(n);
+  positions<<<prep_grid(m), B, 0, stream>>>(row_perm, m, row_pos);
+  positions<<<prep_grid(n), B, 0, stream>>>(col_perm, n, col_pos);
+  // A in permuted row order, each row's entries in permuted column order; A' likewise
+  int* a_ptr = a.alloc<int>(m + 1);
+  int* at_ptr = a.alloc<int>(n + 1);
+  int* lens = a.alloc<int>(std::max(m, n));
+  permuted_lengths<<<prep_grid(m), B, 0, stream>>>(rptr, row_perm, m, lens);
+  lengths_to_ptr(a, lens, m, a_ptr, stream);
+  permuted_lengths<<<prep_grid(n), B, 0, stream>>>(cs, col_perm, n, lens);
+  lengths_to_ptr(a, lens, n, at_ptr, stream);
+  unsigned long long* key_in = a.alloc<unsigned long long>(nnz);
+  unsigned long long* key_out = a.alloc<unsigned long long>(nnz);
+  int* a_idx = a.alloc<int>(nnz);
+  int* at_idx = a.alloc<int>(nnz);
+  double* a_val = a.alloc<double>(nnz);
+  double* at_val = a.alloc<double>(nnz);
+  {
+    const int shift = bits_for(n), end = shift + bits_for(m);
+    pair_keys<<<prep_grid(nnz), B, 0, stream>>>(ri, col, row_pos, col_pos, nnz, shift, key_in);
+    radix_sort_pairs(a, key_in, key_out, v, a_val, nnz, end, stream);
+    low_bits<<<prep_grid(nnz), B, 0, stream>>>(key_out, nnz, shift, a_idx);
+  }
+  {
+    const int shift = bits_for(m), end = shift + bits_for(n);
+    pair_keys<<<prep_grid(nnz), B, 0, stream>>>(col, ri, col_pos, row_pos, nnz, shift, key_in);
+    radix_sort_pairs(a, key_in, key_out, v, at_val, nnz, end, stream);
+    low_bits<<<prep_grid(nnz), B, 0, stream>>>(key_out, nnz, shift, at_idx);
+  }
+  cm.a_ptr = a_ptr;
+  cm.a_idx = a_idx;
+  cm.at_ptr = at_ptr;
+  cm.at_idx = at_idx;
+  cm.a_val64 = a_val;
+  cm.at_val64 = at_val;
+  const auto perm_vec = [&](const int* perm, const double* src, int len) {
+    double* d = a.alloc<double>(len);
+    gather<double><<<prep_grid(len), B, 0, stream>>>(perm, src, len, d);
+    return d;
+  };
+  cm.dr = perm_vec(row_perm, dr, m);
+  cm.dc = perm_vec(col_perm, dc, n);
+  cm.c0 = perm_vec(col_perm, cmin_d, n);
+  cm.cl0 = perm_vec(col_perm, cl, n);
+  cm.cu0 = perm_vec(col_perm, cu, n);
+  cm.rl0 = perm_vec(row_perm, rl, m);
+  cm.ru0 = perm_vec(row_perm, ru, m);
+  cm.c64 = perm_vec(col_perm, c_s, n);
+  cm.cl64 = perm_vec(col_perm, cl_s, n);
+  cm.cu64 = perm_vec(col_perm, cu_s, n);
+  cm.rl64 = perm_vec(row_perm, rl_s, m);
+  cm.ru64 = perm_vec(row_perm, ru_s, m);
+  double* x0_d = a.alloc<double>(n);
+  start_point<<<prep_grid(n), B, 0, stream>>>(cm.cl64, cm.cu64, n, x0_d);
+  SIH26_CUDA(cudaGetLastError(), SANKHYA_GPU_KERNEL_LAUNCH_FAILED);
+  // host copies the partition and the output un-permutation need
+  q.row_perm.resize(m);
+  q.col_perm.resize(n);
+  q.a_ptr.resize(m + 1);
+  q.at_ptr.resize(n + 1);
+  x0.resize(n);
+  a.get(q.row_perm.data(), row_perm, m * sizeof(int), stream);
+  a.get(q.col_perm.data(), col_perm, n * sizeof(int), stream);
+  a.get(q.a_ptr.data(), a_ptr, (m + 1) * sizeof(int), stream);
+  a.get(q.at_ptr.data(), at_ptr, (n + 1) * sizeof(int), stream);
+  a.get(x0.data(), x0_d, n * sizeof(double), stream);
+  SIH26_CUDA(cudaStreamSynchronize(stream), SANKHYA_GPU_SYNC_FAILED);
+}
+
 // Mean microseconds of one probe SpMV over `part` (after one warm-up launch).
 template <class T>
 static double time_probe(const int* ptr, const int* idx, const T* val, const Part& part,
@@ -524,13 +736,10 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
   const double bound_norm = std::sqrt(bs2);
 
   // ---- preconditioning and layout ----
-  const Scaling sc = build_scaling(prob, cmin, 10);
-  const PermutedLp q = permute(prob, sc.values);
-
   int bpsm = std::min(blocks_per_sm<double>(), prm.precision == SANKHYA_PDHG_MIXED ? blocks_per_sm<float>() : 1 << 20);
   if (bpsm < 1) throw Failure{SANKHYA_GPU_INIT_FAILED, "kernel does not fit on an SM"};
   int G = props.multiProcessorCount * std::min(bpsm, 2);
-  const long long work = q.nnz + m + n;
+  const long long work = static_cast<long long>(prob.num_nonzeros) + m + n;
   G = static_cast<int>(std::max<long long>(1, std::min<long long>(G, (work + 4095) / 4096)));
   if (prm.grid_blocks > 0) G = std::min(G_max_coresident(props, bpsm), prm.grid_blocks);
 
@@ -543,24 +752,42 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
   } guard{stream};
 
   Common cm{};
-  cm.a_ptr = a.upload_same(q.a_ptr);
-  cm.a_idx = a.upload_same(q.a_idx);
-  cm.at_ptr = a.upload_same(q.at_ptr);
-  cm.at_idx = a.upload_same(q.at_idx);
-  cm.a_val64 = a.upload_same(q.a_val);
-  cm.at_val64 = a.upload_same(q.at_val);
-  cm.dr = a.upload_same(gather(sc.dr, q.row_perm));
-  cm.dc = a.upload_same(gather(sc.dc, q.col_perm));
-  cm.c0 = a.upload_same(gather(cmin, q.col_perm));
-  cm.cl0 = a.upload_same(gather_ptr(prob.col_lower, q.col_perm));
-  cm.cu0 = a.upload_same(gather_ptr(prob.col_upper, q.col_perm));
-  cm.rl0 = a.upload_same(gather_ptr(prob.row_lower, q.row_perm));
-  cm.ru0 = a.upload_same(gather_ptr(prob.row_upper, q.row_perm));
-  cm.c64 = a.upload_same(gather(sc.cost, q.col_perm));
-  cm.cl64 = a.upload_same(gather(sc.cl, q.col_perm));
-  cm.cu64 = a.upload_same(gather(sc.cu, q.col_perm));
-  cm.rl64 = a.upload_same(gather(sc.rl, q.row_perm));
-  cm.ru64 = a.upload_same(gather(sc.ru, q.row_perm));
+  PermutedLp q;           // host: sizes, permutations, row pointers of A and A'
+  std::vector<double> x0;  // the starting point, permuted
+  if (prm.host_prep) {
+    // build_scaling and permute on the host (pdhg_host.cpp), uploaded
+    const Scaling sc = build_scaling(prob, cmin, 10);
+    q = permute(prob, sc.values);
+    cm.a_ptr = a.upload_same(q.a_ptr);
+    cm.a_idx = a.upload_same(q.a_idx);
+    cm.at_ptr = a.upload_same(q.at_ptr);
+    cm.at_idx = a.upload_same(q.at_idx);
+    cm.a_val64 = a.upload_same(q.a_val);
+    cm.at_val64 = a.upload_same(q.at_val);
+    cm.dr = a.upload_same(gather(sc.dr, q.row_perm));
+    cm.dc = a.upload_same(gather(sc.dc, q.col_perm));
+    cm.c0 = a.upload_same(gather(cmin, q.col_perm));
+    cm.cl0 = a.upload_same(gather_ptr(prob.col_lower, q.col_perm));
+    cm.cu0 = a.upload_same(gather_ptr(prob.col_upper, q.col_perm));
+    cm.rl0 = a.upload_same(gather_ptr(prob.row_lower, q.row_perm));
+    cm.ru0 = a.upload_same(gather_ptr(prob.row_upper, q.row_perm));
+    cm.c64 = a.upload_same(gather(sc.cost, q.col_perm));
+    cm.cl64 = a.upload_same(gather(sc.cl, q.col_perm));
+    cm.cu64 = a.upload_same(gather(sc.cu, q.col_perm));
+    cm.rl64 = a.upload_same(gather(sc.rl, q.row_perm));
+    cm.ru64 = a.upload_same(gather(sc.ru, q.row_perm));
+    // starting point: the projection of zero (pdhg.cpp:329-334), in permuted order
+    x0.resize(n);
+    for (int t = 0; t < n; ++t) {
+      const int j = q.col_perm[t];
+      double v = 0.0;
+      if (host_finite_bound(sc.cl[j]) && v < sc.cl[j]) v = sc.cl[j];
+      else if (host_finite_bound(sc.cu[j]) && v > sc.cu[j]) v = sc.cu[j];
+      x0[t] = v;
+    }
+  } else {
+    prepare_on_device(a, prob, cmin, 10, stream, cm, q, x0);
+  }
   cm.pa = upload_part(a, partition(q.a_ptr, G, kWarps, prm.group_size_rows));
   cm.pat = upload_part(a, partition(q.at_ptr, G, kWarps, prm.group_size_cols));
   cm.best_x = a.zeros<double>(n);
@@ -572,23 +799,13 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
   unsigned* bar_words = a.zeros<unsigned>(2);
   int* flags = a.zeros<int>(2);
   cm.bar = GridBarrier{bar_words, bar_words + 1, flags, 4000000000ull, flags + 1, 0ull};
-
-  // starting point: the projection of zero (pdhg.cpp:329-334), in permuted order
-  std::vector<double> x0(n);
-  for (int t = 0; t < n; ++t) {
-    const int j = q.col_perm[t];
-    double v = 0.0;
-    if (host_finite_bound(sc.cl[j]) && v < sc.cl[j]) v = sc.cl[j];
-    else if (host_finite_bound(sc.cu[j]) && v > sc.cu[j]) v = sc.cu[j];
-    x0[t] = v;
-  }
   a.put(cm.best_x, x0.data(), n * sizeof(double), 0);
   SIH26_CUDA(cudaDeviceSynchronize(), SANKHYA_GPU_SYNC_FAILED);
 
-  Level<double> L64 = make_level<double>(a, cm, q, sc, prm.precision == SANKHYA_PDHG_FP64 ? x0 : std::vector<double>());
+  Level<double> L64 = make_level<double>(a, cm, q, prm.precision == SANKHYA_PDHG_FP64 ? x0 : std::vector<double>());
   Level<float> L32{};
   const bool mixed = prm.precision == SANKHYA_PDHG_MIXED;
-  if (mixed) L32 = make_level<float>(a, cm, q, sc, x0);
+  if (mixed) L32 = make_level<float>(a, cm, q, x0);
 
   // SpMV schedules: the fixed rule, or the autotuner's pick at the level the loop starts in
   Schedule sched_a, sched_at;

@@ -71,7 +71,8 @@ class _Params(C.Structure):
                 ("mixed_switch_tolerance", C.c_double), ("group_size_rows", C.c_int32),
                 ("group_size_cols", C.c_int32), ("grid_blocks", C.c_int32),
                 ("profile_kernels", C.c_int32), ("mixed_stall_checks", C.c_int32),
-                ("algorithm", C.c_int32), ("autotune", C.c_int32), ("reserved", C.c_int32 * 3)]
+                ("algorithm", C.c_int32), ("autotune", C.c_int32), ("host_prep", C.c_int32),
+                ("reserved", C.c_int32 * 2)]
 
 
 class _Residuals(C.Structure):
@@ -157,6 +158,7 @@ class Options:
         "pdhg_mixed_stall_checks": (int, 0),
         "pdhg_algorithm": (str, "reference"),
         "pdhg_autotune": (bool, False),
+        "pdhg_host_prep": (bool, False),
     }
 
     def __init__(self, **values):
@@ -345,6 +347,7 @@ def _params(opt: Options, lib) -> _Params:
     prm.mixed_stall_checks = opt.get("pdhg_mixed_stall_checks")
     prm.algorithm = ALGORITHMS[opt.get("pdhg_algorithm")]
     prm.autotune = int(opt.get("pdhg_autotune"))
+    prm.host_prep = int(opt.get("pdhg_host_prep"))
     return prm
 
 
