@@ -574,8 +574,9 @@ static std::vector<int> settle(Server& s, const std::vector<int>& list, const Ct
         Ctrl r = c;
         r.state = kRunning;
         r.farkas_cooldown = kCertCooldown;
-        SIH26_SCUDA(cudaMemcpy(s.d_ctrls + slot, &r, sizeof(Ctrl), cudaMemcpyHostToDevice),
-                    SANKHYA_GPU_COPY_FAILED);
+        SIH26_SCUDA(cudaMemcpyAsync(s.d_ctrls + slot, &r, sizeof(Ctrl), cudaMemcpyHostToDevice,
+                                    s.stream), SANKHYA_GPU_COPY_FAILED);
+        SIH26_SCUDA(cudaStreamSynchronize(s.stream), SANKHYA_GPU_SYNC_FAILED);
       }
     }
     if (done) {
@@ -671,7 +672,7 @@ int sankhya_pdhg_server_create(const sankhya_pdhg_server_config* config,
       SIH26_SCUDA(cudaMalloc(&s->d_active[k], cap * sizeof(int)), SANKHYA_GPU_OUT_OF_MEMORY);
       SIH26_SCUDA(cudaMalloc(&s->d_count[k], sizeof(int)), SANKHYA_GPU_OUT_OF_MEMORY);
       SIH26_SCUDA(cudaMalloc(&s->d_head[k], sizeof(int)), SANKHYA_GPU_OUT_OF_MEMORY);
-      SIH26_SCUDA(cudaMemset(s->d_count[k], 0, sizeof(int)), SANKHYA_GPU_INIT_FAILED);
+      SIH26_SCUDA(cudaMemsetAsync(s->d_count[k], 0, sizeof(int), s->stream), SANKHYA_GPU_INIT_FAILED);
     }
     SIH26_SCUDA(cudaMalloc(&s->d_compact2, cap * sizeof(sih26::Ctrl)), SANKHYA_GPU_OUT_OF_MEMORY);
     SIH26_SCUDA(cudaMallocHost(&s->h_compact, cap * sizeof(sih26::Ctrl)), SANKHYA_GPU_OUT_OF_MEMORY);

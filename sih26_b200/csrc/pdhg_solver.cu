@@ -39,7 +39,9 @@ static double seconds_since(Clock::time_point t0) {
   return std::chrono::duration<double>(Clock::now() - t0).count();
 }
 
-// Owns every device allocation of one solve and counts the bytes it copies.
+// Owns every device allocation of one solve and counts the bytes it copies. Buffers are
+// carved, 256-byte aligned, out of a few large cudaMalloc chunks (one call per 64 MiB or per
+// larger buffer), so a solve's ~60 buffers cost a handful of allocations.
 class Arena {
  public:
   long long h2d_bytes = 0;
@@ -50,15 +52,31 @@ class Arena {
   template <class T>
   T* alloc(size_t count) {
     if (count == 0) count = 1;
-    void* p = nullptr;
-    SIH26_CUDA(cudaMalloc(&p, count * sizeof(T)), SANKHYA_GPU_OUT_OF_MEMORY);
-    ptrs_.push_back(p);
+    const size_t bytes = (count * sizeof(T) + 255) & ~size_t(255);
+    if (bytes > left_) {
+      constexpr size_t kChunk = size_t(64) << 20;
+      const size_t size = std::max(bytes, kChunk);
+      void* p = nullptr;
+      SIH26_CUDA(cudaMalloc(&p, size), SANKHYA_GPU_OUT_OF_MEMORY);
+      ptrs_.push_back(p);
+      next_ = static_cast<unsigned char*>(p);
+      left_ = size;
+    }
+    void* p = next_;
+    next_ += bytes;
+    left_ -= bytes;
     return static_cast<T*>(p);
   }
+  // The stream every later use of the arena's buffers is ordered on: zeroing goes there too,
+  // so a kernel on that stream never overtakes the memset of a buffer it reads (a
+  // non-blocking stream does not wait for the legacy default stream).
+  void set_stream(cudaStream_t s) { stream_ = s; }
+  cudaStream_t stream() const { return stream_; }
   template <class T>
   T* zeros(size_t count) {
     T* p = alloc<T>(count);
-    SIH26_CUDA(cudaMemset(p, 0, std::max<size_t>(count, 1) * sizeof(T)), SANKHYA_GPU_COPY_FAILED);
+    SIH26_CUDA(cudaMemsetAsync(p, 0, std::max<size_t>(count, 1) * sizeof(T), stream_),
+               SANKHYA_GPU_COPY_FAILED);
     return p;
   }
   template <class T, class U>
@@ -66,8 +84,8 @@ class Arena {
     T* p = alloc<T>(host.size());
     if (!host.empty()) {
       std::vector<T> conv(host.begin(), host.end());
-      SIH26_CUDA(cudaMemcpy(p, conv.data(), conv.size() * sizeof(T), cudaMemcpyHostToDevice),
-                 SANKHYA_GPU_COPY_FAILED);
+      SIH26_CUDA(cudaMemcpyAsync(p, conv.data(), conv.size() * sizeof(T), cudaMemcpyHostToDevice,
+                                 stream_), SANKHYA_GPU_COPY_FAILED);
       h2d_bytes += conv.size() * sizeof(T);
     }
     return p;
@@ -76,8 +94,8 @@ class Arena {
   T* upload_same(const std::vector<T>& host) {
     T* p = alloc<T>(host.size());
     if (!host.empty()) {
-      SIH26_CUDA(cudaMemcpy(p, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice),
-                 SANKHYA_GPU_COPY_FAILED);
+      SIH26_CUDA(cudaMemcpyAsync(p, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice,
+                                 stream_), SANKHYA_GPU_COPY_FAILED);
       h2d_bytes += host.size() * sizeof(T);
     }
     return p;
@@ -96,6 +114,9 @@ class Arena {
 
  private:
   std::vector<void*> ptrs_;
+  unsigned char* next_ = nullptr;
+  size_t left_ = 0;
+  cudaStream_t stream_ = nullptr;
 };
 
 template <class T>
@@ -175,8 +196,8 @@ static Level<T> make_level(Arena& a, const Common& cm, const PermutedLp& q,
     T* av = a.alloc<T>(q.nnz);
     T* atv = a.alloc<T>(q.nnz);
     const dim3 grid(static_cast<unsigned>(std::max<long long>(1, std::min<long long>((q.nnz + 255) / 256, 148 * 16))));
-    prep::to_float<<<grid, 256>>>(cm.a_val64, q.nnz, av);
-    prep::to_float<<<grid, 256>>>(cm.at_val64, q.nnz, atv);
+    prep::to_float<<<grid, 256, 0, a.stream()>>>(cm.a_val64, q.nnz, av);
+    prep::to_float<<<grid, 256, 0, a.stream()>>>(cm.at_val64, q.nnz, atv);
     SIH26_CUDA(cudaGetLastError(), SANKHYA_GPU_KERNEL_LAUNCH_FAILED);
     SIH26_CUDA(cudaDeviceSynchronize(), SANKHYA_GPU_SYNC_FAILED);
     P.A.val = av;
@@ -234,8 +255,8 @@ static Level<T> make_level(Arena& a, const Common& cm, const PermutedLp& q,
   S.bar = cm.bar;
   if (!x0.empty()) {
     // the FP64 level starts at x0; the FP32 level at the anchor x0 with zero deltas
-    if constexpr (!kDelta<T>) a.put(S.x[0], x0.data(), n * sizeof(double), 0);
-    a.put(S.xr, x0.data(), n * sizeof(double), 0);
+    if constexpr (!kDelta<T>) a.put(S.x[0], x0.data(), n * sizeof(double), a.stream());
+    a.put(S.xr, x0.data(), n * sizeof(double), a.stream());
     SIH26_CUDA(cudaDeviceSynchronize(), SANKHYA_GPU_SYNC_FAILED);
   }
   return L;
@@ -735,6 +756,11 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
   }
   const double bound_norm = std::sqrt(bs2);
 
+  // setup phases, printed with the iteration table (verbose)
+  std::vector<std::pair<const char*, double>> marks;
+  const auto mark = [&](const char* what) { marks.emplace_back(what, seconds_since(t_start)); };
+  mark("validation");
+
   // ---- preconditioning and layout ----
   int bpsm = std::min(blocks_per_sm<double>(), prm.precision == SANKHYA_PDHG_MIXED ? blocks_per_sm<float>() : 1 << 20);
   if (bpsm < 1) throw Failure{SANKHYA_GPU_INIT_FAILED, "kernel does not fit on an SM"};
@@ -743,13 +769,14 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
   G = static_cast<int>(std::max<long long>(1, std::min<long long>(G, (work + 4095) / 4096)));
   if (prm.grid_blocks > 0) G = std::min(G_max_coresident(props, bpsm), prm.grid_blocks);
 
-  Arena a;
   cudaStream_t stream;
   SIH26_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), SANKHYA_GPU_INIT_FAILED);
   struct StreamGuard {
     cudaStream_t s;
     ~StreamGuard() { cudaStreamDestroy(s); }
   } guard{stream};
+  Arena a;  // destroyed before the stream (declared after it)
+  a.set_stream(stream);
 
   Common cm{};
   PermutedLp q;           // host: sizes, permutations, row pointers of A and A'
@@ -788,6 +815,7 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
   } else {
     prepare_on_device(a, prob, cmin, 10, stream, cm, q, x0);
   }
+  mark("scaling and layout");
   cm.pa = upload_part(a, partition(q.a_ptr, G, kWarps, prm.group_size_rows));
   cm.pat = upload_part(a, partition(q.at_ptr, G, kWarps, prm.group_size_cols));
   cm.best_x = a.zeros<double>(n);
@@ -799,9 +827,10 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
   unsigned* bar_words = a.zeros<unsigned>(2);
   int* flags = a.zeros<int>(2);
   cm.bar = GridBarrier{bar_words, bar_words + 1, flags, 4000000000ull, flags + 1, 0ull};
-  a.put(cm.best_x, x0.data(), n * sizeof(double), 0);
+  a.put(cm.best_x, x0.data(), n * sizeof(double), stream);
   SIH26_CUDA(cudaDeviceSynchronize(), SANKHYA_GPU_SYNC_FAILED);
 
+  mark("work partition");
   Level<double> L64 = make_level<double>(a, cm, q, prm.precision == SANKHYA_PDHG_FP64 ? x0 : std::vector<double>());
   Level<float> L32{};
   const bool mixed = prm.precision == SANKHYA_PDHG_MIXED;
@@ -810,6 +839,7 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
   // SpMV schedules: the fixed rule, or the autotuner's pick at the level the loop starts in
   Schedule sched_a, sched_at;
   int autotuned = 0;
+  mark("iterate buffers");
   if (prm.autotune && prm.group_size_rows <= 0 && prm.group_size_cols <= 0 && q.nnz > 0) {
     autotuned = mixed ? autotune_schedules(a, q, L32, G, props.multiProcessorCount, stream,
                                            &sched_a, &sched_at)
@@ -821,6 +851,7 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
     L64.P.pat = L32.P.pat = cm.pat;
   }
 
+  mark("schedules");
   // ||A||_2 by power iteration (scaling.cpp:161-194), seed random_seed + 1
   double spectral_norm = 1.0;
   if (m > 0 && n > 0 && q.nnz > 0) {
@@ -876,13 +907,16 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
   }
 
   // the time limit counts from the start of the call, like the reference's Timer
+  mark("norm estimate and A x0");
   const double setup_seconds = seconds_since(t_start);
   if (std::isfinite(prm.time_limit) && prm.time_limit > 0.0) {
     unsigned long long* d_now = a.zeros<unsigned long long>(1);
     read_clock_kernel<<<1, 1, 0, stream>>>(d_now);
     ++g_launches;
     unsigned long long now = 0;
-    SIH26_CUDA(cudaMemcpy(&now, d_now, sizeof now, cudaMemcpyDeviceToHost), SANKHYA_GPU_COPY_FAILED);
+    SIH26_CUDA(cudaMemcpyAsync(&now, d_now, sizeof now, cudaMemcpyDeviceToHost, stream),
+               SANKHYA_GPU_COPY_FAILED);
+    SIH26_CUDA(cudaStreamSynchronize(stream), SANKHYA_GPU_SYNC_FAILED);
     const double left = prm.time_limit - seconds_since(t_start);
     cm.bar.deadline_ns = now + static_cast<unsigned long long>(std::max(0.0, left) * 1e9);
     L64.S.bar = cm.bar;
@@ -912,6 +946,13 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
   if (prm.verbose) {
     std::printf("GPU PDHG: %d rows, %d columns, %lld nonzeros, %d blocks x %d threads, ||A||_2 ~ %.4e\n",
                 m, n, q.nnz, G, kThreads, spectral_norm);
+    double prev = 0.0;
+    std::printf("setup:");
+    for (const auto& mk : marks) {
+      std::printf(" %s %.1f ms;", mk.first, (mk.second - prev) * 1e3);
+      prev = mk.second;
+    }
+    std::printf("\n");
     std::printf("%10s %12s %10s %10s %10s %9s %9s\n", "iteration", "objective", "primal", "dual",
                 "gap", "eta", "omega");
   }
