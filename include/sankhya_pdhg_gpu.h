@@ -284,6 +284,30 @@ void sankhya_pdhg_server_free(sankhya_pdhg_server* server);
 int sankhya_pdhg_gpu_batch_solve(const sankhya_pdhg_problem* problems, int32_t count,
                                  const sankhya_pdhg_params* params, sankhya_pdhg_result* results);
 
+/* ---- Request wire format -----------------------------------------------------------------
+ *
+ * A binary form of one LP for served mode, where parsing text MPS per request would cost more
+ * than solving (the reference reads MPS/LP text, src/io/mps_reader.cpp; this format has no
+ * counterpart there). Little-endian, every array 8-byte aligned so a received buffer is used
+ * in place:
+ *   0  char[8]  "SKPDHG01"
+ *   8  int32    num_rows, num_cols, num_nonzeros, flags (bit 0: maximize)
+ *   24 double   objective_offset
+ *   32 arrays   col_starts[n+1] int32, row_indices[nnz] int32, values[nnz], cost[n],
+ *               col_lower[n], col_upper[n], row_lower[m], row_upper[m] (doubles), each
+ *               starting on an 8-byte boundary (int32 arrays padded with zeros). */
+#define SANKHYA_PDHG_WIRE_MAGIC "SKPDHG01"
+
+/* Bytes the wire form of `problem` takes. */
+size_t sankhya_pdhg_wire_size(const sankhya_pdhg_problem* problem);
+/* Writes the wire form of `problem` into buffer[0, bytes); INVALID_ARGUMENT if it does not
+ * fit or the problem is malformed. */
+int sankhya_pdhg_wire_write(const sankhya_pdhg_problem* problem, void* buffer, size_t bytes);
+/* Points `problem` into a wire buffer without copying (the buffer must stay alive and be
+ * 8-byte aligned); checks the magic, the sizes against `bytes` and the CSC structure, and
+ * returns INVALID_ARGUMENT with the reason in last_error otherwise. */
+int sankhya_pdhg_wire_view(const void* buffer, size_t bytes, sankhya_pdhg_problem* problem);
+
 /* Reason for the most recent failing call on this thread (never NULL). */
 const char* sankhya_pdhg_gpu_last_error(void);
 

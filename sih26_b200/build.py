@@ -15,7 +15,8 @@ LIBDIR = os.path.join(HERE, "_lib")
 LIBNAME = "libsankhya_pdhg_gpu.so"
 LIBPATH = os.path.join(LIBDIR, LIBNAME)
 
-SOURCES = ["pdhg_solver.cu", "pdhg_host.cpp", "residuals_noalloc.cu", "batch_server.cu"]
+SOURCES = ["pdhg_solver.cu", "pdhg_host.cpp", "residuals_noalloc.cu", "batch_server.cu",
+           "wire.cpp"]
 HEADERS = ["device_common.cuh", "pdhg_kernels.cuh", "pdhg_host.cuh", "batch_kernels.cuh",
            "prep_kernels.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

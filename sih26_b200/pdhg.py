@@ -105,7 +105,8 @@ EXPORTED_SYMBOLS = ("sankhya_pdhg_gpu_default_params", "sankhya_pdhg_gpu_solve",
                     "sankhya_pdhg_server_default_config", "sankhya_pdhg_server_create",
                     "sankhya_pdhg_server_submit", "sankhya_pdhg_server_step",
                     "sankhya_pdhg_server_result", "sankhya_pdhg_server_free",
-                    "sankhya_pdhg_gpu_batch_solve")
+                    "sankhya_pdhg_gpu_batch_solve", "sankhya_pdhg_wire_size",
+                    "sankhya_pdhg_wire_write", "sankhya_pdhg_wire_view")
 
 # SANKHYA_PDHG_NOALLOC_MAX_ROWS: rows the allocation-free residual check's fixed scratch holds
 NOALLOC_MAX_ROWS = 516064
@@ -298,6 +299,61 @@ def solve_pdhg(model: LP, options: Optional[Options] = None) -> Solution:
     if status not in ("model_error", "infeasible", "unbounded"):
         sol.primal_infeasibility = _primal_infeasibility(model, x)
     return sol
+
+
+# ---- request wire format (sankhya_pdhg_wire_*) ----------------------------------------------
+
+def _bind_wire(lib):
+    if getattr(lib, "_wire_bound", False):
+        return
+    lib.sankhya_pdhg_wire_size.argtypes = [C.POINTER(_Problem)]
+    lib.sankhya_pdhg_wire_size.restype = C.c_size_t
+    lib.sankhya_pdhg_wire_write.argtypes = [C.POINTER(_Problem), C.c_void_p, C.c_size_t]
+    lib.sankhya_pdhg_wire_view.argtypes = [C.c_void_p, C.c_size_t, C.POINTER(_Problem)]
+    lib._wire_bound = True
+
+
+def to_wire(model: LP) -> np.ndarray:
+    """The wire form of an LP (include/sankhya_pdhg_gpu.h): an 8-byte-aligned uint8 array."""
+    lib = load_library()
+    _bind_wire(lib)
+    held = _Held(model)
+    size = lib.sankhya_pdhg_wire_size(C.byref(held.problem))
+    buf = np.zeros((size + 7) // 8, dtype=np.uint64).view(np.uint8)[:size]
+    code = lib.sankhya_pdhg_wire_write(C.byref(held.problem), buf.ctypes.data, size)
+    if code != 0:
+        raise GpuError(code, lib.sankhya_pdhg_gpu_last_error().decode())
+    return buf
+
+
+def from_wire(buffer) -> LP:
+    """An LP read from a wire buffer through sankhya_pdhg_wire_view (the arrays are copied out
+    of the buffer, so it need not outlive the result)."""
+    lib = load_library()
+    _bind_wire(lib)
+    raw = np.frombuffer(buffer, dtype=np.uint8)
+    if raw.ctypes.data % 8:
+        raw = np.frombuffer(raw.tobytes(), dtype=np.uint8)
+    aligned = np.zeros((raw.size + 7) // 8, dtype=np.uint64).view(np.uint8)[:raw.size]
+    aligned[:] = raw
+    prob = _Problem()
+    code = lib.sankhya_pdhg_wire_view(aligned.ctypes.data, aligned.size, C.byref(prob))
+    if code != 0:
+        raise GpuError(code, lib.sankhya_pdhg_gpu_last_error().decode())
+    m, n, nnz = prob.num_rows, prob.num_cols, prob.num_nonzeros
+
+    def arr(ptr, count, dtype):
+        if count == 0:
+            return np.zeros(0, dtype=dtype)
+        return np.ctypeslib.as_array(ptr, shape=(count,)).astype(dtype, copy=True)
+
+    lp = LP(num_rows=m, num_cols=n, col_starts=arr(prob.col_starts, n + 1, np.int32),
+            row_indices=arr(prob.row_indices, nnz, np.int32), values=arr(prob.values, nnz, np.float64),
+            cost=arr(prob.cost, n, np.float64), col_lower=arr(prob.col_lower, n, np.float64),
+            col_upper=arr(prob.col_upper, n, np.float64), row_lower=arr(prob.row_lower, m, np.float64),
+            row_upper=arr(prob.row_upper, m, np.float64), maximize=bool(prob.maximize),
+            objective_offset=float(prob.objective_offset))
+    return lp
 
 
 # ---- many LPs at once (the served / batched engine) ---------------------------------------
