@@ -195,6 +195,9 @@ typedef struct sankhya_pdhg_result {
   sankhya_pdhg_residuals residuals;
   int32_t autotuned;    /* 0 fixed rule, 1 schedule measured by this call, 2 read from cache */
   int32_t schedule[4];  /* stream-row limit and nonzeros per lane of A, then of A' */
+  double primal_infeasibility; /* largest bound violation of col_value and of A col_value,
+                                  in original units (Solution::recompute_quality,
+                                  src/core/model.cpp:228-283), computed on the device */
   char message[512];
 } sankhya_pdhg_result;
 
@@ -255,10 +258,15 @@ typedef struct sankhya_pdhg_server_config {
   double memory_fraction;  /* share of free device memory for the pool (default 0.8) */
   int64_t pool_bytes;      /* explicit pool size; 0 = use memory_fraction */
   int32_t max_active;      /* LP slots (default 4096) */
-  int64_t chunk_attempts;  /* attempts per LP per step; 0 = run each LP to its end */
+  int64_t chunk_attempts;  /* attempts per LP per step for LPs with at most 16,384 nonzeros
+                              per block; larger LPs get proportionally fewer (at least 8), so
+                              a step lasts about as long for every LP; 0 = run each LP to its
+                              end */
   int64_t cluster_min_nnz; /* LPs with at least this many nonzeros run on an 8-block thread
                               block cluster instead of one block (default 16384; 0 = never) */
-  int32_t clusters;        /* clusters kept for those LPs (default 16) */
+  int32_t clusters;        /* clusters for those LPs; 0 (default): chosen every round from
+                              the large LPs' share of the active nonzeros (the rest of the GPU
+                              runs the small LPs on single blocks) */
   int32_t reserved[7];
 } sankhya_pdhg_server_config;
 

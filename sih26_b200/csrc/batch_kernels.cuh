@@ -29,6 +29,7 @@ namespace sih26 {
 namespace cg = cooperative_groups;
 
 constexpr int kClusterSize = 8;
+constexpr long long kChunkNnz = 16384;  // nonzeros per block an attempt of chunk_attempts covers
 constexpr int kGroupSlots = 16;
 
 struct BatchSlot {
@@ -264,8 +265,11 @@ __device__ __noinline__ void group_report(const BatchSlot& B, Ctrl& c, double* s
   ColEval<double, 1> ce{P.dc, P.cl0, P.cu0, P.c0, nullptr, nullptr, S.best_x, B.x_out, B.red_out};
   run_phase<1, kEvalSlots>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pat, Gather1<double>{S.best_y}, ce,
                            acc, stream, rank);
-  grp.template reduce<kEvalSlots, kEvalMaxMask>(acc, sh);
-  if (threadIdx.x == 0) c.best = make_residuals(acc, 0, c.bound_norm, c.cost_norm);
+  grp.template reduce<kEvalSlots, kReportMaxMask>(acc, sh);
+  if (threadIdx.x == 0) {
+    c.best = make_residuals(acc, 0, c.bound_norm, c.cost_norm);
+    c.primal_violation = dmax(0.0, dmax(acc[1], acc[9]));
+  }
   __syncthreads();
 }
 
@@ -277,6 +281,16 @@ __device__ inline void run_instance(const BatchSlot& B, Ctrl& c, double* sh, dou
   const int rank = grp.rank();
   if (threadIdx.x == 0) c = *S.ctrl;
   __syncthreads();
+  // The chunk is a budget of work, not of attempts: chunk_attempts for an LP with at most
+  // kChunkNnz nonzeros per block, proportionally fewer attempts (at least 8) for larger ones,
+  // so a launch lasts about as long for every LP and no slot idles behind one large LP.
+  {
+    const long long per_block = (long long)__ldg(P.A.ptr + P.m) / Grp::kSize;
+    if (per_block > kChunkNnz && chunk_attempts < (1ll << 40)) {
+      const long long scaled = chunk_attempts * kChunkNnz / per_block;
+      chunk_attempts = scaled < 8 ? 8 : scaled;
+    }
+  }
   if (c.state == kSetup) {
     const int nnz = __ldg(P.A.ptr + P.m);
     const double norm = group_power(P, S, nnz, sh, stream, grp);

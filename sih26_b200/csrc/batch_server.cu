@@ -17,6 +17,7 @@
 #include <atomic>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -307,6 +308,12 @@ struct Server {
   int* h_active2 = nullptr;
   int* h_counts = nullptr;
   cudaGraphExec_t graph = nullptr;
+  // the split of the GPU between the two classes: clusters for the large LPs, single blocks
+  // for the others; chosen per round from the active work, the graph rebuilt when it changes
+  int slots_total = 0;     // co-resident blocks of the batch kernels
+  int max_clusters = 0;    // co-resident 8-block clusters
+  int clusters = 0;        // clusters of the current graph
+  int small_grid = 0;      // single blocks of the current graph
   std::vector<int> free_slots;
   std::vector<std::shared_ptr<Job>> slot_job;
   std::vector<int> active;  // slot indices, largest LP first
@@ -383,13 +390,8 @@ BatchSlot relocate(const Job& J, unsigned char* base, Ctrl* ctrl) {
   return b;
 }
 
-void build_graph(Server& s) {
-  cudaStream_t cap, side;
-  SIH26_SCUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), SANKHYA_GPU_INIT_FAILED);
-  SIH26_SCUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking), SANKHYA_GPU_INIT_FAILED);
-  cudaEvent_t fork, join;
-  SIH26_SCUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), SANKHYA_GPU_INIT_FAILED);
-  SIH26_SCUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming), SANKHYA_GPU_INIT_FAILED);
+// Occupancy of the batch kernels: how many blocks, and how many 8-block clusters, fit at once.
+void query_capacity(Server& s) {
   int bpsm = 0;
   SIH26_SCUDA(cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)stream_smem_bytes()), SANKHYA_GPU_INIT_FAILED);
@@ -401,8 +403,7 @@ void build_graph(Server& s) {
               SANKHYA_GPU_INIT_FAILED);
   cudaDeviceProp props{};
   SIH26_SCUDA(cudaGetDeviceProperties(&props, s.cfg.device), SANKHYA_GPU_INIT_FAILED);
-  const int slots_total = props.multiProcessorCount * std::max(1, std::min(bpsm, 2));
-  // clusters that fit at once
+  s.slots_total = props.multiProcessorCount * std::max(1, std::min(bpsm, 2));
   cudaLaunchConfig_t lc{};
   lc.gridDim = dim3(kClusterSize);
   lc.blockDim = dim3(kThreads);
@@ -417,9 +418,27 @@ void build_graph(Server& s) {
   int max_clusters = 0;
   SIH26_SCUDA(cudaOccupancyMaxActiveClusters(&max_clusters, cluster_batch_kernel, &lc),
               SANKHYA_GPU_INIT_FAILED);
-  const int want = s.cfg.clusters > 0 ? s.cfg.clusters : 16;  // clusters for big LPs
-  const int clusters = std::max(1, std::min(want, max_clusters / 2 > 0 ? max_clusters / 2 : 1));
-  const int small_grid = std::max(1, slots_total - clusters * kClusterSize);
+  // keep at least one cluster's worth of blocks for the single-block class
+  s.max_clusters = std::max(1, std::min(max_clusters, (s.slots_total - kClusterSize) / kClusterSize));
+}
+
+// The round's graph for `clusters` 8-block clusters and the remaining blocks as single blocks:
+// the two persistent kernels side by side on two forked streams, then the control blocks of
+// both classes compacted for the host.
+void build_graph(Server& s, int clusters) {
+  clusters = std::max(1, std::min(clusters, s.max_clusters));
+  const int small_grid = std::max(1, s.slots_total - clusters * kClusterSize);
+  if (s.graph && clusters == s.clusters && small_grid == s.small_grid) return;
+  if (s.graph) {
+    cudaGraphExecDestroy(s.graph);
+    s.graph = nullptr;
+  }
+  cudaStream_t cap, side;
+  SIH26_SCUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), SANKHYA_GPU_INIT_FAILED);
+  SIH26_SCUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking), SANKHYA_GPU_INIT_FAILED);
+  cudaEvent_t fork, join;
+  SIH26_SCUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), SANKHYA_GPU_INIT_FAILED);
+  SIH26_SCUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming), SANKHYA_GPU_INIT_FAILED);
   const long long chunk = s.cfg.chunk_attempts > 0 ? s.cfg.chunk_attempts : (1ll << 40);
   cudaGraph_t g;
   SIH26_SCUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal), SANKHYA_GPU_INIT_FAILED);
@@ -442,6 +461,21 @@ void build_graph(Server& s) {
   cudaEventDestroy(join);
   cudaStreamDestroy(side);
   cudaStreamDestroy(cap);
+  s.clusters = clusters;
+  s.small_grid = small_grid;
+}
+
+// Clusters for this round: the large class's share of the active nonzeros (its work per
+// attempt) of the GPU's blocks, no more than it has LPs, and the configured number when the
+// split is fixed (config.clusters > 0 and no adaptation).
+int clusters_for_round(const Server& s, long long small_nnz, long long big_nnz, int big_count) {
+  if (s.cfg.clusters > 0) return s.cfg.clusters;
+  if (big_count == 0) return 1;
+  const double share = static_cast<double>(big_nnz) / static_cast<double>(std::max(1ll, small_nnz + big_nnz));
+  int want = static_cast<int>(std::lround(share * s.slots_total / kClusterSize));
+  want = std::min(want, big_count);
+  if (small_nnz > 0) want = std::min(want, s.max_clusters);
+  return std::max(1, want);
 }
 
 void finish_job(Server& s, Job& J, const Ctrl& c) {
@@ -594,6 +628,13 @@ static std::vector<int> settle(Server& s, const std::vector<int>& list, const Ct
 static void run_round(Server& s) {
   const int c0 = static_cast<int>(s.active.size()), c1 = static_cast<int>(s.active_big.size());
   if (c0 + c1 == 0) return;
+  long long small_nnz = 0, big_nnz = 0;
+  for (int slot : s.active) small_nnz += s.slot_job[slot]->nnz;
+  for (int slot : s.active_big) big_nnz += s.slot_job[slot]->nnz;
+  int want = clusters_for_round(s, small_nnz, big_nnz, c1);
+  // hysteresis: a small change of the ideal split is not worth a new graph
+  if (s.graph && std::abs(want - s.clusters) <= std::max(1, s.clusters / 4)) want = s.clusters;
+  build_graph(s, want);
   std::memcpy(s.h_active, s.active.data(), c0 * sizeof(int));
   std::memcpy(s.h_active2, s.active_big.data(), c1 * sizeof(int));
   s.h_counts[0] = c0;
@@ -638,7 +679,7 @@ void sankhya_pdhg_server_default_config(sankhya_pdhg_server_config* c) {
   c->max_active = 4096;
   c->chunk_attempts = 2048;
   c->cluster_min_nnz = 16384;
-  c->clusters = 16;
+  c->clusters = 0;  // adaptive: the large class's share of the active nonzeros
 }
 
 int sankhya_pdhg_server_create(const sankhya_pdhg_server_config* config,
@@ -659,9 +700,10 @@ int sankhya_pdhg_server_create(const sankhya_pdhg_server_config* config,
     size_t free_b = 0, total_b = 0;
     SIH26_SCUDA(cudaMemGetInfo(&free_b, &total_b), SANKHYA_GPU_INIT_FAILED);
     const int cap = s->cfg.max_active > 0 ? s->cfg.max_active : 4096;
-    s->pool_bytes = s->cfg.pool_bytes > 0
-                        ? static_cast<size_t>(s->cfg.pool_bytes)
-                        : static_cast<size_t>(free_b * std::min(0.95, std::max(0.01, s->cfg.memory_fraction)));
+    const size_t share =
+        static_cast<size_t>(free_b * std::min(0.95, std::max(0.01, s->cfg.memory_fraction)));
+    s->pool_bytes = s->cfg.pool_bytes > 0 ? std::min(static_cast<size_t>(s->cfg.pool_bytes), share)
+                                          : share;
     s->pool_bytes &= ~size_t(255);
     SIH26_SCUDA(cudaMalloc(&s->pool, s->pool_bytes), SANKHYA_GPU_OUT_OF_MEMORY);
     s->alloc = std::make_unique<sih26::PoolAllocator>(s->pool_bytes);
@@ -682,7 +724,8 @@ int sankhya_pdhg_server_create(const sankhya_pdhg_server_config* config,
     SIH26_SCUDA(cudaMallocHost(&s->h_counts, 2 * sizeof(int)), SANKHYA_GPU_OUT_OF_MEMORY);
     s->slot_job.resize(cap);
     for (int k = cap - 1; k >= 0; --k) s->free_slots.push_back(k);
-    sih26::build_graph(*s);
+    sih26::query_capacity(*s);
+    sih26::build_graph(*s, s->cfg.clusters > 0 ? s->cfg.clusters : 16);
     unsigned long long* d_clock = nullptr;
     SIH26_SCUDA(cudaMalloc(&d_clock, sizeof *d_clock), SANKHYA_GPU_OUT_OF_MEMORY);
     sih26::read_clock<<<1, 1, 0, s->stream>>>(d_clock);
@@ -818,6 +861,7 @@ int sankhya_pdhg_server_result(sankhya_pdhg_server* server, int64_t ticket,
   for (int j = 0; j < J.n && !J.x.empty(); ++j) obj += J.cost[j] * J.x[j];
   r->objective = obj;
   const sih26::Residuals& f = c.best;
+  r->primal_infeasibility = c.primal_violation;
   r->residuals = sankhya_pdhg_residuals{f.primal, f.dual, f.gap, f.primal_objective,
                                         f.dual_objective, f.absolute_primal, f.absolute_dual,
                                         f.gap_as_verified, f.complementarity};
@@ -852,6 +896,20 @@ int sankhya_pdhg_gpu_batch_solve(const sankhya_pdhg_problem* problems, int32_t c
   sankhya_pdhg_server_default_config(&cfg);
   if (params) cfg.device = params->device;
   cfg.chunk_attempts = 0;  // run every LP to its end in one launch
+  // a pool just large enough for every image at once (an upper bound of the layout of
+  // prepare(): 24 bytes per nonzero for both orientations, 17 FP64 vectors per row and per
+  // column, the work partitions and alignment), instead of a share of all free memory
+  {
+    size_t bound = size_t(64) << 20;
+    for (int k = 0; k < count; ++k) {
+      const sankhya_pdhg_problem& q = problems[k];
+      if (q.num_rows < 0 || q.num_cols < 0 || q.num_nonzeros < 0) continue;
+      bound += 26 * static_cast<size_t>(q.num_nonzeros) +
+               200 * (static_cast<size_t>(q.num_rows) + static_cast<size_t>(q.num_cols)) +
+               (size_t(64) << 10);
+    }
+    cfg.pool_bytes = static_cast<int64_t>(bound);
+  }
   sankhya_pdhg_server* server = nullptr;
   int rc = sankhya_pdhg_server_create(&cfg, &server);
   if (rc != SANKHYA_GPU_SUCCESS) return rc;

@@ -71,6 +71,7 @@ struct Ctrl {
   int time_up, farkas_cooldown;
   unsigned long long deadline_ns;  // batched LPs: device-clock deadline, 0 = none
   double farkas_margin;            // batched LPs: normalised margin S - M of the last test
+  double primal_violation;         // report: the reported point's largest bound violation
 };
 
 // SpMV work partition of one CSR matrix in permuted row order (rows sorted by length,
@@ -171,6 +172,10 @@ constexpr int kPartSlots = 32;
 constexpr int kEvalSlots = 16;
 // complementarity slots of the evaluation are max-reductions
 constexpr unsigned kEvalMaxMask = (1u << 6) | (1u << 7) | (1u << 12) | (1u << 13);
+// the report (one candidate) also keeps the largest row and column bound violations of the
+// point in the second candidate's slots 1 and 9: Solution::recompute_quality's
+// primal_infeasibility (src/core/model.cpp:228-283), on the device
+constexpr unsigned kReportMaxMask = kEvalMaxMask | (1u << 1) | (1u << 9);
 
 // dynamic shared memory of the phase kernels: one stream buffer of kItemNnz products per warp
 constexpr size_t stream_smem_bytes() { return (size_t)kWarps * kItemNnz * sizeof(double); }
@@ -1073,6 +1078,7 @@ struct RowEval {
       if (finite_bound(lo)) viol = dmax(viol, lo - act);
       if (finite_bound(hi)) viol = dmax(viol, act - hi);
       acc[0 + q] += viol * viol;
+      if (y_out && q == 0) acc[1] = dmax(acc[1], viol);  // report: largest row violation
       if (yi > 0.0) {
         if (finite_bound(hi)) acc[2 + q] += yi * hi; else acc[4 + q] += yi * yi;
       } else if (yi < 0.0) {
@@ -1124,6 +1130,9 @@ struct ColEval {
       if (x_out && q == 0) {
         x_out[j] = xj;
         reduced_out[j] = d;
+        // report: largest column bound violation
+        if (finite_bound(lo)) acc[9] = dmax(acc[9], lo - xj);
+        if (finite_bound(hi)) acc[9] = dmax(acc[9], xj - hi);
       }
       if (d > 0.0) {
         if (finite_bound(lo)) acc[10 + q] += d * lo; else acc[8 + q] += d * d;
@@ -1460,16 +1469,17 @@ __global__ void __launch_bounds__(kThreads, 2) report_kernel(Prob<T> P, State<T>
   ColEval<T, 1> ce{P.dc, P.cl0, P.cu0, P.c0, nullptr, nullptr, S.best_x, x_out, reduced_out};
   run_phase<1, kEvalSlots>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pat, Gather1<double>{S.best_y}, ce,
                            acc, stream);
-  block_reduce<kEvalSlots, kEvalMaxMask>(acc, sh);
+  block_reduce<kEvalSlots, kReportMaxMask>(acc, sh);
   write_partials(S.partials, 2, acc, kEvalSlots);
   if (!grid_barrier(S.bar)) {
     if (blockIdx.x == 0 && threadIdx.x == 0) S.ctrl->state = kDeviceError;
     return;
   }
   double t[kEvalSlots];
-  reduce_partials<kEvalSlots, kEvalMaxMask>(S.partials, 2, t, sh);
+  reduce_partials<kEvalSlots, kReportMaxMask>(S.partials, 2, t, sh);
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     S.ctrl->best = make_residuals(t, 0, S.ctrl->bound_norm, S.ctrl->cost_norm);
+    S.ctrl->primal_violation = dmax(0.0, dmax(t[1], t[9]));
   }
 }
 

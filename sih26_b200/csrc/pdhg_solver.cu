@@ -1123,6 +1123,7 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
   res->iterate_launches = timer.launches;
   res->kernel_launches = g_launches;
   res->autotuned = autotuned;
+  res->primal_infeasibility = rep.primal_violation;
   res->schedule[0] = sched_a.stream_row_max;
   res->schedule[1] = sched_a.nnz_per_lane;
   res->schedule[2] = sched_at.stream_row_max;

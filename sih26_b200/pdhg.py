@@ -94,7 +94,7 @@ class _Result(C.Structure):
                 ("d2h_bytes", C.c_int64), ("iterate_kernel_seconds", C.c_double),
                 ("iterate_launches", C.c_int64), ("kernel_launches", C.c_int64),
                 ("residuals", _Residuals), ("autotuned", C.c_int32),
-                ("schedule", C.c_int32 * 4),
+                ("schedule", C.c_int32 * 4), ("primal_infeasibility", C.c_double),
                 ("message", C.c_char * 512)]
 
 
@@ -234,8 +234,9 @@ def _arr(a, dtype):
     return np.ascontiguousarray(a, dtype=dtype)
 
 
-def _primal_infeasibility(lp: LP, x: np.ndarray) -> float:
-    """Max row/column bound violation (Solution::recompute_quality, src/core/model.cpp:228-283)."""
+def primal_infeasibility_host(lp: LP, x: np.ndarray) -> float:
+    """Max row/column bound violation (Solution::recompute_quality, src/core/model.cpp:228-283),
+    on the host; the solves report the same figure computed on the device."""
     act = lp.to_scipy_csc() @ x if lp.num_rows else np.zeros(0)
     fin = lambda v: np.abs(v) < 1e30  # noqa: E731
     viol = [0.0]
@@ -297,7 +298,7 @@ def solve_pdhg(model: LP, options: Optional[Options] = None) -> Solution:
         kernel_launches=res.kernel_launches, autotuned=res.autotuned,
         schedule=tuple(res.schedule))
     if status not in ("model_error", "infeasible", "unbounded"):
-        sol.primal_infeasibility = _primal_infeasibility(model, x)
+        sol.primal_infeasibility = res.primal_infeasibility  # computed on the device
     return sol
 
 
@@ -451,7 +452,7 @@ class _Outputs:
             setup_seconds=res.setup_seconds, device_seconds=res.solve_seconds,
             kernel_launches=res.kernel_launches)
         if status not in ("model_error", "infeasible", "unbounded"):
-            sol.primal_infeasibility = _primal_infeasibility(model, self.x)
+            sol.primal_infeasibility = res.primal_infeasibility  # computed on the device
         return sol
 
 
@@ -479,11 +480,12 @@ class Server:
     """A resident GPU server for many LPs (sankhya_pdhg_server_*): submit() queues an LP,
     step() admits what fits and runs one launch over every active LP, result() collects.
     LPs with at least `cluster_min_nnz` nonzeros run on an 8-block thread-block cluster
-    (`clusters` of them are kept), the others on one block each."""
+    (`clusters` of them; 0 = chosen every round from the large LPs' share of the active
+    nonzeros), the others on one block each."""
 
     def __init__(self, device: int = 0, memory_fraction: float = 0.8, pool_bytes: int = 0,
                  max_active: int = 4096, chunk_attempts: int = 2048,
-                 cluster_min_nnz: int = 16384, clusters: int = 16):
+                 cluster_min_nnz: int = 16384, clusters: int = 0):
         self.lib = load_library()
         _bind_server(self.lib)
         cfg = _ServerConfig()

@@ -234,3 +234,18 @@ def test_block_angular_full_size_mixed_to_1e6():
         assert abs(s.objective - lp.optimal_objective) <= 1e-5 * scale, algorithm
         print(f"{algorithm}: {s.iterations} iterations ({s.fp32_iterations} FP32), "
               f"{s.device_seconds:.2f} s on the device")
+
+
+def test_device_primal_infeasibility_matches_the_host_figure():
+    """Solution::recompute_quality's primal_infeasibility (src/core/model.cpp:228-283), which the
+    library now computes on the device for every answer, against the same figure on the host."""
+    lps = [lp for _, lp in generated_cases()] + [lp for _, lp, _ in hand_cases()]
+    for lp in lps:
+        s = P.solve_pdhg(lp, _opts(pdhg_tolerance=1e-4, iteration_limit=2000))
+        host = P.primal_infeasibility_host(lp, s.col_value)
+        scale = max(1.0, float(np.max(np.abs(s.col_value))) if s.col_value.size else 1.0)
+        assert abs(s.primal_infeasibility - host) <= 1e-9 * scale, (lp.name, s.primal_infeasibility, host)
+    sols = P.batch_solve(lps[:4], _opts(pdhg_tolerance=1e-4, iteration_limit=2000))
+    for lp, s in zip(lps[:4], sols):
+        host = P.primal_infeasibility_host(lp, s.col_value)
+        assert abs(s.primal_infeasibility - host) <= 1e-9 * max(1.0, float(np.max(np.abs(s.col_value))))
