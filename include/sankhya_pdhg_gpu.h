@@ -147,8 +147,10 @@ typedef struct sankhya_pdhg_params {
                                row-length statistics and cached on disk
                                (SANKHYA_PDHG_AUTOTUNE_CACHE, else ~/.cache/sih26_b200/
                                autotune.tsv); 0 (default): the fixed rule */
-  int32_t host_prep;        /* 1: scale and permute the LP on the host (build_scaling, permute);
-                               0 (default): on the device. Both give identical bits. */
+  int32_t prep;             /* where the LP is scaled and laid out: 0 (default) on the device
+                               from 100,000 nonzeros and on the host below (per-call launch
+                               costs dominate there), 1 always on the host, 2 always on the
+                               device. All give identical bits. */
   int32_t reserved[2];
 } sankhya_pdhg_params;
 

@@ -12,6 +12,9 @@
 #include <cstdio>
 #include <cstring>
 #include <limits>
+#include <map>
+#include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -288,6 +291,30 @@ static int blocks_per_sm() {
   SIH26_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, ek, kThreads, stream_smem_bytes()),
              SANKHYA_GPU_INIT_FAILED);
   return std::min(best, b);
+}
+
+// Per-device facts that do not change while the process runs: the properties and how many
+// blocks of each level's kernels fit on an SM. The queries (and the shared-memory opt-ins)
+// cost milliseconds -- most of the setup of a small LP -- so they run once per device.
+struct DeviceFacts {
+  cudaDeviceProp props{};
+  int bpsm_fp64 = 0, bpsm_fp32 = 0;
+};
+static const DeviceFacts& device_facts(int device) {
+  static std::mutex mu;
+  static std::map<int, std::unique_ptr<DeviceFacts>> cache;
+  std::lock_guard<std::mutex> lock(mu);
+  std::unique_ptr<DeviceFacts>& slot = cache[device];
+  if (!slot) {
+    auto f = std::make_unique<DeviceFacts>();
+    SIH26_CUDA(cudaGetDeviceProperties(&f->props, device), SANKHYA_GPU_INIT_FAILED);
+    if (f->props.major >= 10) {
+      f->bpsm_fp64 = blocks_per_sm<double>();
+      f->bpsm_fp32 = blocks_per_sm<float>();
+    }
+    slot = std::move(f);
+  }
+  return *slot;
 }
 
 // Runs (iterate, evaluate) launch pairs until the device reports a final state. With
@@ -733,8 +760,8 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
   if (prm.device < 0 || prm.device >= devices)
     throw Failure{SANKHYA_GPU_INVALID_ARGUMENT, "device ordinal out of range"};
   SIH26_CUDA(cudaSetDevice(prm.device), SANKHYA_GPU_INIT_FAILED);
-  cudaDeviceProp props{};
-  SIH26_CUDA(cudaGetDeviceProperties(&props, prm.device), SANKHYA_GPU_INIT_FAILED);
+  const DeviceFacts& facts = device_facts(prm.device);
+  const cudaDeviceProp& props = facts.props;
   if (props.major < 10)
     throw Failure{SANKHYA_GPU_NO_COMPATIBLE_DEVICE, "this library is built for sm_100a (B200)"};
   if (!props.cooperativeLaunch)
@@ -762,7 +789,7 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
   mark("validation");
 
   // ---- preconditioning and layout ----
-  int bpsm = std::min(blocks_per_sm<double>(), prm.precision == SANKHYA_PDHG_MIXED ? blocks_per_sm<float>() : 1 << 20);
+  int bpsm = std::min(facts.bpsm_fp64, prm.precision == SANKHYA_PDHG_MIXED ? facts.bpsm_fp32 : 1 << 20);
   if (bpsm < 1) throw Failure{SANKHYA_GPU_INIT_FAILED, "kernel does not fit on an SM"};
   int G = props.multiProcessorCount * std::min(bpsm, 2);
   const long long work = static_cast<long long>(prob.num_nonzeros) + m + n;
@@ -781,7 +808,9 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
   Common cm{};
   PermutedLp q;           // host: sizes, permutations, row pointers of A and A'
   std::vector<double> x0;  // the starting point, permuted
-  if (prm.host_prep) {
+  constexpr long long kDevicePrepMinNnz = 100000;
+  const bool host_prep = prm.prep == 1 || (prm.prep == 0 && prob.num_nonzeros < kDevicePrepMinNnz);
+  if (host_prep) {
     // build_scaling and permute on the host (pdhg_host.cpp), uploaded
     const Scaling sc = build_scaling(prob, cmin, 10);
     q = permute(prob, sc.values);
@@ -928,12 +957,10 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
     }
   }
 
-  Ctrl* host_ctrl = nullptr;
-  SIH26_CUDA(cudaMallocHost(&host_ctrl, sizeof(Ctrl)), SANKHYA_GPU_OUT_OF_MEMORY);
-  struct HostFree {
-    void* p;
-    ~HostFree() { cudaFreeHost(p); }
-  } hf{host_ctrl};
+  // the pinned control-block mirror: one per calling thread, kept for the thread's lifetime
+  // (a pinned allocation per call costs as much as a small LP's whole setup)
+  thread_local Ctrl* host_ctrl = nullptr;
+  if (!host_ctrl) SIH26_CUDA(cudaMallocHost(&host_ctrl, sizeof(Ctrl)), SANKHYA_GPU_OUT_OF_MEMORY);
 
   cudaEvent_t ev0, ev1;
   SIH26_CUDA(cudaEventCreate(&ev0), SANKHYA_GPU_INIT_FAILED);

@@ -39,6 +39,7 @@ SOLVE_STATUS = {0: "not_solved", 1: "optimal", 2: "feasible", 3: "infeasible", 4
 
 PRECISIONS = {"fp64": 0, "mixed": 1}
 ALGORITHMS = {"reference": 0, "halpern": 1}
+PREPS = {"auto": 0, "host": 1, "device": 2}
 STOP_RULES = {"reference": 0, "relative_kkt": 1}
 
 
@@ -71,7 +72,7 @@ class _Params(C.Structure):
                 ("mixed_switch_tolerance", C.c_double), ("group_size_rows", C.c_int32),
                 ("group_size_cols", C.c_int32), ("grid_blocks", C.c_int32),
                 ("profile_kernels", C.c_int32), ("mixed_stall_checks", C.c_int32),
-                ("algorithm", C.c_int32), ("autotune", C.c_int32), ("host_prep", C.c_int32),
+                ("algorithm", C.c_int32), ("autotune", C.c_int32), ("prep", C.c_int32),
                 ("reserved", C.c_int32 * 2)]
 
 
@@ -159,7 +160,7 @@ class Options:
         "pdhg_mixed_stall_checks": (int, 0),
         "pdhg_algorithm": (str, "reference"),
         "pdhg_autotune": (bool, False),
-        "pdhg_host_prep": (bool, False),
+        "pdhg_prep": (str, "auto"),
     }
 
     def __init__(self, **values):
@@ -175,7 +176,7 @@ class Options:
             value = value.lower() in ("1", "true", "on", "yes")
         if typ is str:
             allowed = {"pdhg_precision": PRECISIONS, "pdhg_stop_rule": STOP_RULES,
-                       "pdhg_algorithm": ALGORITHMS}.get(name)
+                       "pdhg_algorithm": ALGORITHMS, "pdhg_prep": PREPS}.get(name)
             if allowed is not None and value not in allowed:
                 raise ValueError(f"{name} must be one of {sorted(allowed)}")
         self._v[name] = typ(value)
@@ -404,7 +405,7 @@ def _params(opt: Options, lib) -> _Params:
     prm.mixed_stall_checks = opt.get("pdhg_mixed_stall_checks")
     prm.algorithm = ALGORITHMS[opt.get("pdhg_algorithm")]
     prm.autotune = int(opt.get("pdhg_autotune"))
-    prm.host_prep = int(opt.get("pdhg_host_prep"))
+    prm.prep = PREPS[opt.get("pdhg_prep")]
     return prm
 
 

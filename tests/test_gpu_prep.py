@@ -15,8 +15,8 @@ pytestmark = pytest.mark.gpu
 
 def _both(lp, **kw):
     out = []
-    for host in (True, False):
-        o = P.Options(pdhg_tolerance=1e-6, iteration_limit=3000, pdhg_host_prep=host)
+    for where in ("host", "device"):
+        o = P.Options(pdhg_tolerance=1e-6, iteration_limit=3000, pdhg_prep=where)
         for k, v in kw.items():
             o.set(k, v)
         out.append(P.solve_pdhg(lp, o))
