@@ -151,7 +151,9 @@ typedef struct sankhya_pdhg_params {
                                from 100,000 nonzeros and on the host below (per-call launch
                                costs dominate there), 1 always on the host, 2 always on the
                                device. All give identical bits. */
-  int32_t reserved[2];
+  int32_t qp_assume_convex; /* QP only: 1 skips the convexity test (for QPs beyond its
+                                2,000-column limit whose convexity the caller knows) */
+  int32_t reserved[1];
 } sankhya_pdhg_params;
 
 /* Unscaled residual block of the reported point (src/pdhg/pdhg.cpp:81-110). */
@@ -293,6 +295,33 @@ void sankhya_pdhg_server_free(sankhya_pdhg_server* server);
  * to the end, results collected). results[k] is filled like sankhya_pdhg_gpu_solve's. */
 int sankhya_pdhg_gpu_batch_solve(const sankhya_pdhg_problem* problems, int32_t count,
                                  const sankhya_pdhg_params* params, sankhya_pdhg_result* results);
+
+/* ---- Convex QP ------------------------------------------------------------------------------
+ *
+ * min 0.5 x'Qx + c'x (in the model's sense) over the same constraints, by the reference's
+ * Condat-Vu primal-dual method (src/qp/qp_condat_vu.cpp:150-323): the LP engine's primal step
+ * plus the gradient Qx, fixed steps from power-iteration estimates of ||A|| and ||Q||,
+ * termination on max-norm primal and projected-gradient residuals every 50 iterations. Q is
+ * given as its lower triangle in CSC (the reference's Model::hessian, model.hpp:156); the
+ * 0.5 lives in the objective, so an off-diagonal entry stands for two entries of Q. */
+typedef struct sankhya_qp_hessian {
+  int32_t num_nonzeros;
+  const int32_t* col_starts;  /* [n+1], n = problem->num_cols */
+  const int32_t* row_indices; /* [nnz], row >= column, ascending within a column */
+  const double* values;       /* [nnz] */
+} sankhya_qp_hessian;
+
+/* Replaces qp::solve_convex_qp (src/qp/qp_condat_vu.cpp:150). params->tolerance is the
+ * reference's qp_tolerance (default 1e-8 when params->tolerance <= 0); iteration_limit,
+ * time_limit and device as for sankhya_pdhg_gpu_solve. Like the reference, a Q that is not
+ * convex in minimisation sense -- or whose convexity the dense test (n <= 2,000,
+ * src/qp/convexity.cpp:17-136) cannot decide -- returns SUCCESS with status MODEL_ERROR,
+ * unless params->qp_assume_convex is 1. Fills col_value, row_dual (= -sense y), col_dual
+ * (= c + Qx + sense A'y, as the reference), objective (with the quadratic term), status,
+ * iterations, the residual block's absolute_primal / absolute_dual (the two termination
+ * measures), primal_infeasibility and message. */
+int sankhya_qp_gpu_solve(const sankhya_pdhg_problem* problem, const sankhya_qp_hessian* hessian,
+                         const sankhya_pdhg_params* params, sankhya_pdhg_result* result);
 
 /* ---- Request wire format -----------------------------------------------------------------
  *

@@ -125,6 +125,8 @@ def _ref():
         lib.ref_spectral_norm.argtypes = [C.POINTER(_LP), C.c_int, C.c_uint]
         lib.ref_farkas_check.argtypes = [C.POINTER(_LP), _f64p, C.c_char_p, C.c_int]
         lib.ref_ray_check.argtypes = [C.POINTER(_LP), _f64p, C.c_char_p, C.c_int]
+        lib.ref_qp_solve.argtypes = [C.POINTER(_LP), _i32p, _i32p, _f64p, C.c_double, C.c_int64,
+                                     _f64p, _f64p, _f64p, C.POINTER(_RefOut)]
         lib.ref_read_model.argtypes = [C.c_char_p, C.POINTER(_LP), C.c_char_p, C.c_int]
         _libs["ref"] = lib
     return _libs["ref"]
@@ -249,6 +251,28 @@ def ref_ray_check(lp, d) -> tuple[bool, str]:
     why = C.create_string_buffer(512)
     rc = _ref().ref_ray_check(C.byref(pin.s), _p(d, _f64p), why, 512)
     return rc == 1, why.value.decode()
+
+
+def ref_qp_solve(lp, tolerance=1e-8, iteration_limit=-1) -> OracleResult:
+    """qp::solve_convex_qp (src/qp/qp_condat_vu.cpp:150) of the reference build on an LP with
+    a Hessian (lp.hessian_*: lower triangle, CSC)."""
+    lib = _ref()
+    pin = _Pinned(lp)
+    hcs = np.ascontiguousarray(lp.hessian_col_starts, dtype=np.int32)
+    hri = np.ascontiguousarray(lp.hessian_row_indices, dtype=np.int32)
+    hv = np.ascontiguousarray(lp.hessian_values, dtype=np.float64)
+    x = np.zeros(lp.num_cols)
+    rd = np.zeros(lp.num_rows)
+    cd = np.zeros(lp.num_cols)
+    out = _RefOut()
+    rc = lib.ref_qp_solve(C.byref(pin.s), _p(hcs, _i32p), _p(hri, _i32p), _p(hv, _f64p),
+                          tolerance, iteration_limit, _p(x, _f64p), _p(rd, _f64p), _p(cd, _f64p),
+                          C.byref(out))
+    if rc != 0:
+        raise RuntimeError(out.message.decode())
+    return OracleResult(STATUS_NAMES[out.status], out.iterations, out.objective,
+                        out.dual_bound, x, rd, cd, message=out.message.decode(),
+                        solve_seconds=out.solve_seconds)
 
 
 def ref_read_model(path):

@@ -12,6 +12,7 @@
 //   sankhya::farkas_proves_infeasible    src/core/certificate.cpp:29
 //   sankhya::ray_proves_unbounded        src/core/certificate.cpp:121
 //   sankhya::io::read_model              include/sankhya/io.hpp:53  (MPS/LP files, for pins)
+//   sankhya::qp::solve_convex_qp         src/qp/qp_condat_vu.cpp:150 include/sankhya/qp.hpp:20
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -25,6 +26,7 @@
 #include "sankhya/model.hpp"
 #include "sankhya/options.hpp"
 #include "sankhya/pdhg.hpp"
+#include "sankhya/qp.hpp"
 
 #include "la/scaling.hpp"
 
@@ -239,6 +241,52 @@ int ref_read_model(const char* path, ref_lp* lp, char* why, int why_len) {
     return 0;
   } catch (const std::exception& e) {
     if (why) copy_text(why, static_cast<std::size_t>(why_len), e.what());
+    return 1;
+  }
+}
+
+}  // extern "C"
+
+extern "C" {
+
+/// sankhya::qp::solve_convex_qp on the LP plus a Hessian given as its lower triangle in CSC
+/// (the reference's Model::hessian storage). Outputs may be NULL.
+int ref_qp_solve(const ref_lp* lp, const std::int32_t* h_col_starts,
+                 const std::int32_t* h_row_indices, const double* h_values, double tolerance,
+                 std::int64_t iteration_limit, double* col_value, double* row_dual,
+                 double* col_dual, ref_pdhg_out* out) {
+  using namespace sankhya;
+  try {
+    Model model = to_model(*lp);
+    model.hessian.reset(lp->num_cols, lp->num_cols);
+    for (Index j = 0; j < lp->num_cols; ++j) {
+      for (Index k = h_col_starts[j]; k < h_col_starts[j + 1]; ++k) {
+        model.hessian.add_entry(h_row_indices[k], j, h_values[k]);
+      }
+    }
+    model.hessian.finalize(0.0);
+    Options options;
+    options.set_double("qp_tolerance", tolerance);
+    options.set_int("iteration_limit", iteration_limit);
+    Logger logger(stdout, LogLevel::kOff);
+    const Solution s = qp::solve_convex_qp(model, options, logger);
+    out->status = static_cast<std::int32_t>(s.status);
+    out->iterations = s.iterations;
+    out->objective = s.objective;
+    out->dual_bound = s.dual_bound;
+    out->solve_seconds = s.solve_seconds;
+    out->primal_infeasibility = s.primal_infeasibility;
+    out->dual_infeasibility = s.dual_infeasibility;
+    copy_text(out->algorithm, sizeof(out->algorithm), s.algorithm);
+    copy_text(out->message, sizeof(out->message), s.message);
+    const auto n = static_cast<std::size_t>(lp->num_cols);
+    const auto m = static_cast<std::size_t>(lp->num_rows);
+    if (col_value && s.col_value.size() == n) std::memcpy(col_value, s.col_value.data(), n * 8);
+    if (col_dual && s.col_dual.size() == n) std::memcpy(col_dual, s.col_dual.data(), n * 8);
+    if (row_dual && s.row_dual.size() == m) std::memcpy(row_dual, s.row_dual.data(), m * 8);
+    return 0;
+  } catch (const std::exception& e) {
+    copy_text(out->message, sizeof(out->message), e.what());
     return 1;
   }
 }

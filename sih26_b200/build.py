@@ -16,7 +16,7 @@ LIBNAME = "libsankhya_pdhg_gpu.so"
 LIBPATH = os.path.join(LIBDIR, LIBNAME)
 
 SOURCES = ["pdhg_solver.cu", "pdhg_host.cpp", "residuals_noalloc.cu", "batch_server.cu",
-           "wire.cpp"]
+           "wire.cpp", "qp_solver.cu"]
 HEADERS = ["device_common.cuh", "pdhg_kernels.cuh", "pdhg_host.cuh", "batch_kernels.cuh",
            "prep_kernels.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

@@ -56,6 +56,10 @@ class LP:
     farkas_star: Optional[np.ndarray] = None
     # a primal ray when the instance was made unbounded on purpose
     ray_star: Optional[np.ndarray] = None
+    # a quadratic objective 0.5 x'Qx: Q's lower triangle in CSC (include/sankhya/model.hpp:156)
+    hessian_col_starts: Optional[np.ndarray] = None
+    hessian_row_indices: Optional[np.ndarray] = None
+    hessian_values: Optional[np.ndarray] = None
 
     @property
     def num_nonzeros(self) -> int:
@@ -283,6 +287,43 @@ def make_unbounded(lp: LP, rng: np.random.Generator) -> LP:
     out.ray_star = ray
     out.check()
     return out
+
+
+def qp_planted(m: int, n: int, nnz_per_col: int, seed: int, maximize: bool = False,
+               name: str = "") -> LP:
+    """A convex QP with a planted optimum: the LP family of uniform_planted plus
+    Q = diag(d) + B'B (d ~ U(0.1, 1), B sparse with two N(0, 0.5^2) entries per row), stored
+    as its lower triangle; c = A'lam + z - Q x* makes (x*, lam, z) a KKT point, so x* is optimal.
+    With maximize the model is stated as max -(c'x + 0.5 x'Qx), the same problem."""
+    import scipy.sparse as sp
+
+    rng = np.random.default_rng(seed)
+    rows = _distinct_rows_per_column(rng, m, n, nnz_per_col)
+    cols = np.repeat(np.arange(n), nnz_per_col)
+    vals = rng.standard_normal(rows.size)
+    cs, ri, v = _csc_from_coo(m, n, rows.ravel(), cols, vals)
+    a = sp.csc_matrix((v, ri, cs), shape=(m, n))
+    k = max(1, n // 2)
+    b_rows = np.repeat(np.arange(k), 2)
+    b_cols = rng.integers(0, n, size=2 * k)
+    b = sp.coo_matrix((0.5 * rng.standard_normal(2 * k), (b_rows, b_cols)), shape=(k, n)).tocsc()
+    q = (sp.diags(rng.uniform(0.1, 1.0, n)) + (b.T @ b)).tocsc()
+    low = sp.tril(q).tocsc()
+    low.sum_duplicates()
+    low.sort_indices()
+    x, lam, c_lin, lo, up, rl, ru = _plant(rng, a, m, n, np.zeros(m, dtype=np.int8))
+    # _plant set c = A'lam + z for the LP; the QP's gradient adds Q x*
+    c = c_lin - q @ x
+    sense = -1.0 if maximize else 1.0
+    lp = LP(num_rows=m, num_cols=n, col_starts=cs, row_indices=ri, values=v, cost=sense * c,
+            col_lower=lo, col_upper=up, row_lower=rl, row_upper=ru, maximize=maximize,
+            name=name or f"qp-{m}x{n}-s{seed}", x_star=x, row_dual_star=lam,
+            optimal_objective=float(sense * (c @ x + 0.5 * x @ (q @ x))))
+    lp.hessian_col_starts = low.indptr.astype(np.int32)
+    lp.hessian_row_indices = low.indices.astype(np.int32)
+    lp.hessian_values = (sense * low.data).astype(np.float64)
+    lp.check()
+    return lp
 
 
 def uneven_batch(count: int = 512, m_lo: int = 50, m_hi: int = 5_000,

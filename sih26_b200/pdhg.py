@@ -73,7 +73,7 @@ class _Params(C.Structure):
                 ("group_size_cols", C.c_int32), ("grid_blocks", C.c_int32),
                 ("profile_kernels", C.c_int32), ("mixed_stall_checks", C.c_int32),
                 ("algorithm", C.c_int32), ("autotune", C.c_int32), ("prep", C.c_int32),
-                ("reserved", C.c_int32 * 2)]
+                ("qp_assume_convex", C.c_int32), ("reserved", C.c_int32 * 1)]
 
 
 class _Residuals(C.Structure):
@@ -107,7 +107,8 @@ EXPORTED_SYMBOLS = ("sankhya_pdhg_gpu_default_params", "sankhya_pdhg_gpu_solve",
                     "sankhya_pdhg_server_submit", "sankhya_pdhg_server_step",
                     "sankhya_pdhg_server_result", "sankhya_pdhg_server_free",
                     "sankhya_pdhg_gpu_batch_solve", "sankhya_pdhg_wire_size",
-                    "sankhya_pdhg_wire_write", "sankhya_pdhg_wire_view")
+                    "sankhya_pdhg_wire_write", "sankhya_pdhg_wire_view",
+                    "sankhya_qp_gpu_solve")
 
 # SANKHYA_PDHG_NOALLOC_MAX_ROWS: rows the allocation-free residual check's fixed scratch holds
 NOALLOC_MAX_ROWS = 516064
@@ -161,6 +162,8 @@ class Options:
         "pdhg_algorithm": (str, "reference"),
         "pdhg_autotune": (bool, False),
         "pdhg_prep": (str, "auto"),
+        "qp_tolerance": (float, 1e-8),
+        "qp_assume_convex": (bool, False),
     }
 
     def __init__(self, **values):
@@ -300,6 +303,46 @@ def solve_pdhg(model: LP, options: Optional[Options] = None) -> Solution:
         schedule=tuple(res.schedule))
     if status not in ("model_error", "infeasible", "unbounded"):
         sol.primal_infeasibility = res.primal_infeasibility  # computed on the device
+    return sol
+
+
+# ---- convex QP (sankhya_qp_gpu_solve) --------------------------------------------------------
+
+class _Hessian(C.Structure):
+    _fields_ = [("num_nonzeros", C.c_int32), ("col_starts", _i32p), ("row_indices", _i32p),
+                ("values", _f64p)]
+
+
+def solve_qp(model: LP, options: Optional[Options] = None) -> Solution:
+    """GPU successor of qp::solve_convex_qp (src/qp/qp_condat_vu.cpp:150): `model` carries Q's
+    lower triangle in hessian_col_starts / hessian_row_indices / hessian_values; the options
+    read are qp_tolerance, iteration_limit, time_limit, gpu_device and qp_assume_convex."""
+    opt = options or Options()
+    lib = load_library()
+    if not getattr(lib, "_qp_bound", False):
+        lib.sankhya_qp_gpu_solve.argtypes = [C.POINTER(_Problem), C.POINTER(_Hessian),
+                                             C.POINTER(_Params), C.POINTER(_Result)]
+        lib._qp_bound = True
+    held = _Held(model)
+    n = model.num_cols
+    hcs = _arr(model.hessian_col_starts if model.hessian_col_starts is not None
+               else np.zeros(n + 1), np.int32)
+    hri = _arr(model.hessian_row_indices if model.hessian_row_indices is not None
+               else np.zeros(0), np.int32)
+    hv = _arr(model.hessian_values if model.hessian_values is not None else np.zeros(0),
+              np.float64)
+    hes = _Hessian(int(hcs[-1]) if hcs.size else 0, hcs.ctypes.data_as(_i32p),
+                   hri.ctypes.data_as(_i32p), hv.ctypes.data_as(_f64p))
+    prm = _params(opt, lib)
+    prm.tolerance = opt.get("qp_tolerance")
+    prm.qp_assume_convex = int(opt.get("qp_assume_convex"))
+    out = _Outputs(model)
+    code = lib.sankhya_qp_gpu_solve(C.byref(held.problem), C.byref(hes), C.byref(prm),
+                                    C.byref(out.res))
+    if code != 0:
+        raise GpuError(code, lib.sankhya_pdhg_gpu_last_error().decode())
+    sol = out.solution(model)
+    sol.algorithm = "qp-condat-vu-gpu"
     return sol
 
 
