@@ -32,6 +32,9 @@ FP64, unscaled) through the library's C ABI.
           p50 / p99 / p99.9 arrival-to-answer latency, next to one-at-a-time FP64 solves of
           the same pool. Rank 0 only.
 
+  qp      the convex-QP engine on a planted 800 x 2,000 QP next to the reference's own QP
+          engine on the host, and on a 40,000 x 100,000 QP alone (rank 0 only).
+
 `--impl reference` times that CPU reference alone on the same workload and prints its line.
 With torchrun (N > 1) every rank solves its own replica of the LP (a single LP does not
 shard); the time is the maximum over ranks.
@@ -347,6 +350,38 @@ def served_leg(local, rates, seconds, chunk, algorithm="halpern", pool_size=24, 
     return out
 
 
+def qp_leg(local):
+    """Convex QP (sankhya_qp_gpu_solve) beside the reference's own QP engine on the host: the
+    planted 800 x 2,000 QP (the largest the reference's dense convexity test accepts) to its
+    qp_tolerance 1e-6, and a 40,000 x 100,000 one on the GPU alone (convexity asserted by the
+    caller, which the reference cannot do)."""
+    import oracle
+    from sih26_b200 import lpgen, pdhg
+
+    out = {}
+    small = lpgen.qp_planted(800, 2000, 10, seed=21)
+    big = lpgen.qp_planted(40000, 100000, 10, seed=21)
+    for name, lp, assume in (("800x2000", small, False), ("40000x100000", big, True)):
+        o = pdhg.Options(qp_tolerance=1e-6, iteration_limit=400000, qp_assume_convex=assume,
+                         gpu_device=local)
+        pdhg.solve_qp(lp, pdhg.Options(qp_tolerance=1e-6, iteration_limit=100,
+                                       qp_assume_convex=assume, gpu_device=local))
+        t0 = time.perf_counter()
+        s = pdhg.solve_qp(lp, o)
+        gpu = time.perf_counter() - t0
+        rec = {"gpu_s": gpu, "status": s.status, "iterations": s.iterations,
+               "objective_rel_error": abs(s.objective - lp.optimal_objective)
+               / abs(lp.optimal_objective)}
+        if not assume and oracle.ref_available():
+            t0 = time.perf_counter()
+            r = oracle.ref_qp_solve(lp, tolerance=1e-6, iteration_limit=400000)
+            rec["reference_s"] = time.perf_counter() - t0
+            rec["reference_iterations"] = r.iterations
+            rec["reference_status"] = r.status
+        out[name] = rec
+    return out
+
+
 def make_workload():
     from sih26_b200 import lpgen
 
@@ -487,6 +522,7 @@ def run_ours(args):
         rates = [float(r) for r in args.served_rates.split(",") if r]
         served = served_leg(local, rates, args.served_seconds, args.served_chunk,
                             args.algorithm)
+    qp = qp_leg(local) if rank == 0 and not args.no_qp else None
     if rank == 0:
         line = {
             "metric": "time-to-rel-KKT 1e-6 (s), FP32-mixed", "value": dev, "unit": "s",
@@ -525,6 +561,7 @@ def run_ours(args):
             "clocks": clocks.summary(),
             "batched": batched,
             "served": served,
+            "qp": qp,
         }
         print(json.dumps(line))
     if dist is not None:
@@ -566,6 +603,7 @@ def main():
                          "in each precision for comparison)")
     ap.add_argument("--no-batched", action="store_true", help="skip the 512-LP batched leg")
     ap.add_argument("--no-served", action="store_true", help="skip the served-stream leg")
+    ap.add_argument("--no-qp", action="store_true", help="skip the convex-QP leg")
     ap.add_argument("--served-rates", default="50,200",
                     help="Poisson rates, LPs/s, comma-separated (the served family's full "
                          "study is 200,1000,5000 for 60 s)")

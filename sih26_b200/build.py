@@ -35,7 +35,8 @@ def build_library(force: bool = False, verbose: bool = False) -> str:
         return LIBPATH
     os.makedirs(LIBDIR, exist_ok=True)
     tmp = LIBPATH + ".tmp"
-    cmd = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
+    cmd = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-fopenmp",
+           "-shared", "-lgomp",
            "-Xptxas", "-v" if verbose else "-O3",
            "-I", os.path.join(ROOT, "include"), "-I", CSRC,
            *[os.path.join(CSRC, s) for s in SOURCES], "-o", tmp]

@@ -323,6 +323,8 @@ std::string qp_convexity(int n, const sankhya_qp_hessian& h, double sense) {
       continue;
     }
     d[j] = pivot;
+    // the rows below the pivot are independent: each keeps the reference's order over k
+#pragma omp parallel for schedule(static) if (n - j > 256)
     for (int i = j + 1; i < n; ++i) {
       double sum = q[i * un + j];
       for (int k = 0; k < j; ++k) sum -= l[i * un + k] * l[j * un + k] * d[k];
