@@ -67,18 +67,22 @@ __device__ __forceinline__ void block_reduce(double (&v)[NS], double* shared) {
   __syncthreads();
 }
 
-// Grid-wide barrier for a cooperative launch (all blocks co-resident). Thread 0 of each
-// block arrives on a counter with an acq_rel atomic; the last arriver resets the counter and
-// publishes a new generation with a release store; the others poll the generation with
-// acquire loads. bar.sync on either side extends the ordering to every thread of the block,
-// so every write before the barrier is visible to every read after it.
+// Grid-wide barrier for a cooperative launch (all blocks co-resident), on one word. Thread 0
+// of each block adds to the word with an acq_rel atomic: block 0 adds 2^31 - (G - 1), every
+// other block adds 1, so the word's top bit flips exactly when the last block arrives and
+// its low 31 bits return to zero. The last arriver learns it from its own atomic; the others
+// poll the word with acquire loads until the top bit differs from the value their atomic
+// returned. bar.sync on either side extends the ordering to every thread of the block, so
+// every write before the barrier is visible to every read after it. One atomic round trip
+// for the last arriver, one poll after the flip for the others.
 //
 // Waiters give up after `limit_ns` (or as soon as another block has given up): they record an
 // error and return false instead of waiting on, so a broken launch ends instead of hanging
-// the GPU.
+// the GPU. A block that passed a barrier while another gave up stops at the next one, where
+// its own wait sees the error word.
 struct GridBarrier {
-  unsigned* count;
-  unsigned* generation;
+  unsigned* count;                  // the barrier word; zero before the first barrier
+  unsigned* generation;             // unused (kept for the layout of the control words)
   int* error;
   unsigned long long limit_ns;
   int* time_up;                     // set by the last arriver: global time > deadline_ns
@@ -106,17 +110,17 @@ __device__ __forceinline__ bool grid_barrier(const GridBarrier& b) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
-    const unsigned g = ld_acquire(b.generation);
-    const unsigned arrived = atom_add_acq_rel(b.count, 1u);
+    const unsigned add = blockIdx.x == 0 ? 0x80000000u - (gridDim.x - 1u) : 1u;
+    const unsigned old = atom_add_acq_rel(b.count, add);
     int good = 1;
-    if (arrived == gridDim.x - 1) {
-      if (b.deadline_ns != 0ull && global_ns() > b.deadline_ns) atomicExch(b.time_up, 1);
-      st_relaxed(b.count, 0u);
-      st_release(b.generation, g + 1u);
+    if (((old ^ (old + add)) & 0x80000000u) != 0u) {
+      // the last arriver
+      if (b.deadline_ns != 0ull && global_ns() > b.deadline_ns)
+        st_relaxed(reinterpret_cast<unsigned*>(b.time_up), 1u);
     } else {
       const unsigned long long t0 = global_ns();
       unsigned spins = 0;
-      while (ld_acquire(b.generation) == g) {
+      while (((ld_acquire(b.count) ^ old) & 0x80000000u) == 0u) {
         ++spins;
         if (spins > 4096) __nanosleep(32);
         if ((spins & 1023u) == 0) {
@@ -132,7 +136,7 @@ __device__ __forceinline__ bool grid_barrier(const GridBarrier& b) {
         }
       }
     }
-    ok = good && (*((volatile int*)b.error) == 0);
+    ok = good;
   }
   __syncthreads();
   return ok != 0;

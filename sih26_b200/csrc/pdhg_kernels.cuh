@@ -901,7 +901,13 @@ __global__ void __launch_bounds__(kThreads, 2) iterate_kernel(Prob<T> P, State<T
   __shared__ Ctrl c;
   __shared__ double sh[kWarps * 4];
   double* stream = warp_stream();
-  if (threadIdx.x == 0) c = *S.ctrl;
+  if (threadIdx.x == 0) {
+    c = *S.ctrl;
+    // The deadline flag is read once per launch: the last arriver of a barrier sets it after
+    // the barrier opens, so only a read made before this launch's first barrier is the same
+    // in every block.
+    c.time_up |= *((volatile int*)S.bar.time_up);
+  }
   __syncthreads();
   if (c.state != kRunning) return;
   const int G = gridDim.x;
@@ -947,10 +953,7 @@ __global__ void __launch_bounds__(kThreads, 2) iterate_kernel(Prob<T> P, State<T
       SIH26_MARK(2);
       if (!grid_barrier(S.bar)) goto device_error;
       SIH26_MARK(3);
-      if (threadIdx.x == 0) {
-        halpern_control(c);
-        c.time_up = *((volatile int*)S.bar.time_up);
-      }
+      if (threadIdx.x == 0) halpern_control(c);
       __syncthreads();
       SIH26_MARK(4);
       if (c.state != kRunning) break;
@@ -984,10 +987,7 @@ __global__ void __launch_bounds__(kThreads, 2) iterate_kernel(Prob<T> P, State<T
     {
       double tot[3];
       reduce_partials<3, 0u>(part, 0, tot, sh);
-      if (threadIdx.x == 0) {
-        step_control(c, tot);
-        c.time_up = *((volatile int*)S.bar.time_up);
-      }
+      if (threadIdx.x == 0) step_control(c, tot);
       __syncthreads();
       SIH26_MARK(4);
       if (c.state != kRunning) break;

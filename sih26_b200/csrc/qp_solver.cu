@@ -142,7 +142,11 @@ __global__ void __launch_bounds__(kThreads, 2) qp_kernel(QpDev Q, long long max_
   __shared__ Ctrl c;
   __shared__ double sh[kWarps * 2];
   double* stream = warp_stream();
-  if (threadIdx.x == 0) c = *Q.ctrl;
+  if (threadIdx.x == 0) {
+    c = *Q.ctrl;
+    // read once per launch, before the first barrier, so every block sees the same flag
+    c.time_up |= *((volatile int*)Q.bar.time_up);
+  }
   __syncthreads();
   if (c.state != kRunning) return;
   const int G = gridDim.x;
@@ -187,7 +191,6 @@ __global__ void __launch_bounds__(kThreads, 2) qp_kernel(QpDev Q, long long max_
     if (threadIdx.x == 0) {
       c.cur = nxt;
       if (c.state != kConverged) ++c.iteration;
-      c.time_up = *((volatile int*)Q.bar.time_up);
     }
     __syncthreads();
     if (c.state != kRunning) break;
