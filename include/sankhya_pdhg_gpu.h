@@ -172,6 +172,22 @@ typedef struct sankhya_pdhg_residuals {
 /* Result. The caller allocates the arrays (any may be NULL); the library fills the rest.
  * Sign conventions follow src/pdhg/pdhg.cpp:647-661: row_dual = sense * (-y),
  * col_dual = sense * (c_min + A'y), with y the PDHG multiplier. */
+/* Quality of the reported point, as Solution::recompute_quality (src/core/model.cpp:228-424)
+ * measures it, computed on the device from the reported x, row_dual and col_dual in original
+ * units. The same definitions term by term; only the rounding of the row and column sums
+ * differs from the host code's. LP solves fill every field; the QP solve fills
+ * primal_infeasibility only and sets the other fields to NaN. */
+typedef struct sankhya_pdhg_quality {
+  double primal_infeasibility;        /* max violation over row and column bounds */
+  double primal_infeasibility_scaled; /* each violation over its quantity's term scale */
+  double dual_infeasibility;          /* max reduced-cost / row-price sign violation and
+                                         max |c - A'row_dual - col_dual| */
+  double dual_infeasibility_scaled;   /* the same (and complementarity) over their scales */
+  double complementarity_violation;   /* max |multiplier| * distance to the nearest bound */
+  double absolute_gap;                /* |objective - dual_bound| */
+  double relative_gap;                /* absolute_gap / max(1, |objective|) */
+} sankhya_pdhg_quality;
+
 typedef struct sankhya_pdhg_result {
   double* col_value;   /* [n] */
   double* row_dual;    /* [m] */
@@ -202,6 +218,7 @@ typedef struct sankhya_pdhg_result {
   double primal_infeasibility; /* largest bound violation of col_value and of A col_value,
                                   in original units (Solution::recompute_quality,
                                   src/core/model.cpp:228-283), computed on the device */
+  sankhya_pdhg_quality quality; /* the whole recompute_quality block of the reported point */
   char message[512];
 } sankhya_pdhg_result;
 

@@ -23,7 +23,9 @@ from .loader import (  # noqa: F401
     ref_qp_solve,
     ref_ray_check,
     ref_read_model,
+    ref_recompute_quality,
     ref_scaling,
     ref_solve,
     ref_spectral_norm,
 )
+from .quality import recompute_quality  # noqa: F401,E402

@@ -128,6 +128,8 @@ def _ref():
         lib.ref_qp_solve.argtypes = [C.POINTER(_LP), _i32p, _i32p, _f64p, C.c_double, C.c_int64,
                                      _f64p, _f64p, _f64p, C.POINTER(_RefOut)]
         lib.ref_read_model.argtypes = [C.c_char_p, C.POINTER(_LP), C.c_char_p, C.c_int]
+        lib.ref_recompute_quality.argtypes = [C.POINTER(_LP), _f64p, _f64p, _f64p, C.c_double,
+                                              _f64p]
         _libs["ref"] = lib
     return _libs["ref"]
 
@@ -297,3 +299,20 @@ def ref_read_model(path):
               row_lower=arrs["rl"], row_upper=arrs["ru"], maximize=bool(head.maximize),
               objective_offset=head.objective_offset,
               name=os.path.splitext(os.path.basename(path))[0])
+
+
+QUALITY_KEYS = ("primal_infeasibility", "primal_infeasibility_scaled", "dual_infeasibility",
+                "dual_infeasibility_scaled", "complementarity_violation", "objective",
+                "absolute_gap", "relative_gap")
+
+
+def ref_recompute_quality(lp, x, row_dual, col_dual, dual_bound) -> dict:
+    """Solution::recompute_quality (src/core/model.cpp:228-424) of the reference build."""
+    pin = _Pinned(lp)
+    arrs = [np.ascontiguousarray(v, dtype=np.float64) for v in (x, row_dual, col_dual)]
+    out = np.zeros(8)
+    rc = _ref().ref_recompute_quality(C.byref(pin.s), *[_p(a, _f64p) for a in arrs],
+                                      float(dual_bound), _p(out, _f64p))
+    if rc != 0:
+        raise RuntimeError("recompute_quality failed")
+    return dict(zip(QUALITY_KEYS, out.tolist()))

@@ -13,6 +13,8 @@
 //   sankhya::ray_proves_unbounded        src/core/certificate.cpp:121
 //   sankhya::io::read_model              include/sankhya/io.hpp:53  (MPS/LP files, for pins)
 //   sankhya::qp::solve_convex_qp         src/qp/qp_condat_vu.cpp:150 include/sankhya/qp.hpp:20
+//   sankhya::Solution::recompute_quality src/core/model.cpp:228      include/sankhya/model.hpp:373
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -287,6 +289,42 @@ int ref_qp_solve(const ref_lp* lp, const std::int32_t* h_col_starts,
     return 0;
   } catch (const std::exception& e) {
     copy_text(out->message, sizeof(out->message), e.what());
+    return 1;
+  }
+}
+
+}  // extern "C"
+
+extern "C" {
+
+/// Solution::recompute_quality of a given point (x, row_dual, col_dual in the reference's
+/// sign conventions) and dual bound on the LP. out[8] = primal_infeasibility,
+/// primal_infeasibility_scaled, dual_infeasibility, dual_infeasibility_scaled,
+/// complementarity_violation, objective, absolute_gap, relative_gap.
+int ref_recompute_quality(const ref_lp* lp, const double* col_value, const double* row_dual,
+                          const double* col_dual, double dual_bound, double* out) {
+  using namespace sankhya;
+  try {
+    const Model model = to_model(*lp);
+    Solution s;
+    s.allocate_for(model);
+    const auto n = static_cast<std::size_t>(lp->num_cols);
+    const auto m = static_cast<std::size_t>(lp->num_rows);
+    std::copy(col_value, col_value + n, s.col_value.begin());
+    std::copy(col_dual, col_dual + n, s.col_dual.begin());
+    std::copy(row_dual, row_dual + m, s.row_dual.begin());
+    s.dual_bound = dual_bound;
+    s.recompute_quality(model);
+    out[0] = s.primal_infeasibility;
+    out[1] = s.primal_infeasibility_scaled;
+    out[2] = s.dual_infeasibility;
+    out[3] = s.dual_infeasibility_scaled;
+    out[4] = s.complementarity_violation;
+    out[5] = s.objective;
+    out[6] = s.absolute_gap;
+    out[7] = s.relative_gap;
+    return 0;
+  } catch (const std::exception&) {
     return 1;
   }
 }

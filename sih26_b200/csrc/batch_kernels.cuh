@@ -270,6 +270,17 @@ __device__ __noinline__ void group_report(const BatchSlot& B, Ctrl& c, double* s
     c.best = make_residuals(acc, 0, c.bound_norm, c.cost_norm);
     c.primal_violation = dmax(0.0, dmax(acc[1], acc[9]));
   }
+  // quality of the reported point (the group's reduction above ordered the outputs' writes)
+  double qv[kQualitySlots];
+#pragma unroll
+  for (int k = 0; k < kQualitySlots; ++k) qv[k] = 0.0;
+  quality_pass(P, S.best_x, S.best_y, B.x_out, B.y_out, B.red_out,
+               rank * kWarps + (int)(threadIdx.x >> 5), Grp::kSize * kWarps, qv);
+  grp.template reduce<kQualitySlots, 0xFFu>(qv, sh);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < kQualitySlots; ++k) c.quality[k] = qv[k];
+  }
   __syncthreads();
 }
 

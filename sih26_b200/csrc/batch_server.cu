@@ -869,6 +869,8 @@ int sankhya_pdhg_server_result(sankhya_pdhg_server* server, int64_t ticket,
   r->dual_bound = (J.status == SANKHYA_PDHG_OPTIMAL)
                       ? sense * f.dual_objective + J.view.objective_offset
                       : (J.view.maximize ? INFINITY : -INFINITY);
+  r->quality = sih26::quality_from_slots(c.quality, r->objective, r->dual_bound);
+  r->quality.primal_infeasibility = r->primal_infeasibility;  // one figure for both fields
   if (r->col_value && !J.x.empty()) std::memcpy(r->col_value, J.x.data(), J.n * 8);
   if (r->col_dual && !J.col_dual.empty()) std::memcpy(r->col_dual, J.col_dual.data(), J.n * 8);
   if (r->row_dual && !J.row_dual.empty()) std::memcpy(r->row_dual, J.row_dual.data(), J.m * 8);

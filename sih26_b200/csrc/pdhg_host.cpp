@@ -476,6 +476,19 @@ PermutedLp permute(const sankhya_pdhg_problem& p, const std::vector<double>& v) 
   return q;
 }
 
+sankhya_pdhg_quality quality_from_slots(const double* q, double objective, double dual_bound) {
+  sankhya_pdhg_quality r{};
+  r.primal_infeasibility = q[0];
+  r.primal_infeasibility_scaled = q[1];
+  r.dual_infeasibility = q[2];
+  const double price_scale = std::max(1.0, q[7]);
+  r.dual_infeasibility_scaled = std::max(q[3], std::max(q[5], q[6]) / price_scale);
+  r.complementarity_violation = q[4];
+  r.absolute_gap = std::fabs(objective - dual_bound);
+  r.relative_gap = r.absolute_gap / std::max(1.0, std::fabs(objective));
+  return r;
+}
+
 static int lanes_for(int len, int nnz_per_lane) {
   // smallest power of two with at most nnz_per_lane nonzeros per lane, capped at a warp
   int lanes = 1;

@@ -63,6 +63,11 @@ struct Schedule {
   int stream_row_max = 32;
   int nnz_per_lane = 16;
 };
+// The result's quality block from the device's quality slots (kQualitySlots in
+// pdhg_kernels.cuh), the objective and the dual bound: the row-price terms take the dual-norm
+// scale max(1, max |row_dual|) here, and the gaps follow src/core/model.cpp:419-421.
+sankhya_pdhg_quality quality_from_slots(const double* slots, double objective, double dual_bound);
+
 struct HostPart {
   std::vector<int> blk_seg_begin, blk_long_begin, blk_item_begin;
   std::vector<int4> segs, longs, items;

@@ -55,6 +55,14 @@ struct Residuals {
       gap_as_verified, complementarity;
 };
 
+// Quality of a reported point (Solution::recompute_quality, src/core/model.cpp:228-424), every
+// slot a maximum of non-negative terms: 0 primal_infeasibility, 1 primal_infeasibility_scaled,
+// 2 dual_infeasibility, 3 dual_infeasibility_scaled (column terms), 4
+// complementarity_violation, 5 the largest row-price sign violation and 6 the largest row
+// complementarity product over its row scale (both divided by the dual-norm scale once slot 7,
+// max |row_dual|, is known).
+constexpr int kQualitySlots = 8;
+
 // Host <-> device control block of one LP. Block 0 writes it at kernel exit; every block
 // reads it at kernel entry.
 struct Ctrl {
@@ -72,6 +80,7 @@ struct Ctrl {
   unsigned long long deadline_ns;  // batched LPs: device-clock deadline, 0 = none
   double farkas_margin;            // batched LPs: normalised margin S - M of the last test
   double primal_violation;         // report: the reported point's largest bound violation
+  double quality[kQualitySlots];   // report: the reported point's quality slots (above)
 };
 
 // SpMV work partition of one CSR matrix in permuted row order (rows sorted by length,
@@ -893,7 +902,9 @@ __device__ unsigned long long g_phase_ns[4096 * 5];
 #define SIH26_MARK_START() (mark_ns = 0ull)
 #endif
 
-template <class T>
+// One instance per operator (kHalpern: the Halpern operator, else the reference's adaptive
+// step), so each carries only its own step's registers.
+template <class T, bool kHalpern>
 __global__ void __launch_bounds__(kThreads, 2) iterate_kernel(Prob<T> P, State<T> S,
                                                               long long max_attempts) {
   unsigned long long mark_ns = 0;
@@ -930,7 +941,7 @@ __global__ void __launch_bounds__(kThreads, 2) iterate_kernel(Prob<T> P, State<T
     double* part = S.partials + (size_t)(c.attempts & 1) * G * kPartSlots;
     double acc[3] = {0.0, 0.0, 0.0};
     SIH26_MARK_START();
-    if (c.halpern) {
+    if constexpr (kHalpern) {
       const double w = (double)(c.averaged + 1) / (double)(c.averaged + 2);
       if constexpr (kDelta<T>) {
         PrimalStepHalpernDelta<T> ps{S.x[cur], S.x[nxt], S.xt, S.cg, S.dl, S.du, tau, w};
@@ -1453,6 +1464,125 @@ device_error:
   if (blockIdx.x == 0 && threadIdx.x == 0) S.ctrl->state = kDeviceError;
 }
 
+// ---- quality of the reported point ------------------------------------------------------
+//
+// Solution::recompute_quality (src/core/model.cpp:228-424) on the device, from the reported
+// point in original units (x_out, y_out = the PDHG multiplier y, whose reference row_dual is
+// -sense y, and red_out = c + A'y in min space, whose sign-folded col_dual is red_out itself)
+// and the scaled FP64 point the matrix terms are formed from: a_ij x_j = (A^_ij x^_j) / Dr_i
+// and a_ij row_dual_i = -sense (A^_ij y^_i) / Dc_j. One warp per row of A, then per row of
+// A' (column of A); `wid` of `wtot` warps. Each term is the reference's term; only the
+// rounding of the sums and of the scaled products differs.
+__device__ __forceinline__ double nearest_bound_distance(double v, double lo, double hi) {
+  double d = INFINITY;
+  if (finite_bound(lo)) d = dmin(d, fabs(v - lo));
+  if (finite_bound(hi)) d = dmin(d, fabs(v - hi));
+  return d;
+}
+
+template <class T>
+__device__ __forceinline__ void quality_pass(const Prob<T>& P, const double* bx, const double* by,
+                                             const double* x_out, const double* y_out,
+                                             const double* red_out, int wid, int wtot,
+                                             double (&q)[kQualitySlots]) {
+  const int lane = threadIdx.x & 31;
+  // rows: activity, the row's term scale max(1, max_j |a_ij x_j|), bounds, row prices
+  for (int i = wid; i < P.m; i += wtot) {
+    double sum = 0.0, big = 0.0;
+    const int kb = __ldg(P.A.ptr + i), ke = __ldg(P.A.ptr + i + 1);
+    for (int k = kb + lane; k < ke; k += 32) {
+      const double t = __ldg(P.A.val64 + k) * __ldcg(bx + __ldg(P.A.idx + k));
+      sum += t;
+      big = dmax(big, fabs(t));
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      sum += __shfl_xor_sync(0xffffffffu, sum, off);
+      big = dmax(big, __shfl_xor_sync(0xffffffffu, big, off));
+    }
+    if (lane == 0) {
+      const double dr = __ldg(P.dr + i), lo = __ldg(P.rl0 + i), hi = __ldg(P.ru0 + i);
+      const double act = sum / dr;
+      const double scale = dmax(1.0, big / dr);
+      if (finite_bound(lo) && lo - act > 0.0) {
+        q[0] = dmax(q[0], lo - act);
+        q[1] = dmax(q[1], (lo - act) / scale);
+      }
+      if (finite_bound(hi) && act - hi > 0.0) {
+        q[0] = dmax(q[0], act - hi);
+        q[1] = dmax(q[1], (act - hi) / scale);
+      }
+      const double yref = -__ldcg(y_out + i);  // sense * row_dual
+      q[7] = dmax(q[7], fabs(yref));
+      if (lo != hi) {
+        double sign = 0.0;
+        if (yref > 0.0 && !finite_bound(lo)) sign = yref;
+        if (yref < 0.0 && !finite_bound(hi)) sign = -yref;
+        if (sign > 0.0) {
+          q[2] = dmax(q[2], sign);
+          q[5] = dmax(q[5], sign);
+        }
+        const double slack = nearest_bound_distance(act, lo, hi);
+        if (yref != 0.0 && finite_bound(slack)) {
+          const double product = fabs(yref) * slack;
+          q[4] = dmax(q[4], product);
+          q[6] = dmax(q[6], product / scale);
+        }
+      }
+    }
+  }
+  // columns: bounds, the consistency of col_dual with c - A'row_dual, sign, complementarity
+  for (int j = wid; j < P.n; j += wtot) {
+    double sum = 0.0, big = 0.0;
+    const int kb = __ldg(P.AT.ptr + j), ke = __ldg(P.AT.ptr + j + 1);
+    for (int k = kb + lane; k < ke; k += 32) {
+      const double t = __ldg(P.AT.val64 + k) * __ldcg(by + __ldg(P.AT.idx + k));
+      sum += t;
+      big = dmax(big, fabs(t));
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      sum += __shfl_xor_sync(0xffffffffu, sum, off);
+      big = dmax(big, __shfl_xor_sync(0xffffffffu, big, off));
+    }
+    if (lane == 0) {
+      const double dc = __ldg(P.dc + j), lo = __ldg(P.cl0 + j), hi = __ldg(P.cu0 + j);
+      const double c = __ldg(P.c0 + j);
+      const double x = __ldcg(x_out + j), d = __ldcg(red_out + j);
+      const double xs = dmax(1.0, fabs(x));
+      if (finite_bound(lo) && lo - x > 0.0) {
+        q[0] = dmax(q[0], lo - x);
+        q[1] = dmax(q[1], (lo - x) / xs);
+      }
+      if (finite_bound(hi) && x - hi > 0.0) {
+        q[0] = dmax(q[0], x - hi);
+        q[1] = dmax(q[1], (x - hi) / xs);
+      }
+      const double scale = dmax(1.0, dmax(fabs(c), big / dc));
+      const double gap = fabs(c + sum / dc - d);  // |implied - col_dual|, sign folded
+      if (gap > 0.0) {
+        q[2] = dmax(q[2], gap);
+        q[3] = dmax(q[3], gap / scale);
+      }
+      if (lo != hi) {
+        double sign = 0.0;
+        if (d > 0.0 && !finite_bound(lo)) sign = d;
+        if (d < 0.0 && !finite_bound(hi)) sign = -d;
+        if (sign > 0.0) {
+          q[2] = dmax(q[2], sign);
+          q[3] = dmax(q[3], sign / scale);
+        }
+        const double slack = nearest_bound_distance(x, lo, hi);
+        if (d != 0.0 && finite_bound(slack)) {
+          const double product = fabs(d) * slack;
+          q[4] = dmax(q[4], product);
+          q[3] = dmax(q[3], product / (scale * xs));
+        }
+      }
+    }
+  }
+}
+
 // Final report (pdhg.cpp:647-661): residuals of the best point, its unscaled value, reduced
 // costs and multipliers. Writes the residual block to ctrl->best.
 template <class T>
@@ -1480,6 +1610,23 @@ __global__ void __launch_bounds__(kThreads, 2) report_kernel(Prob<T> P, State<T>
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     S.ctrl->best = make_residuals(t, 0, S.ctrl->bound_norm, S.ctrl->cost_norm);
     S.ctrl->primal_violation = dmax(0.0, dmax(t[1], t[9]));
+  }
+  // quality of the reported point, read back after the barrier above
+  double qv[kQualitySlots];
+#pragma unroll
+  for (int k = 0; k < kQualitySlots; ++k) qv[k] = 0.0;
+  quality_pass(P, S.best_x, S.best_y, x_out, y_out, reduced_out,
+               (int)((blockIdx.x * kThreads + threadIdx.x) >> 5), (int)(gridDim.x * kWarps), qv);
+  block_reduce<kQualitySlots, 0xFFu>(qv, sh);
+  write_partials(S.partials, 2 + kEvalSlots, qv, kQualitySlots);
+  if (!grid_barrier(S.bar)) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) S.ctrl->state = kDeviceError;
+    return;
+  }
+  reduce_partials<kQualitySlots, 0xFFu>(S.partials, 2 + kEvalSlots, qv, sh);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < kQualitySlots; ++k) S.ctrl->quality[k] = qv[k];
   }
 }
 

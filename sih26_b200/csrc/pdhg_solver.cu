@@ -163,6 +163,7 @@ template <class T>
 struct Level {
   Prob<T> P;
   State<T> S;
+  bool halpern = false;  // which iteration kernel runs the loop
 };
 
 struct Common {
@@ -269,7 +270,8 @@ static Level<T> make_level(Arena& a, const Common& cm, const PermutedLp& q,
 // on an SM (the minimum over the kernels, which share one work partition).
 template <class T>
 static int blocks_per_sm() {
-  const void* k1[] = {reinterpret_cast<const void*>(iterate_kernel<T>),
+  const void* k1[] = {reinterpret_cast<const void*>(iterate_kernel<T, false>),
+                      reinterpret_cast<const void*>(iterate_kernel<T, true>),
                       reinterpret_cast<const void*>(init_ax_kernel<T>),
                       reinterpret_cast<const void*>(anchor_kernel<T>),
                       reinterpret_cast<const void*>(report_kernel<T>),
@@ -371,7 +373,9 @@ static Ctrl run_loop(Level<T>& L, int G, cudaStream_t stream, Ctrl* host_ctrl, i
     for (int k = 0; k < pairs; ++k) {
       void* ia[] = {&L.P, &L.S, &max_attempts};
       if (timer.on) SIH26_CUDA(cudaEventRecord(timer.start[k], stream), SANKHYA_GPU_INIT_FAILED);
-      launch_coop(reinterpret_cast<const void*>(iterate_kernel<T>), G, ia, stream_smem_bytes(), stream);
+      launch_coop(L.halpern ? reinterpret_cast<const void*>(iterate_kernel<T, true>)
+                            : reinterpret_cast<const void*>(iterate_kernel<T, false>),
+                  G, ia, stream_smem_bytes(), stream);
       if (timer.on) SIH26_CUDA(cudaEventRecord(timer.stop[k], stream), SANKHYA_GPU_INIT_FAILED);
       void* ea[] = {&L.P, &L.S};
       launch_coop(reinterpret_cast<const void*>(evaluate_kernel<T>), G, ea, stream_smem_bytes(), stream);
@@ -934,6 +938,7 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
     c0.halpern = 1;
     c0.eta = 0.998 / std::max(spectral_norm, 1e-12);  // constant: tau sigma ||A||^2 < 1
   }
+  L64.halpern = L32.halpern = halpern;
 
   // the time limit counts from the start of the call, like the reference's Timer
   mark("norm estimate and A x0");
@@ -1151,6 +1156,8 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
   res->kernel_launches = g_launches;
   res->autotuned = autotuned;
   res->primal_infeasibility = rep.primal_violation;
+  res->quality = quality_from_slots(rep.quality, res->objective, res->dual_bound);
+  res->quality.primal_infeasibility = res->primal_infeasibility;  // one figure for both fields
   res->schedule[0] = sched_a.stream_row_max;
   res->schedule[1] = sched_a.nnz_per_lane;
   res->schedule[2] = sched_at.stream_row_max;

@@ -632,6 +632,8 @@ int qp_solve_impl(const sankhya_pdhg_problem& prob, const sankhya_qp_hessian& he
       if (host_finite_bound(prob.row_upper[i])) worst = std::max(worst, act[i] - prob.row_upper[i]);
     }
     res->primal_infeasibility = worst;
+    // the dual measures are the LP engines' (the QP's gradient is c + Qx): not measured here
+    res->quality = sankhya_pdhg_quality{worst, NAN, NAN, NAN, NAN, NAN, NAN};
   }
   if (host.state == kConverged) {
     res->status = SANKHYA_PDHG_OPTIMAL;

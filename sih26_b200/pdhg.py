@@ -83,6 +83,13 @@ class _Residuals(C.Structure):
         "complementarity")]
 
 
+class _Quality(C.Structure):
+    _fields_ = [(k, C.c_double) for k in (
+        "primal_infeasibility", "primal_infeasibility_scaled", "dual_infeasibility",
+        "dual_infeasibility_scaled", "complementarity_violation", "absolute_gap",
+        "relative_gap")]
+
+
 class _Result(C.Structure):
     _fields_ = [("col_value", _f64p), ("row_dual", _f64p), ("col_dual", _f64p),
                 ("farkas_dual", _f64p), ("primal_ray", _f64p), ("status", C.c_int32),
@@ -96,7 +103,7 @@ class _Result(C.Structure):
                 ("iterate_launches", C.c_int64), ("kernel_launches", C.c_int64),
                 ("residuals", _Residuals), ("autotuned", C.c_int32),
                 ("schedule", C.c_int32 * 4), ("primal_infeasibility", C.c_double),
-                ("message", C.c_char * 512)]
+                ("quality", _Quality), ("message", C.c_char * 512)]
 
 
 # Every symbol include/sankhya_pdhg_gpu.h declares.
@@ -211,6 +218,10 @@ class Solution:
     algorithm: str
     message: str
     primal_infeasibility: float = 0.0
+    # Solution::recompute_quality's figures of the reported point, measured on the device:
+    # primal_infeasibility(_scaled), dual_infeasibility(_scaled), complementarity_violation,
+    # absolute_gap, relative_gap (src/core/model.cpp:228-424)
+    quality: Optional[dict] = None
     farkas_dual: Optional[np.ndarray] = None
     primal_ray: Optional[np.ndarray] = None
     # engine detail
@@ -303,7 +314,12 @@ def solve_pdhg(model: LP, options: Optional[Options] = None) -> Solution:
         schedule=tuple(res.schedule))
     if status not in ("model_error", "infeasible", "unbounded"):
         sol.primal_infeasibility = res.primal_infeasibility  # computed on the device
+        sol.quality = _quality(res)
     return sol
+
+
+def _quality(res) -> dict:
+    return {k: getattr(res.quality, k) for k, _ in _Quality._fields_}
 
 
 # ---- convex QP (sankhya_qp_gpu_solve) --------------------------------------------------------
@@ -497,6 +513,7 @@ class _Outputs:
             kernel_launches=res.kernel_launches)
         if status not in ("model_error", "infeasible", "unbounded"):
             sol.primal_infeasibility = res.primal_infeasibility  # computed on the device
+            sol.quality = _quality(res)
         return sol
 
 
