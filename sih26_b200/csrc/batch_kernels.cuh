@@ -284,6 +284,61 @@ __device__ __noinline__ void group_report(const BatchSlot& B, Ctrl& c, double* s
   __syncthreads();
 }
 
+// One attempt of each operator, out of line: each step gets the registers of its own
+// epilogues instead of sharing one allocation with the other operator's.
+template <class Grp>
+__device__ __noinline__ void group_halpern_step(const BatchSlot& B, Ctrl& c, double* stream,
+                                                Grp grp) {
+  const Prob<double>& P = B.P;
+  const State<double>& S = B.S;
+  const int rank = grp.rank();
+  const int cur = c.cur, nxt = cur ^ 1;
+  const double tau = c.eta / c.omega;
+  const double sigma = c.eta * c.omega;
+  double acc[3] = {0.0, 0.0, 0.0};
+  // the Halpern operator (see PrimalStepHalpern in pdhg_kernels.cuh)
+  const double w = (double)(c.averaged + 1) / (double)(c.averaged + 2);
+  run_phase<1, 3>(P.AT.ptr, P.AT.idx, P.AT.val, P.pat, Gather1<double>{S.y[cur]},
+                  PrimalStepHalpern<double>{S.x[cur], S.x[nxt], S.xt, P.c, P.cl, P.cu, S.xr,
+                                            tau, w},
+                  acc, stream, rank);
+  grp.sync();
+  run_phase<1, 3>(P.A.ptr, P.A.idx, P.A.val, P.pa, Gather1<double>{S.x[nxt]},
+                  DualStepHalpern<double>{S.y[cur], S.y[nxt], S.yt, S.ax[nxt], P.rl, P.ru,
+                                          S.yr, S.axr, sigma, w},
+                  acc, stream, rank);
+  grp.sync();
+  if (threadIdx.x == 0) halpern_control(c);
+  __syncthreads();
+}
+
+template <class Grp>
+__device__ __noinline__ void group_reference_step(const BatchSlot& B, Ctrl& c, double* sh,
+                                                  double* stream, Grp grp) {
+  const Prob<double>& P = B.P;
+  const State<double>& S = B.S;
+  const int rank = grp.rank();
+  const int cur = c.cur, nxt = cur ^ 1;
+  const double tau = c.eta / c.omega;
+  const double sigma = c.eta * c.omega;
+  double acc[3] = {0.0, 0.0, 0.0};
+  {
+    PrimalStep<double> ps{S.x[cur], S.x[nxt], P.c, P.cl, P.cu, S.xsum, tau, c.pending};
+    run_phase<1, 3>(P.AT.ptr, P.AT.idx, P.AT.val, P.pat, Gather1<double>{S.y[cur]}, ps, acc,
+                    stream, rank);
+  }
+  grp.sync();
+  {
+    DualStep<double> ds{S.y[cur], S.y[nxt], S.ax[cur], S.ax[nxt], P.rl, P.ru, S.ysum, sigma,
+                        c.pending};
+    run_phase<1, 3>(P.A.ptr, P.A.idx, P.A.val, P.pa, Gather1<double>{S.x[nxt]}, ds, acc,
+                    stream, rank);
+  }
+  grp.template reduce<3, 0u>(acc, sh);
+  if (threadIdx.x == 0) step_control(c, acc);
+  __syncthreads();
+}
+
 template <class Grp>
 __device__ inline void run_instance(const BatchSlot& B, Ctrl& c, double* sh, double* stream,
                                     int* flags, long long chunk_attempts, Grp grp) {
@@ -342,43 +397,8 @@ __device__ inline void run_instance(const BatchSlot& B, Ctrl& c, double* sh, dou
     __syncthreads();
     if (c.state != kRunning || flags[5]) break;
     ++a;
-    const int cur = c.cur, nxt = cur ^ 1;
-    const double tau = c.eta / c.omega;
-    const double sigma = c.eta * c.omega;
-    double acc[3] = {0.0, 0.0, 0.0};
-    if (c.halpern) {
-      // the Halpern operator (see PrimalStepHalpern in pdhg_kernels.cuh)
-      const double w = (double)(c.averaged + 1) / (double)(c.averaged + 2);
-      run_phase<1, 3>(P.AT.ptr, P.AT.idx, P.AT.val, P.pat, Gather1<double>{S.y[cur]},
-                      PrimalStepHalpern<double>{S.x[cur], S.x[nxt], S.xt, P.c, P.cl, P.cu, S.xr,
-                                                tau, w},
-                      acc, stream, rank);
-      grp.sync();
-      run_phase<1, 3>(P.A.ptr, P.A.idx, P.A.val, P.pa, Gather1<double>{S.x[nxt]},
-                      DualStepHalpern<double>{S.y[cur], S.y[nxt], S.yt, S.ax[nxt], P.rl, P.ru,
-                                              S.yr, S.axr, sigma, w},
-                      acc, stream, rank);
-      grp.sync();
-      if (threadIdx.x == 0) halpern_control(c);
-      __syncthreads();
-      if (c.state == kNeedEval) group_evaluate(B, c, sh, stream, flags, grp);
-      continue;
-    }
-    {
-      PrimalStep<double> ps{S.x[cur], S.x[nxt], P.c, P.cl, P.cu, S.xsum, tau, c.pending};
-      run_phase<1, 3>(P.AT.ptr, P.AT.idx, P.AT.val, P.pat, Gather1<double>{S.y[cur]}, ps, acc,
-                      stream, rank);
-    }
-    grp.sync();
-    {
-      DualStep<double> ds{S.y[cur], S.y[nxt], S.ax[cur], S.ax[nxt], P.rl, P.ru, S.ysum, sigma,
-                          c.pending};
-      run_phase<1, 3>(P.A.ptr, P.A.idx, P.A.val, P.pa, Gather1<double>{S.x[nxt]}, ds, acc,
-                      stream, rank);
-    }
-    grp.template reduce<3, 0u>(acc, sh);
-    if (threadIdx.x == 0) step_control(c, acc);
-    __syncthreads();
+    if (c.halpern) group_halpern_step(B, c, stream, grp);
+    else group_reference_step(B, c, sh, stream, grp);
     if (c.state == kNeedEval) group_evaluate(B, c, sh, stream, flags, grp);
   }
   if (c.state == kConverged || c.state == kIterationLimit || c.state == kTimeLimit ||
