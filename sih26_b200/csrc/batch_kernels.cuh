@@ -284,10 +284,10 @@ __device__ __noinline__ void group_report(const BatchSlot& B, Ctrl& c, double* s
   __syncthreads();
 }
 
-// One attempt of each operator, out of line: each step gets the registers of its own
-// epilogues instead of sharing one allocation with the other operator's.
+// One attempt of each operator. Inlined: a call per attempt (and the spills of the callee's
+// saved registers) cost more than the shared register allocation of the inlined loop.
 template <class Grp>
-__device__ __noinline__ void group_halpern_step(const BatchSlot& B, Ctrl& c, double* stream,
+__device__ __forceinline__ void group_halpern_step(const BatchSlot& B, Ctrl& c, double* stream,
                                                 Grp grp) {
   const Prob<double>& P = B.P;
   const State<double>& S = B.S;
@@ -313,7 +313,7 @@ __device__ __noinline__ void group_halpern_step(const BatchSlot& B, Ctrl& c, dou
 }
 
 template <class Grp>
-__device__ __noinline__ void group_reference_step(const BatchSlot& B, Ctrl& c, double* sh,
+__device__ __forceinline__ void group_reference_step(const BatchSlot& B, Ctrl& c, double* sh,
                                                   double* stream, Grp grp) {
   const Prob<double>& P = B.P;
   const State<double>& S = B.S;
