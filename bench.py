@@ -172,6 +172,59 @@ def cpu_reference_sample(lp, iterations):
     return kind, threads, setup, per_iteration
 
 
+CPU_BATCH_CAP = 20000       # iterations charged to an LP the CPU reference cannot certify
+CPU_BATCH_PROBE = 200       # iterations timed per LP of the CPU batch sample
+
+
+def _cpu_worker_init():
+    os.environ["OMP_NUM_THREADS"] = "1"
+
+
+def _cpu_ref_one(args):
+    """Setup time and time per iteration of the reference solve_pdhg on one LP (one thread)."""
+    import oracle
+
+    lp, probe = args
+    t0 = time.perf_counter()
+    oracle.ref_solve(lp, tolerance=TOLERANCE, iteration_limit=0, stop_at_request=True)
+    setup = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    oracle.ref_solve(lp, tolerance=TOLERANCE, iteration_limit=probe, stop_at_request=True)
+    per_it = max(time.perf_counter() - t0 - setup, 1e-9) / probe
+    return setup, per_it
+
+
+def cpu_batch_sample(lps, iterations):
+    """The reference solve_pdhg on a sample of the batch, one LP per host core (processes
+    started with spawn, OMP_NUM_THREADS=1 each). Each LP is timed for its setup and
+    CPU_BATCH_PROBE iterations and charged `iterations[k]` (the reference operator's count on
+    the GPU; CPU_BATCH_CAP for an LP the CPU reference cannot certify); the LPs are packed onto
+    the cores largest first, and the rate is the sample over that makespan."""
+    import multiprocessing as mp
+
+    import oracle
+
+    if not oracle.ref_available():
+        return None
+    cores = os.cpu_count() or 1
+    with mp.get_context("spawn").Pool(cores, initializer=_cpu_worker_init) as pool:
+        timed = pool.map(_cpu_ref_one, [(lp, CPU_BATCH_PROBE) for lp in lps], chunksize=1)
+    cost = sorted((setup + per_it * its for (setup, per_it), its in zip(timed, iterations)),
+                  reverse=True)
+    load = [0.0] * cores
+    for c in cost:
+        load[load.index(min(load))] += c
+    makespan = max(load)
+    return {"value": len(lps) / makespan, "unit": "LPs/s", "cores": cores, "kind": "reference",
+            "seconds": makespan, "cpu_seconds": sum(cost),
+            "sample": f"every 8th LP ({len(lps)}), reference solve_pdhg (pdhg_tolerance "
+                      f"{TOLERANCE:g}, pdhg_stop_at_request), one process per core "
+                      f"(OMP_NUM_THREADS=1): setup + {CPU_BATCH_PROBE} iterations timed per LP, "
+                      f"extrapolated to the iterations the reference operator needed on the GPU "
+                      f"(an infeasible LP, which the CPU reference cannot certify, at "
+                      f"{CPU_BATCH_CAP}), packed onto the cores largest first"}
+
+
 def _percentiles(values):
     import numpy as np
 
@@ -229,9 +282,17 @@ def batched_leg(local, world, rank, dist, torch, algorithm="halpern"):
     # the reference operator on the same batch, for comparison
     other = "reference" if algorithm == "halpern" else "halpern"
     t0 = time.perf_counter()
-    pdhg.batch_solve(lps, pdhg.Options(pdhg_tolerance=TOLERANCE, pdhg_stop_rule="relative_kkt",
-                                       gpu_device=local, pdhg_algorithm=other))
+    osols = pdhg.batch_solve(lps, pdhg.Options(pdhg_tolerance=TOLERANCE,
+                                               pdhg_stop_rule="relative_kkt",
+                                               gpu_device=local, pdhg_algorithm=other))
     other_rate = len(lps) / (time.perf_counter() - t0)
+    # the reference operator's iteration counts: this batch's when it ran the reference
+    # operator, else the comparison batch's
+    ref_its = ([osols[k].iterations for k in sample] if other == "reference"
+               else [allres[k][3] for k in sample])
+    ref_its = [CPU_BATCH_CAP if lps[k].farkas_star is not None else its
+               for k, its in zip(sample, ref_its)]
+    cpu_batch = cpu_batch_sample([lps[k] for k in sample], ref_its)
     rate = len(lps) / wall
     return {
         "workload": "512 uneven LPs, m log-uniform [50, 5000], n = m U(1.5,3), 5-15 nnz/col, "
@@ -246,6 +307,7 @@ def batched_leg(local, world, rank, dist, torch, algorithm="halpern"):
         "one_at_a_time_fp64": {"value": one_rate, "unit": "LPs/s", "algorithm": algorithm,
                                "sample": f"every 8th LP ({len(sample)}), once each"},
         "speedup_vs_one_at_a_time": rate / one_rate,
+        "cpu_reference": cpu_batch,
         "sharding": f"{world} rank(s), by nonzeros" if world > 1 else "single GPU",
     }
 
