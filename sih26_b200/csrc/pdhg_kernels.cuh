@@ -223,7 +223,12 @@ __device__ __forceinline__ double ro(const T* p) {
 //   epi.apply(r, s, in, acc);
 // `stream` is this warp's kItemNnz doubles of dynamic shared memory; a stream item with
 // NV > 1 gathered vectors passes over it once per vector.
-template <int NV, int NS, class V, class Gather, class Epi>
+//
+// kShared: the block's warps take its short-row items from a shared-memory counter as they
+// finish the last one, instead of every 16th item each, so no warp idles while another still
+// has two items to go. For phases that reduce nothing across rows: a row's sum is the same
+// whichever warp takes it, but a per-thread accumulator would group its terms differently.
+template <int NV, int NS, bool kShared = false, class V, class Gather, class Epi>
 __device__ __forceinline__ void run_phase(const int* __restrict__ ptr, const int* __restrict__ idx,
                                           const V* __restrict__ val, const Part& p,
                                           const Gather& g, const Epi& epi, double (&acc)[NS],
@@ -254,11 +259,23 @@ __device__ __forceinline__ void run_phase(const int* __restrict__ ptr, const int
   }
   // 2. short rows; each item first pulls the warp's next item towards L2
   const int ib = __ldg(p.blk_item_begin + b), ie = __ldg(p.blk_item_begin + b + 1);
+  __shared__ int next_item;  // kShared: the block's next unclaimed item
+  if constexpr (kShared) {
+    if (threadIdx.x == 0) next_item = ib + kWarps;  // the first kWarps go one to each warp
+    __syncthreads();
+  }
   int4 item = ib + warp < ie ? __ldg(p.items + ib + warp) : make_int4(0, 0, 0, 0);
-  for (int it = ib + warp; it < ie; it += kWarps) {
+  for (int it = ib + warp; it < ie;) {
     int4 next = make_int4(0, 0, 0, 0);
-    if (it + kWarps < ie) {
-      next = __ldg(p.items + it + kWarps);
+    int nit;
+    if constexpr (kShared) {
+      nit = lane == 0 ? atomicAdd(&next_item, 1) : 0;
+      nit = __shfl_sync(0xffffffffu, nit, 0);
+    } else {
+      nit = it + kWarps;
+    }
+    if (nit < ie) {
+      next = __ldg(p.items + nit);
       prefetch_range(idx, val, __ldg(ptr + next.x), __ldg(ptr + next.y), lane);
     }
     if (item.z == 0) {
@@ -314,6 +331,7 @@ __device__ __forceinline__ void run_phase(const int* __restrict__ ptr, const int
       if (valid && gl == 0) epi.apply(r, s, in, acc);
     }
     item = next;
+    it = nit;
   }
   // 3. long rows: sum the block's segment partials in segment order, then the epilogue
   const int lb = __ldg(p.blk_long_begin + b), le = __ldg(p.blk_long_begin + b + 1);
@@ -945,10 +963,10 @@ __global__ void __launch_bounds__(kThreads, 2) iterate_kernel(Prob<T> P, State<T
       const double w = (double)(c.averaged + 1) / (double)(c.averaged + 2);
       if constexpr (kDelta<T>) {
         PrimalStepHalpernDelta<T> ps{S.x[cur], S.x[nxt], S.xt, S.cg, S.dl, S.du, tau, w};
-        run_phase<1, 3>(P.AT.ptr, P.AT.idx, P.AT.val, P.pat, Gather1<T>{S.y[cur]}, ps, acc, stream);
+        run_phase<1, 3, true>(P.AT.ptr, P.AT.idx, P.AT.val, P.pat, Gather1<T>{S.y[cur]}, ps, acc, stream);
       } else {
         PrimalStepHalpern<T> ps{S.x[cur], S.x[nxt], S.xt, P.c, P.cl, P.cu, S.xr, tau, w};
-        run_phase<1, 3>(P.AT.ptr, P.AT.idx, P.AT.val, P.pat, Gather1<T>{S.y[cur]}, ps, acc, stream);
+        run_phase<1, 3, true>(P.AT.ptr, P.AT.idx, P.AT.val, P.pat, Gather1<T>{S.y[cur]}, ps, acc, stream);
       }
       SIH26_MARK(0);
       if (!grid_barrier(S.bar)) goto device_error;
@@ -956,10 +974,10 @@ __global__ void __launch_bounds__(kThreads, 2) iterate_kernel(Prob<T> P, State<T
       if constexpr (kDelta<T>) {
         DualStepHalpernDelta<T> ds{S.y[cur], S.y[nxt], S.yt, S.ax[nxt], S.yr, S.axr, P.rl64,
                                    P.ru64, sigma, w};
-        run_phase<1, 3>(P.A.ptr, P.A.idx, P.A.val, P.pa, Gather1<T>{S.x[nxt]}, ds, acc, stream);
+        run_phase<1, 3, true>(P.A.ptr, P.A.idx, P.A.val, P.pa, Gather1<T>{S.x[nxt]}, ds, acc, stream);
       } else {
         DualStepHalpern<T> ds{S.y[cur], S.y[nxt], S.yt, S.ax[nxt], P.rl, P.ru, S.yr, S.axr, sigma, w};
-        run_phase<1, 3>(P.A.ptr, P.A.idx, P.A.val, P.pa, Gather1<T>{S.x[nxt]}, ds, acc, stream);
+        run_phase<1, 3, true>(P.A.ptr, P.A.idx, P.A.val, P.pa, Gather1<T>{S.x[nxt]}, ds, acc, stream);
       }
       SIH26_MARK(2);
       if (!grid_barrier(S.bar)) goto device_error;
