@@ -20,6 +20,12 @@
 //     information (pdhg.cpp:502-503): unscaled FP64 residuals of the current iterate and of
 //     the running average (pdhg.cpp:143-263), candidate choice, best point, stopping test
 //     and restart with the primal-weight update (pdhg.cpp:505-643).
+//   report_kernel: the best point in original units, its residuals and its quality block
+//     (Solution::recompute_quality, src/core/model.cpp:228-424).
+//
+// The iteration kernel has one instance per operator: the reference's adaptive step above,
+// and the reflected Halpern step (PrimalStepHalpern below: a constant step, no acceptance
+// test, the second candidate is the PDHG output T(z) instead of the average).
 //
 // Two precision levels share this code: FP64 (iterates, matrix and reductions in FP64) and
 // the FP32 level of the mixed mode (FP32 matrix and FP32 iterate deltas about an FP64 restart
@@ -28,7 +34,8 @@
 // Internal index spaces are permuted: rows of A sorted by nonzero count (descending) and
 // columns likewise, so a work item holds rows of similar length; the host un-permutes
 // outputs. Reductions use fixed trees over a fixed work partition, so a run is bit-for-bit
-// repeatable.
+// repeatable; the Halpern phases, which reduce nothing, let a block's warps share its items
+// at run time (each row is still summed by one warp in a fixed order).
 #pragma once
 
 #include <cstdint>
