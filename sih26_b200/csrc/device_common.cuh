@@ -82,7 +82,6 @@ __device__ __forceinline__ void block_reduce(double (&v)[NS], double* shared) {
 // its own wait sees the error word.
 struct GridBarrier {
   unsigned* count;                  // the barrier word; zero before the first barrier
-  unsigned* generation;             // unused (kept for the layout of the control words)
   int* error;
   unsigned long long limit_ns;
   int* time_up;                     // set by the last arriver: global time > deadline_ns
@@ -98,9 +97,6 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
   unsigned v;
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
-}
-__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
-  asm volatile("st.release.gpu.global.u32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
 }
 __device__ __forceinline__ void st_relaxed(unsigned* p, unsigned v) {
   asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" :: "l"(p), "r"(v) : "memory");

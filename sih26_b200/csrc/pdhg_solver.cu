@@ -859,7 +859,7 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
   cm.ctrl = a.zeros<Ctrl>(1);
   unsigned* bar_words = a.zeros<unsigned>(2);
   int* flags = a.zeros<int>(2);
-  cm.bar = GridBarrier{bar_words, bar_words + 1, flags, 4000000000ull, flags + 1, 0ull};
+  cm.bar = GridBarrier{bar_words, flags, 4000000000ull, flags + 1, 0ull};
   a.put(cm.best_x, x0.data(), n * sizeof(double), stream);
   SIH26_CUDA(cudaDeviceSynchronize(), SANKHYA_GPU_SYNC_FAILED);
 

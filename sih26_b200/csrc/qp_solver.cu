@@ -542,7 +542,7 @@ int qp_solve_impl(const sankhya_pdhg_problem& prob, const sankhya_qp_hessian& he
   std::vector<int> fl(2, 0);
   unsigned* bar_words = dev_upload(owned, bw);
   int* flags = dev_upload(owned, fl);
-  Q.bar = GridBarrier{bar_words, bar_words + 1, flags, 4000000000ull, flags + 1, 0ull};
+  Q.bar = GridBarrier{bar_words, flags, 4000000000ull, flags + 1, 0ull};
   Q.tau = tau;
   Q.sigma = sigma;
   Q.tolerance = tolerance;
