@@ -194,7 +194,7 @@ def _cpu_ref_one(args):
     return setup, per_it
 
 
-def cpu_batch_sample(lps, iterations):
+def cpu_batch_sample(lps, iterations, what="every 8th LP"):
     """The reference solve_pdhg on a sample of the batch, one LP per host core (processes
     started with spawn, OMP_NUM_THREADS=1 each). Each LP is timed for its setup and
     CPU_BATCH_PROBE iterations and charged `iterations[k]` (the reference operator's count on
@@ -217,7 +217,7 @@ def cpu_batch_sample(lps, iterations):
     makespan = max(load)
     return {"value": len(lps) / makespan, "unit": "LPs/s", "cores": cores, "kind": "reference",
             "seconds": makespan, "cpu_seconds": sum(cost),
-            "sample": f"every 8th LP ({len(lps)}), reference solve_pdhg (pdhg_tolerance "
+            "sample": f"{what} ({len(lps)}), reference solve_pdhg (pdhg_tolerance "
                       f"{TOLERANCE:g}, pdhg_stop_at_request), one process per core "
                       f"(OMP_NUM_THREADS=1): setup + {CPU_BATCH_PROBE} iterations timed per LP, "
                       f"extrapolated to the iterations the reference operator needed on the GPU "
@@ -355,6 +355,13 @@ def served_leg(local, rates, seconds, chunk, algorithm="halpern", pool_size=24, 
     base_rate = one_at_a_time(pool, local, algorithm)
     opts = pdhg.Options(pdhg_tolerance=TOLERANCE, pdhg_stop_rule="relative_kkt",
                         gpu_device=local, pdhg_algorithm=algorithm)
+    # the CPU reference on the pool, one LP per host core, charged the iterations the
+    # reference operator needs (counted on the GPU)
+    ref_sols = pdhg.batch_solve(pool, pdhg.Options(pdhg_tolerance=TOLERANCE,
+                                                   pdhg_stop_rule="relative_kkt",
+                                                   gpu_device=local,
+                                                   pdhg_algorithm="reference"))
+    cpu_pool = cpu_batch_sample(pool, [s.iterations for s in ref_sols], "the pool's LPs")
     out = []
     for rate in rates:
         rng = np.random.default_rng(seed + 1)
@@ -408,6 +415,7 @@ def served_leg(local, rates, seconds, chunk, algorithm="halpern", pool_size=24, 
             "one_at_a_time_fp64": {"value": base_rate, "unit": "LPs/s",
                                    "sample": f"the {pool_size} LPs of the pool, once each"},
             "speedup_vs_one_at_a_time": (served_rate / base_rate) if served_rate else None,
+            "cpu_reference": cpu_pool,
         })
     return out
 
