@@ -299,14 +299,14 @@ __device__ __forceinline__ void group_halpern_step(const BatchSlot& B, Ctrl& c, 
   // the Halpern operator (see PrimalStepHalpern in pdhg_kernels.cuh)
   const double w = (double)(c.averaged + 1) / (double)(c.averaged + 2);
   run_phase<1, 3>(P.AT.ptr, P.AT.idx, P.AT.val, P.pat, Gather1<double>{S.y[cur]},
-                        PrimalStepHalpern<double>{S.x[cur], S.x[nxt], S.xt, P.c, P.cl, P.cu,
-                                                  S.xr, tau, w},
-                        acc, stream, rank);
+                  PrimalStepHalpern<double>{S.x[cur], S.x[nxt], S.xt, P.c, P.cl, P.cu, S.xr,
+                                            tau, w},
+                  acc, stream, rank);
   grp.sync();
   run_phase<1, 3>(P.A.ptr, P.A.idx, P.A.val, P.pa, Gather1<double>{S.x[nxt]},
-                        DualStepHalpern<double>{S.y[cur], S.y[nxt], S.yt, S.ax[nxt], P.rl,
-                                                P.ru, S.yr, S.axr, sigma, w},
-                        acc, stream, rank);
+                  DualStepHalpern<double>{S.y[cur], S.y[nxt], S.yt, S.ax[nxt], P.rl, P.ru,
+                                          S.yr, S.axr, sigma, w},
+                  acc, stream, rank);
   grp.sync();
   if (threadIdx.x == 0) halpern_control(c);
   __syncthreads();
