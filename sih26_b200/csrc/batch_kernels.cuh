@@ -288,7 +288,7 @@ __device__ __noinline__ void group_report(const BatchSlot& B, Ctrl& c, double* s
 // saved registers) cost more than the shared register allocation of the inlined loop.
 template <class Grp>
 __device__ __forceinline__ void group_halpern_step(const BatchSlot& B, Ctrl& c, double* stream,
-                                                Grp grp) {
+                                                   Grp grp) {
   const Prob<double>& P = B.P;
   const State<double>& S = B.S;
   const int rank = grp.rank();
@@ -314,7 +314,7 @@ __device__ __forceinline__ void group_halpern_step(const BatchSlot& B, Ctrl& c, 
 
 template <class Grp>
 __device__ __forceinline__ void group_reference_step(const BatchSlot& B, Ctrl& c, double* sh,
-                                                  double* stream, Grp grp) {
+                                                     double* stream, Grp grp) {
   const Prob<double>& P = B.P;
   const State<double>& S = B.S;
   const int rank = grp.rank();
