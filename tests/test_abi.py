@@ -105,3 +105,38 @@ def test_no_cpu_fallback_without_a_gpu(lib):
     with pytest.raises(P.GpuError) as e:
         P.solve_pdhg(_tiny())
     assert e.value.code == 2
+
+
+@pytest.mark.skipif(not any(os.access(os.path.join(d, "gcc"), os.X_OK)
+                            for d in os.environ.get("PATH", "").split(os.pathsep)),
+                    reason="no C compiler")
+def test_python_mirrors_match_the_header_layout(tmp_path):
+    """Every ctypes mirror in sih26_b200/pdhg.py has the size and field offsets the C compiler
+    gives the header's struct (a field added to one side only would shift the others)."""
+    import subprocess
+
+    pairs = [("sankhya_pdhg_problem", P._Problem), ("sankhya_pdhg_params", P._Params),
+             ("sankhya_pdhg_residuals", P._Residuals), ("sankhya_pdhg_quality", P._Quality),
+             ("sankhya_pdhg_result", P._Result), ("sankhya_pdhg_server_config", P._ServerConfig),
+             ("sankhya_qp_hessian", P._Hessian)]
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "sankhya_pdhg_gpu.h"',
+             "int main(void) {"]
+    for cname, py in pairs:
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for field, _ in py._fields_:
+            lines.append(f'  printf("{cname} {field} %zu\\n", offsetof({cname}, {field}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)],
+                   check=True, capture_output=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout
+    got = {}
+    for line in out.splitlines():
+        cname, key, val = line.split()
+        got[(cname, key)] = int(val)
+    for cname, py in pairs:
+        assert got[(cname, "size")] == C.sizeof(py), cname
+        for field, _ in py._fields_:
+            assert got[(cname, field)] == getattr(py, field).offset, (cname, field)
