@@ -18,6 +18,7 @@ import oracle
 from sih26_b200 import lpgen
 from sih26_b200 import pdhg as P
 from tests.cases import generated_cases, hand_cases
+from tests.test_quality_oracle import edge_lps
 
 pytestmark = pytest.mark.gpu
 
@@ -51,6 +52,7 @@ def _check(lp, s):
 
 def _lps():
     out = [lp for _, lp, _ in hand_cases()] + [lp for _, lp in generated_cases()]
+    out += [lp for _, lp in edge_lps()]
     out.append(lpgen.block_angular_planted(blocks=3, block_rows=40, block_cols=100,
                                            nnz_per_col=4, linking_rows=6, seed=4))
     mx = lpgen.uniform_planted(60, 150, 4, seed=9)

@@ -19,8 +19,22 @@ needs_ref = pytest.mark.skipif(not oracle.ref_available(),
                                reason="reference build (oracle/_ref) not present")
 
 
+def edge_lps():
+    """Every bound kind at once: a free column, a fixed one, a boxed one; >=, <=, range and
+    equality rows; both senses, with an objective offset."""
+    inf = math.inf
+    rows = [[1, 1, 1, 0], [1, 0, -1, 0], [0, 1, 1, 0], [0, 1, 0, -1]]
+    kw = dict(col_lower=[0, -inf, 1, -inf], col_upper=[5, inf, 1, inf])
+    return [("edge_min", lpgen.from_dense(rows, [1, -inf, 0, 0], [inf, 2, 3, 0], [1, 2, -1, 0],
+                                          name="edge_min", **kw)),
+            ("edge_max", lpgen.from_dense(rows, [1, -inf, 0, 0], [inf, 2, 3, 0], [-1, -2, 1, 0],
+                                          maximize=True, objective_offset=3.5, name="edge_max",
+                                          **kw))]
+
+
 def _lps():
     out = [(name, lp) for name, lp, _ in hand_cases()]
+    out += edge_lps()
     out += generated_cases()
     out.append(("block_angular", lpgen.block_angular_planted(blocks=3, block_rows=40,
                                                              block_cols=100, nnz_per_col=4,
