@@ -181,17 +181,26 @@ def _cpu_worker_init():
 
 
 def _cpu_ref_one(args):
-    """Setup time and time per iteration of the reference solve_pdhg on one LP (one thread)."""
+    """Setup time and time per iteration of the reference solve_pdhg on one LP (one thread):
+    the setup is the faster of two runs without iterations; the iterations are timed over at
+    least `probe` of them and at least 10 ms (fewer if the LP converges first)."""
     import oracle
 
     lp, probe = args
-    t0 = time.perf_counter()
-    oracle.ref_solve(lp, tolerance=TOLERANCE, iteration_limit=0, stop_at_request=True)
-    setup = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    oracle.ref_solve(lp, tolerance=TOLERANCE, iteration_limit=probe, stop_at_request=True)
-    per_it = max(time.perf_counter() - t0 - setup, 1e-9) / probe
-    return setup, per_it
+
+    def run(limit):
+        t0 = time.perf_counter()
+        r = oracle.ref_solve(lp, tolerance=TOLERANCE, iteration_limit=limit, stop_at_request=True)
+        return time.perf_counter() - t0, r.iterations
+
+    setup = min(run(0)[0] for _ in range(2))
+    k = probe
+    while True:
+        t, its = run(k)
+        if t - setup >= 0.01 or its < k or k >= 100 * probe:
+            break
+        k *= 4
+    return setup, max(t - setup, 1e-9) / max(1, its)
 
 
 def cpu_batch_sample(lps, iterations, what="every 8th LP"):
@@ -219,7 +228,8 @@ def cpu_batch_sample(lps, iterations, what="every 8th LP"):
             "seconds": makespan, "cpu_seconds": sum(cost),
             "sample": f"{what} ({len(lps)}), reference solve_pdhg (pdhg_tolerance "
                       f"{TOLERANCE:g}, pdhg_stop_at_request), one process per core "
-                      f"(OMP_NUM_THREADS=1): setup + {CPU_BATCH_PROBE} iterations timed per LP, "
+                      f"(OMP_NUM_THREADS=1): setup and at least {CPU_BATCH_PROBE} iterations (and 10 ms) "
+                      f"timed per LP, "
                       f"extrapolated to the iterations the reference operator needed on the GPU "
                       f"(an infeasible LP, which the CPU reference cannot certify, at "
                       f"{CPU_BATCH_CAP}), packed onto the cores largest first"}
