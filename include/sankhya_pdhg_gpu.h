@@ -246,15 +246,18 @@ int sankhya_pdhg_gpu_solve(const sankhya_pdhg_problem* problem,
  * residuals_out[9] (written in sankhya_pdhg_residuals field order), are DEVICE pointers on
  * the current device; the struct itself is read on the host. Work is queued on `stream`
  * (a cudaStream_t; NULL = the legacy default stream) and residuals_out is valid once that
- * stream reaches it. An out-of-range row index makes every output NaN.
+ * stream reaches it. An out-of-range row index makes every output NaN. A x is accumulated
+ * with FP64 atomic adds, so the last bits of the outputs can differ from call to call; every
+ * other entry point of this library is bit-for-bit repeatable.
  *
  * Scratch is a fixed 4 MiB device array inside the library (held by every GPU that loads
  * it until the process exits), so problems with more than SANKHYA_PDHG_NOALLOC_MAX_ROWS rows
- * are rejected with SANKHYA_GPU_INVALID_ARGUMENT. The first call on each device resolves the
- * array's device address (cudaGetSymbolAddress); make that first call before any stream
- * capture. All calls share the array and each leaves its contents behind (each clears what it
- * needs zeroed before use): calls whose work overlaps on the GPU race and must be ordered on
- * one stream. Nothing is allocated, host or device. */
+ * are rejected with SANKHYA_GPU_INVALID_ARGUMENT. Every call looks up the array's device
+ * address on the current device (cudaGetSymbolAddress, which allocates nothing); the first
+ * call on a device is also the one that loads the library's device code there, so make it
+ * before any stream capture. All calls share the array and each leaves its contents behind
+ * (each clears what it needs zeroed before use): calls whose work overlaps on the GPU race and
+ * must be ordered on one stream. Nothing is allocated, host or device. */
 #define SANKHYA_PDHG_NOALLOC_MAX_ROWS 516064
 int sankhya_pdhg_gpu_residuals_noalloc(const sankhya_pdhg_problem* problem, const double* x,
                                        const double* row_dual, double* residuals_out,

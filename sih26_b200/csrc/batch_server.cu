@@ -691,6 +691,7 @@ int sankhya_pdhg_server_create(const sankhya_pdhg_server_config* config,
   *out = nullptr;
   auto s = std::make_unique<Server>();
   if (config) s->cfg = *config; else sankhya_pdhg_server_default_config(&s->cfg);
+  sih26::DeviceGuard guard;
   try {
     int devices = 0;
     if (cudaGetDeviceCount(&devices) != cudaSuccess || devices == 0)
@@ -746,6 +747,8 @@ int sankhya_pdhg_server_create(const sankhya_pdhg_server_config* config,
 void sankhya_pdhg_server_free(sankhya_pdhg_server* server) {
   Server* s = reinterpret_cast<Server*>(server);
   if (!s) return;
+  sih26::DeviceGuard guard;
+  cudaSetDevice(s->cfg.device);
   if (s->stream) cudaStreamSynchronize(s->stream);
   if (s->graph) cudaGraphExecDestroy(s->graph);
   cudaFree(s->pool);
@@ -814,6 +817,7 @@ int sankhya_pdhg_server_step(sankhya_pdhg_server* server, int32_t* active, int32
     return SANKHYA_GPU_INVALID_ARGUMENT;
   }
   std::lock_guard<std::mutex> lock(s->mu);
+  sih26::DeviceGuard guard;
   try {
     SIH26_SCUDA(cudaSetDevice(s->cfg.device), SANKHYA_GPU_INIT_FAILED);
     sih26::admit(*s);

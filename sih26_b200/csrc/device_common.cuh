@@ -10,8 +10,24 @@ namespace sih26 {
 constexpr int kThreads = 512;
 constexpr int kWarps = kThreads / 32;
 
-// An absent bound is +-inf or any |v| >= 1e30 (include/sankhya/types.hpp:32-39).
-__device__ __forceinline__ bool finite_bound(double v) { return fabs(v) < 1e30; }
+// An absent bound is +-inf or any |v| >= 1e30; anything else (NaN included) is a finite bound
+// (is_finite_bound, include/sankhya/types.hpp:32-39).
+__device__ __forceinline__ bool finite_bound(double v) { return !(fabs(v) >= 1e30); }
+
+// Host side: puts the calling thread's current device back when an entry point that switched
+// to its own device returns, so a call never changes the device the caller works on.
+struct DeviceGuard {
+  int saved = -1;
+  DeviceGuard() {
+    if (cudaGetDevice(&saved) != cudaSuccess) saved = -1;
+  }
+  ~DeviceGuard() {
+    int now = -1;
+    if (saved >= 0 && cudaGetDevice(&now) == cudaSuccess && now != saved) cudaSetDevice(saved);
+  }
+  DeviceGuard(const DeviceGuard&) = delete;
+  DeviceGuard& operator=(const DeviceGuard&) = delete;
+};
 
 // Componentwise projection onto [lo, hi], tolerant of infinite sides (src/pdhg/pdhg.cpp:63-67).
 __device__ __forceinline__ double project(double v, double lo, double hi) {
@@ -79,13 +95,16 @@ __device__ __forceinline__ void block_reduce(double (&v)[NS], double* shared) {
 // Waiters give up after `limit_ns` (or as soon as another block has given up): they record an
 // error and return false instead of waiting on, so a broken launch ends instead of hanging
 // the GPU. A block that passed a barrier while another gave up stops at the next one, where
-// its own wait sees the error word.
+// its own wait sees the error word. A test can make the give-up path run: `skip_block` names
+// a block that returns from the barrier without arriving (the host sets it only when the
+// SANKHYA_PDHG_TEST_BARRIER_FAULT environment variable asks for it).
 struct GridBarrier {
   unsigned* count;                  // the barrier word; zero before the first barrier
   int* error;
   unsigned long long limit_ns;
   int* time_up;                     // set by the last arriver: global time > deadline_ns
   unsigned long long deadline_ns;   // 0 = no deadline
+  int skip_block;                   // fault injection (tests): this block never arrives; -1 none
 };
 
 __device__ __forceinline__ unsigned atom_add_acq_rel(unsigned* p, unsigned v) {
@@ -105,7 +124,9 @@ __device__ __forceinline__ void st_relaxed(unsigned* p, unsigned v) {
 __device__ __forceinline__ bool grid_barrier(const GridBarrier& b) {
   __shared__ int ok;
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (threadIdx.x == 0 && (int)blockIdx.x == b.skip_block) {
+    ok = 0;  // the injected fault: this block stays away and the others give up
+  } else if (threadIdx.x == 0) {
     const unsigned add = blockIdx.x == 0 ? 0x80000000u - (gridDim.x - 1u) : 1u;
     const unsigned old = atom_add_acq_rel(b.count, add);
     int good = 1;

@@ -502,7 +502,7 @@ static int lanes_for(int len, int nnz_per_lane) {
 static double unit_cost(int nnz) { return 1.0 + nnz / 2048.0; }
 
 HostPart partition(const std::vector<int>& ptr, int G, int warps_per_block, int lanes_override,
-                   Schedule sched) {
+                   Schedule sched, bool sliced) {
   constexpr int kSeg = 512;        // == kSegment in pdhg_kernels.cuh
   constexpr int kItem = 512;       // == kItemNnz
   // rows up to this length go to stream items (at most kStreamRowMax = 32 rows per item)
@@ -518,6 +518,7 @@ HostPart partition(const std::vector<int>& ptr, int G, int warps_per_block, int 
   // when a lane count is forced; stream items for the rest
   std::vector<int4> items;
   std::vector<double> item_cost;
+  long long sell_entries = 0;
   for (int r = L; r < rows;) {
     if (lanes_override > 0 || len(r) > kStreamRow) {
       const int lanes = lanes_override > 0 ? lanes_override : lanes_for(len(r), npl);
@@ -531,6 +532,19 @@ HostPart partition(const std::vector<int>& ptr, int G, int warps_per_block, int 
       }
       items.push_back(make_int4(begin, r, lanes, 0));
       item_cost.push_back(unit_cost(nnz));
+    } else if (sliced) {
+      // a slice: up to 32 consecutive short rows, padded to the longest of them
+      const int begin = r;
+      int nnz = 0, longest = 0;
+      while (r < rows && r - begin < 32 && len(r) <= kStreamRow) {
+        nnz += len(r);
+        longest = std::max(longest, len(r));
+        ++r;
+      }
+      longest = std::max(longest, 1);
+      items.push_back(make_int4(begin, r, -longest, static_cast<int>(sell_entries)));
+      sell_entries += static_cast<long long>(r - begin) * longest;
+      item_cost.push_back(unit_cost(nnz));
     } else {
       const int begin = r;
       int nnz = 0;
@@ -542,6 +556,8 @@ HostPart partition(const std::vector<int>& ptr, int G, int warps_per_block, int 
       item_cost.push_back(unit_cost(nnz));
     }
   }
+  if (sell_entries > 0x7fffffffLL)
+    throw Failure{SANKHYA_GPU_INVALID_ARGUMENT, "slice arrays exceed 2^31 entries"};
   // work of each long row: its segments plus the segment-sum step
   double total = 0.0;
   std::vector<double> long_cost(L);
@@ -604,6 +620,7 @@ HostPart partition(const std::vector<int>& ptr, int G, int warps_per_block, int 
   items.swap(ordered);
   (void)target;
   hp.items = std::move(items);
+  hp.sell_entries = sell_entries;
   return hp;
 }
 

@@ -71,9 +71,14 @@ sankhya_pdhg_quality quality_from_slots(const double* slots, double objective, d
 struct HostPart {
   std::vector<int> blk_seg_begin, blk_long_begin, blk_item_begin;
   std::vector<int4> segs, longs, items;
+  long long sell_entries = 0;  // sliced partitions: entries of the slice arrays
 };
+// sliced = true: the rows that would go to stream items go to slices instead ({row_begin,
+// row_end, -L, offset}: up to 32 consecutive rows stored column-major in separate arrays,
+// entry k of row row_begin + l at offset + k * rows + l, L the longest row), which one thread
+// per row sums with coalesced loads and no shared memory (the iteration kernel's layout).
 HostPart partition(const std::vector<int>& ptr, int G, int warps_per_block, int lanes_override,
-                   Schedule sched = Schedule{});
+                   Schedule sched = Schedule{}, bool sliced = false);
 
 // The autotuner's cache (one line per key, see pdhg_host.cpp). The key is built from the
 // row-length statistics of A and A' (mean, max, coefficient of variation, share of nonzeros

@@ -116,7 +116,15 @@ struct Part {
   const int* blk_item_begin;
   const int4* items;
   double* seg_sum;  // [segments * 2] scratch
+  // sliced partitions only (the iteration kernel's): the slice arrays, column indices and
+  // values (of the level's value type) in slice order; items {row_begin, row_end, -L, offset}
+  const int* sell_idx;
+  const void* sell_val;
 };
+
+// Unrolled loads per lane and round in a slice: every round issues this many independent
+// gathers before it sums them.
+constexpr int kSliceUnroll = 8;
 
 template <class T>
 struct Csr {
@@ -131,6 +139,7 @@ struct Prob {
   int m, n;
   Csr<T> A, AT;
   Part pa, pat;
+  Part pai, pati;  // the iteration kernel's sliced partitions (slice values of type T)
   // scaled problem, permuted (src/la/scaling.hpp:36-58)
   const T* c;
   const T* cl;
@@ -235,7 +244,13 @@ __device__ __forceinline__ double ro(const T* p) {
 // finish the last one, instead of every 16th item each, so no warp idles while another still
 // has two items to go. For phases that reduce nothing across rows: a row's sum is the same
 // whichever warp takes it, but a per-thread accumulator would group its terms differently.
-template <int NV, int NS, bool kShared = false, class V, class Gather, class Epi>
+//
+// kSliced: the partition holds slices instead of stream items (partition(..., sliced = true)):
+// lane l of the warp owns row row_begin + l and sums it in its stored order from the slice
+// arrays, kUnroll independent gathers in flight per round; the products are summed in the
+// row's order, as in a stream item. Such a phase uses no shared-memory stream buffer.
+template <int NV, int NS, bool kShared = false, bool kSliced = false, int kUnroll = kSliceUnroll,
+          class V, class Gather, class Epi>
 __device__ __forceinline__ void run_phase(const int* __restrict__ ptr, const int* __restrict__ idx,
                                           const V* __restrict__ val, const Part& p,
                                           const Gather& g, const Epi& epi, double (&acc)[NS],
@@ -283,9 +298,52 @@ __device__ __forceinline__ void run_phase(const int* __restrict__ ptr, const int
     }
     if (nit < ie) {
       next = __ldg(p.items + nit);
-      prefetch_range(idx, val, __ldg(ptr + next.x), __ldg(ptr + next.y), lane);
+      if (kSliced && next.z < 0)
+        prefetch_range(p.sell_idx, static_cast<const V*>(p.sell_val), next.w,
+                       next.w + (next.y - next.x) * (-next.z), lane);
+      else
+        prefetch_range(idx, val, __ldg(ptr + next.x), __ldg(ptr + next.y), lane);
     }
-    if (item.z == 0) {
+    if (kSliced && item.z < 0) {
+      // slice: lane l sums row item.x + l over the slice arrays
+      const int rows = item.y - item.x, L = -item.z;
+      const int r = item.x + lane;
+      const bool mine = lane < rows;
+      typename Epi::In in{};
+      int len = 0;
+      if (mine) {
+        in = epi.load(r);
+        len = __ldg(ptr + r + 1) - __ldg(ptr + r);
+      }
+      const int* __restrict__ si = p.sell_idx + item.w + lane;
+      const V* __restrict__ sv = static_cast<const V*>(p.sell_val) + item.w + lane;
+      double s[NV];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) s[v] = 0.0;
+      for (int k0 = 0; k0 < L; k0 += kUnroll) {
+        int j[kUnroll];
+        double a[kUnroll];
+#pragma unroll
+        for (int t = 0; t < kUnroll; ++t) {
+          const bool live = mine && k0 + t < len;
+          j[t] = live ? __ldg(si + (size_t)(k0 + t) * rows) : 0;
+          a[t] = live ? ro(sv + (size_t)(k0 + t) * rows) : 0.0;
+        }
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+          double pr[kUnroll];
+#pragma unroll
+          for (int t = 0; t < kUnroll; ++t)
+            pr[t] = (mine && k0 + t < len) ? g.product(v, a[t], j[t]) : 0.0;
+#pragma unroll
+          for (int t = 0; t < kUnroll; ++t)
+            if (k0 + t < len) s[v] += pr[t];
+        }
+      }
+      if (mine) epi.apply(r, s, in, acc);
+    } else if (kSliced && item.z == 0) {
+      // never produced by a sliced partition
+    } else if (!kSliced && item.z == 0) {
       // stream item
       const int rows = item.y - item.x;
       const int r = item.x + lane;
@@ -970,10 +1028,10 @@ __global__ void __launch_bounds__(kThreads, 2) iterate_kernel(Prob<T> P, State<T
       const double w = (double)(c.averaged + 1) / (double)(c.averaged + 2);
       if constexpr (kDelta<T>) {
         PrimalStepHalpernDelta<T> ps{S.x[cur], S.x[nxt], S.xt, S.cg, S.dl, S.du, tau, w};
-        run_phase<1, 3, true>(P.AT.ptr, P.AT.idx, P.AT.val, P.pat, Gather1<T>{S.y[cur]}, ps, acc, stream);
+        run_phase<1, 3, true, true>(P.AT.ptr, P.AT.idx, P.AT.val, P.pati, Gather1<T>{S.y[cur]}, ps, acc, stream);
       } else {
         PrimalStepHalpern<T> ps{S.x[cur], S.x[nxt], S.xt, P.c, P.cl, P.cu, S.xr, tau, w};
-        run_phase<1, 3, true>(P.AT.ptr, P.AT.idx, P.AT.val, P.pat, Gather1<T>{S.y[cur]}, ps, acc, stream);
+        run_phase<1, 3, true, true>(P.AT.ptr, P.AT.idx, P.AT.val, P.pati, Gather1<T>{S.y[cur]}, ps, acc, stream);
       }
       SIH26_MARK(0);
       if (!grid_barrier(S.bar)) goto device_error;
@@ -981,10 +1039,10 @@ __global__ void __launch_bounds__(kThreads, 2) iterate_kernel(Prob<T> P, State<T
       if constexpr (kDelta<T>) {
         DualStepHalpernDelta<T> ds{S.y[cur], S.y[nxt], S.yt, S.ax[nxt], S.yr, S.axr, P.rl64,
                                    P.ru64, sigma, w};
-        run_phase<1, 3, true>(P.A.ptr, P.A.idx, P.A.val, P.pa, Gather1<T>{S.x[nxt]}, ds, acc, stream);
+        run_phase<1, 3, true, true>(P.A.ptr, P.A.idx, P.A.val, P.pai, Gather1<T>{S.x[nxt]}, ds, acc, stream);
       } else {
         DualStepHalpern<T> ds{S.y[cur], S.y[nxt], S.yt, S.ax[nxt], P.rl, P.ru, S.yr, S.axr, sigma, w};
-        run_phase<1, 3, true>(P.A.ptr, P.A.idx, P.A.val, P.pa, Gather1<T>{S.x[nxt]}, ds, acc, stream);
+        run_phase<1, 3, true, true>(P.A.ptr, P.A.idx, P.A.val, P.pai, Gather1<T>{S.x[nxt]}, ds, acc, stream);
       }
       SIH26_MARK(2);
       if (!grid_barrier(S.bar)) goto device_error;
@@ -997,10 +1055,10 @@ __global__ void __launch_bounds__(kThreads, 2) iterate_kernel(Prob<T> P, State<T
     }
     if constexpr (kDelta<T>) {
       PrimalStepDelta<T> ps{S.x[cur], S.x[nxt], S.cg, S.dl, S.du, S.xsum, tau, c.pending};
-      run_phase<1, 3>(P.AT.ptr, P.AT.idx, P.AT.val, P.pat, Gather1<T>{S.y[cur]}, ps, acc, stream);
+      run_phase<1, 3, false, true>(P.AT.ptr, P.AT.idx, P.AT.val, P.pati, Gather1<T>{S.y[cur]}, ps, acc, stream);
     } else {
       PrimalStep<T> ps{S.x[cur], S.x[nxt], P.c, P.cl, P.cu, S.xsum, tau, c.pending};
-      run_phase<1, 3>(P.AT.ptr, P.AT.idx, P.AT.val, P.pat, Gather1<T>{S.y[cur]}, ps, acc, stream);
+      run_phase<1, 3, false, true>(P.AT.ptr, P.AT.idx, P.AT.val, P.pati, Gather1<T>{S.y[cur]}, ps, acc, stream);
     }
     SIH26_MARK(0);
     if (!grid_barrier(S.bar)) goto device_error;
@@ -1009,10 +1067,10 @@ __global__ void __launch_bounds__(kThreads, 2) iterate_kernel(Prob<T> P, State<T
     if constexpr (kDelta<T>) {
       DualStepDelta<T> ds{S.y[cur], S.y[nxt], S.ax[cur], S.ax[nxt], S.yr, S.axr, P.rl64,
                           P.ru64, S.ysum, sigma, c.pending};
-      run_phase<1, 3>(P.A.ptr, P.A.idx, P.A.val, P.pa, Gather1<T>{S.x[nxt]}, ds, acc, stream);
+      run_phase<1, 3, false, true>(P.A.ptr, P.A.idx, P.A.val, P.pai, Gather1<T>{S.x[nxt]}, ds, acc, stream);
     } else {
       DualStep<T> ds{S.y[cur], S.y[nxt], S.ax[cur], S.ax[nxt], P.rl, P.ru, S.ysum, sigma, c.pending};
-      run_phase<1, 3>(P.A.ptr, P.A.idx, P.A.val, P.pa, Gather1<T>{S.x[nxt]}, ds, acc, stream);
+      run_phase<1, 3, false, true>(P.A.ptr, P.A.idx, P.A.val, P.pai, Gather1<T>{S.x[nxt]}, ds, acc, stream);
     }
     SIH26_MARK(2);
     block_reduce<3, 0u>(acc, sh);
@@ -1043,8 +1101,8 @@ __global__ void __launch_bounds__(kThreads, 2) init_ax_kernel(Prob<T> P, State<T
   double* stream = warp_stream();
   double dummy[1] = {0.0};
   const int cur = S.ctrl->cur;
-  run_phase<1, 1>(P.A.ptr, P.A.idx, P.A.val, P.pa, Gather1<T>{S.x[cur]},
-                  StoreRow<1>{S.ax[cur], -1}, dummy, stream);
+  run_phase<1, 1, false, true>(P.A.ptr, P.A.idx, P.A.val, P.pai, Gather1<T>{S.x[cur]},
+                               StoreRow<1>{S.ax[cur], -1}, dummy, stream);
 }
 
 // out = M v over one partition with nothing fused: the autotuner times candidate schedules
@@ -1055,7 +1113,31 @@ __global__ void __launch_bounds__(kThreads, 2) probe_kernel(const int* ptr, cons
                                                             double* out) {
   double* stream = warp_stream();
   double dummy[1] = {0.0};
-  run_phase<1, 1>(ptr, idx, val, part, Gather1<T>{v}, StoreRow<1>{out, -1}, dummy, stream);
+  run_phase<1, 1, false, true>(ptr, idx, val, part, Gather1<T>{v}, StoreRow<1>{out, -1}, dummy,
+                               stream);
+}
+
+// The slice arrays of a sliced partition from the permuted CSR (one warp per slice item): entry
+// k of row row_begin + l at offset + k * rows + l, in the level's value type; padding past a
+// row's end holds column 0 and value 0 and is never summed.
+template <class T>
+__global__ void slice_fill_kernel(const int* __restrict__ ptr, const int* __restrict__ idx,
+                                  const double* __restrict__ val, const int4* __restrict__ items,
+                                  int count, int* __restrict__ sidx, T* __restrict__ sval) {
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int it = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; it < count; it += warps) {
+    const int4 item = items[it];
+    if (item.z >= 0) continue;
+    const int rows = item.y - item.x, L = -item.z;
+    if (lane >= rows) continue;
+    const int r = item.x + lane, b = ptr[r], len = ptr[r + 1] - b;
+    for (int k = 0; k < L; ++k) {
+      const size_t o = (size_t)item.w + (size_t)k * rows + lane;
+      sidx[o] = k < len ? idx[b + k] : 0;
+      sval[o] = k < len ? static_cast<T>(val[b + k]) : T(0);
+    }
+  }
 }
 
 // The FP32 level's anchor terms from (xr, yr), FP64 values: axr = A xr, cg = c + A'yr, the

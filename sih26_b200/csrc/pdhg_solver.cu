@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <limits>
@@ -135,6 +136,9 @@ static std::vector<T> gather_ptr(const T* v, const std::vector<int>& perm) {
   return out;
 }
 
+// Kernel launches of the current call on this thread (reported in the result).
+thread_local long long g_launches = 0;
+
 static Part upload_part(Arena& a, const HostPart& hp) {
   Part p;
   p.blk_seg_begin = a.upload_same(hp.blk_seg_begin);
@@ -144,11 +148,38 @@ static Part upload_part(Arena& a, const HostPart& hp) {
   p.blk_item_begin = a.upload_same(hp.blk_item_begin);
   p.items = a.upload_same(hp.items);
   p.seg_sum = a.zeros<double>(hp.segs.size() * 2);
+  p.sell_idx = nullptr;
+  p.sell_val = nullptr;
   return p;
 }
 
-// Kernel launches of the current call on this thread (reported in the result).
-thread_local long long g_launches = 0;
+static dim3 fill_grid(size_t items) {
+  return dim3(static_cast<unsigned>(std::max<size_t>(1, std::min<size_t>((items + 7) / 8, 148 * 16))));
+}
+
+// A sliced partition (the iteration kernel's) with its slice arrays in value type T, filled on
+// the device from the permuted CSR. `sidx` / `sval` may be given (scratch of at least
+// hp.sell_entries entries, reused by the autotuner's candidates); else they are allocated.
+template <class T>
+static Part upload_sliced(Arena& a, const HostPart& hp, const int* ptr, const int* idx,
+                          const double* val64, cudaStream_t stream, int* sidx = nullptr,
+                          T* sval = nullptr) {
+  Part p = upload_part(a, hp);
+  const size_t entries = static_cast<size_t>(std::max<long long>(1, hp.sell_entries));
+  if (!sidx) sidx = a.alloc<int>(entries);
+  if (!sval) sval = a.alloc<T>(entries);
+  const int count = static_cast<int>(hp.items.size());
+  if (count > 0) {
+    slice_fill_kernel<T><<<fill_grid(count), 256, 0, stream>>>(ptr, idx, val64, p.items, count,
+                                                                sidx, sval);
+    SIH26_CUDA(cudaGetLastError(), SANKHYA_GPU_KERNEL_LAUNCH_FAILED);
+    ++g_launches;
+  }
+  p.sell_idx = sidx;
+  p.sell_val = sval;
+  return p;
+}
+
 
 static void launch_coop(const void* fn, int grid, void** args, size_t smem, cudaStream_t stream) {
   SIH26_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kThreads), args, smem, stream),
@@ -270,14 +301,23 @@ static Level<T> make_level(Arena& a, const Common& cm, const PermutedLp& q,
 // on an SM (the minimum over the kernels, which share one work partition).
 template <class T>
 static int blocks_per_sm() {
-  const void* k1[] = {reinterpret_cast<const void*>(iterate_kernel<T, false>),
-                      reinterpret_cast<const void*>(iterate_kernel<T, true>),
-                      reinterpret_cast<const void*>(init_ax_kernel<T>),
+  // the iteration kernels run sliced partitions without a stream buffer: no dynamic shared
+  // memory, and the whole on-chip memory they can have goes to L1 (the gathers' cache)
+  int best = 1 << 20;
+  for (const void* f : {reinterpret_cast<const void*>(iterate_kernel<T, false>),
+                        reinterpret_cast<const void*>(iterate_kernel<T, true>)}) {
+    SIH26_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    (int)cudaSharedmemCarveoutMaxL1), SANKHYA_GPU_INIT_FAILED);
+    int b = 0;
+    SIH26_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, f, kThreads, 0),
+               SANKHYA_GPU_INIT_FAILED);
+    best = std::min(best, b);
+  }
+  const void* k1[] = {reinterpret_cast<const void*>(init_ax_kernel<T>),
                       reinterpret_cast<const void*>(anchor_kernel<T>),
                       reinterpret_cast<const void*>(report_kernel<T>),
                       reinterpret_cast<const void*>(power_kernel<T>),
                       reinterpret_cast<const void*>(probe_kernel<T>)};
-  int best = 1 << 20;
   for (const void* f : k1) {
     SIH26_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)stream_smem_bytes()), SANKHYA_GPU_INIT_FAILED);
@@ -375,7 +415,7 @@ static Ctrl run_loop(Level<T>& L, int G, cudaStream_t stream, Ctrl* host_ctrl, i
       if (timer.on) SIH26_CUDA(cudaEventRecord(timer.start[k], stream), SANKHYA_GPU_INIT_FAILED);
       launch_coop(L.halpern ? reinterpret_cast<const void*>(iterate_kernel<T, true>)
                             : reinterpret_cast<const void*>(iterate_kernel<T, false>),
-                  G, ia, stream_smem_bytes(), stream);
+                  G, ia, 0, stream);
       if (timer.on) SIH26_CUDA(cudaEventRecord(timer.stop[k], stream), SANKHYA_GPU_INIT_FAILED);
       void* ea[] = {&L.P, &L.S};
       launch_coop(reinterpret_cast<const void*>(evaluate_kernel<T>), G, ea, stream_smem_bytes(), stream);
@@ -713,18 +753,33 @@ static int autotune_schedules(Arena& a, const PermutedLp& q, const Level<T>& L, 
     ~EvFree() { cudaEventDestroy(a); cudaEventDestroy(b); }
   } ef{e0, e1};
   double best_a = INFINITY, best_at = INFINITY;
+  // the candidates' sliced partitions, and one scratch for their slice arrays per orientation
+  std::vector<HostPart> ha, hat;
+  long long ea = 1, eat = 1;
   for (const Schedule& c : kCandidates) {
-    const Part pa = upload_part(a, partition(q.a_ptr, G, kWarps, 0, c));
+    ha.push_back(partition(q.a_ptr, G, kWarps, 0, c, true));
+    hat.push_back(partition(q.at_ptr, G, kWarps, 0, c, true));
+    ea = std::max(ea, ha.back().sell_entries);
+    eat = std::max(eat, hat.back().sell_entries);
+  }
+  int* sidx_a = a.alloc<int>(ea);
+  T* sval_a = a.alloc<T>(ea);
+  int* sidx_at = a.alloc<int>(eat);
+  T* sval_at = a.alloc<T>(eat);
+  for (size_t k = 0; k < ha.size(); ++k) {
+    const Part pa = upload_sliced<T>(a, ha[k], L.P.A.ptr, L.P.A.idx, L.P.A.val64, stream,
+                                     sidx_a, sval_a);
     const double ta = time_probe<T>(L.P.A.ptr, L.P.A.idx, L.P.A.val, pa, L.S.xt, out, G, stream, e0, e1);
     if (ta < best_a) {
       best_a = ta;
-      *sa = c;
+      *sa = kCandidates[k];
     }
-    const Part pat = upload_part(a, partition(q.at_ptr, G, kWarps, 0, c));
+    const Part pat = upload_sliced<T>(a, hat[k], L.P.AT.ptr, L.P.AT.idx, L.P.AT.val64, stream,
+                                      sidx_at, sval_at);
     const double tat = time_probe<T>(L.P.AT.ptr, L.P.AT.idx, L.P.AT.val, pat, L.S.yt, out, G, stream, e0, e1);
     if (tat < best_at) {
       best_at = tat;
-      *sat = c;
+      *sat = kCandidates[k];
     }
   }
   autotune_store(path, key, *sa, *sat, best_a, best_at);
@@ -859,7 +914,7 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
   cm.ctrl = a.zeros<Ctrl>(1);
   unsigned* bar_words = a.zeros<unsigned>(2);
   int* flags = a.zeros<int>(2);
-  cm.bar = GridBarrier{bar_words, flags, 4000000000ull, flags + 1, 0ull};
+  cm.bar = GridBarrier{bar_words, flags, 4000000000ull, flags + 1, 0ull, -1};
   a.put(cm.best_x, x0.data(), n * sizeof(double), stream);
   SIH26_CUDA(cudaDeviceSynchronize(), SANKHYA_GPU_SYNC_FAILED);
 
@@ -884,6 +939,20 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
     L64.P.pat = L32.P.pat = cm.pat;
   }
 
+  // the iteration kernel's sliced partitions with the same schedule, and their slice arrays
+  // (column indices shared by both levels, values in each level's type)
+  {
+    const HostPart hai = partition(q.a_ptr, G, kWarps, prm.group_size_rows, sched_a, true);
+    const HostPart hati = partition(q.at_ptr, G, kWarps, prm.group_size_cols, sched_at, true);
+    L64.P.pai = upload_sliced<double>(a, hai, cm.a_ptr, cm.a_idx, cm.a_val64, stream);
+    L64.P.pati = upload_sliced<double>(a, hati, cm.at_ptr, cm.at_idx, cm.at_val64, stream);
+    if (mixed) {
+      L32.P.pai = upload_sliced<float>(a, hai, cm.a_ptr, cm.a_idx, cm.a_val64, stream,
+                                       const_cast<int*>(L64.P.pai.sell_idx));
+      L32.P.pati = upload_sliced<float>(a, hati, cm.at_ptr, cm.at_idx, cm.at_val64, stream,
+                                        const_cast<int*>(L64.P.pati.sell_idx));
+    }
+  }
   mark("schedules");
   // ||A||_2 by power iteration (scaling.cpp:161-194), seed random_seed + 1
   double spectral_norm = 1.0;
@@ -960,6 +1029,17 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
       SIH26_CUDA(cudaMemcpy(flags + 1, &one, sizeof one, cudaMemcpyHostToDevice), SANKHYA_GPU_COPY_FAILED);
       c0.time_up = 1;
     }
+  }
+  // Fault injection for the grid barrier's give-up path, for tests only: with
+  // SANKHYA_PDHG_TEST_BARRIER_FAULT=<ms> in the environment the last block of the iteration
+  // kernel never arrives at its first barrier, and the others give up after <ms> ms, so the
+  // call must end with DEVICE_TIMEOUT and leave the context usable.
+  if (const char* fault = std::getenv("SANKHYA_PDHG_TEST_BARRIER_FAULT")) {
+    const double ms = std::atof(fault);
+    const unsigned long long limit =
+        static_cast<unsigned long long>((ms > 0.0 ? std::min(ms, 4000.0) : 200.0) * 1e6);
+    L64.S.bar.skip_block = L32.S.bar.skip_block = G - 1;
+    L64.S.bar.limit_ns = L32.S.bar.limit_ns = limit;
   }
 
   // the pinned control-block mirror: one per calling thread, kept for the thread's lifetime
@@ -1196,6 +1276,7 @@ int sankhya_pdhg_gpu_solve(const sankhya_pdhg_problem* problem, const sankhya_pd
   }
   sankhya_pdhg_params defaults;
   sankhya_pdhg_gpu_default_params(&defaults);
+  DeviceGuard guard;
   try {
     return solve_impl(*problem, params ? *params : defaults, result);
   } catch (const Failure& f) {

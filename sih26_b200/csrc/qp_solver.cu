@@ -542,7 +542,7 @@ int qp_solve_impl(const sankhya_pdhg_problem& prob, const sankhya_qp_hessian& he
   std::vector<int> fl(2, 0);
   unsigned* bar_words = dev_upload(owned, bw);
   int* flags = dev_upload(owned, fl);
-  Q.bar = GridBarrier{bar_words, flags, 4000000000ull, flags + 1, 0ull};
+  Q.bar = GridBarrier{bar_words, flags, 4000000000ull, flags + 1, 0ull, -1};
   Q.tau = tau;
   Q.sigma = sigma;
   Q.tolerance = tolerance;
@@ -673,6 +673,7 @@ extern "C" int sankhya_qp_gpu_solve(const sankhya_pdhg_problem* problem,
     defaults.tolerance = 1e-8;  // qp_tolerance (src/util/options.cpp:335-341)
     params = &defaults;
   }
+  DeviceGuard guard;
   try {
     return qp_solve_impl(*problem, *hessian, *params, result);
   } catch (const Failure& f) {

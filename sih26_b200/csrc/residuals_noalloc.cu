@@ -21,7 +21,6 @@
 
 #include <cmath>
 #include <cstdio>
-#include <mutex>
 #include <string>
 
 #include "sankhya_pdhg_gpu.h"
@@ -59,7 +58,9 @@ __host__ __device__ inline View carve(double* base) {
   return v;
 }
 
-__device__ inline bool finite_bound(double v) { return fabs(v) < 1e30; }
+// An absent bound is +-inf or |v| >= 1e30; anything else, NaN included, is a finite bound, as
+// is_finite_bound (include/sankhya/types.hpp:32-39) decides.
+__device__ inline bool finite_bound(double v) { return !(fabs(v) >= 1e30); }
 __device__ inline double dmax(double a, double b) { return (a < b) ? b : a; }
 __device__ inline double dmin(double a, double b) { return (b < a) ? b : a; }
 
@@ -203,27 +204,27 @@ __global__ void finish_kernel(double* base, int col_blocks, int row_blocks, doub
   out[8] = dmax(c[2], r[3]);
 }
 
-// Device address of g_noalloc_scratch, resolved once per device. In host code the array's
-// name is only a stand-in for the symbol; kernels must be handed this address.
-std::mutex g_scratch_mutex;
-double* g_scratch_address[128] = {};
-
+// Device address of g_noalloc_scratch on the current device. In host code the array's name is
+// only a stand-in for the symbol; kernels must be handed this address. It is resolved on every
+// call with the caller's device current: the lookup allocates nothing and queues no work, and
+// a cached address would go stale when the module is loaded again (after cudaDeviceReset, or
+// under another context the caller makes current). The first call on a device is the one that
+// loads this library's device code there (CUDA loads modules lazily), so make it before any
+// stream capture.
 int scratch_for_current_device(double** out) {
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return SANKHYA_GPU_NO_COMPATIBLE_DEVICE;
-  if (dev < 0 || dev >= 128) return SANKHYA_GPU_INVALID_DEVICE_STATE;
-  std::lock_guard<std::mutex> lock(g_scratch_mutex);
-  if (g_scratch_address[dev] == nullptr) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || p == nullptr) {
-      sih26::g_last_error = std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") +
-                            cudaGetErrorString(e);
-      return SANKHYA_GPU_INIT_FAILED;
-    }
-    g_scratch_address[dev] = static_cast<double*>(p);
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    sih26::g_last_error = "no current CUDA device";
+    return SANKHYA_GPU_NO_COMPATIBLE_DEVICE;
   }
-  *out = g_scratch_address[dev];
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || p == nullptr) {
+    sih26::g_last_error = std::string("cudaGetSymbolAddress(g_noalloc_scratch) on device ") +
+                          std::to_string(dev) + ": " + cudaGetErrorString(e);
+    return SANKHYA_GPU_INIT_FAILED;
+  }
+  *out = static_cast<double*>(p);
   return SANKHYA_GPU_SUCCESS;
 }
 
