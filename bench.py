@@ -16,8 +16,9 @@ FP64, unscaled) through the library's C ABI.
   roofline  the iteration kernel (the dominant kernel): algorithmic bytes per attempt x
           attempts / event-timed launch durations, against the measured HBM copy bandwidth
   cpu_baseline  the reference's own solve_pdhg built from its sources (oracle/_ref), all host
-          threads, on a bounded sample: setup + 20 iterations, extrapolated to the iteration
-          count of this workload
+          threads, on a bounded sample: setup + 20 iterations, extrapolated to the iterations
+          the reference's operator needs in FP64 (counted by this run's FP64 reference-operator
+          leg on the GPU)
 
   batched  512 uneven LPs (m log-uniform on [50, 5,000], n = m U(1.5, 3), 5-15 nonzeros per
           column, 10 % primal-infeasible; lpgen.uneven_batch, seed 3) solved to relative KKT
@@ -26,11 +27,17 @@ FP64, unscaled) through the library's C ABI.
           the same LPs solved one at a time by the plain FP64 single-LP path (a sample of every
           8th LP) for the LPs/s ratio. Under torchrun the 512 LPs are sharded by nonzeros
           (sih26_b200.shard) and the time is the maximum over ranks.
-  served  Poisson request streams (default 50 and 200 LPs/s for 4 s; LPs drawn from a seeded pool of
-          the served family, m log-uniform on [100, 50,000]) into a resident server that admits
-          requests between launches of its persistent kernels (continuous batching): LPs/s and
-          p50 / p99 / p99.9 arrival-to-answer latency, next to one-at-a-time FP64 solves of
-          the same pool. Rank 0 only.
+  served  Poisson request streams at 200, 1,000 and 5,000 LPs/s for 30 s each (--served-seconds 60
+          for the survey's full windows), every request a fresh LP of the served family (m
+          log-uniform on [100, 50,000], 10 % infeasible; lpgen.served_request), into a resident
+          server that admits requests between launches of its persistent kernels (continuous
+          batching): LPs/s and p50 / p99 / p99.9 arrival-to-answer latency, per size class too,
+          next to one-at-a-time FP64 solves of the stream's first LPs. Rank 0 only.
+  configs the 2,000 x 5,000 LP (with the reference CPU solver run to tolerance for real), the
+          headline LP at 1e-4 and 1e-8, and the 258,000 x 640,000 block-angular LP, each answer
+          checked by the oracle (see config_legs).
+  parity  the headline answer's residuals recomputed by the oracle from the returned point, and
+          its active-bound pattern against the planted optimum (see parity_of).
 
   qp      the convex-QP engine on a planted 800 x 2,000 QP next to the reference's own QP
           engine on the host, and on a 40,000 x 100,000 QP alone (rank 0 only).
@@ -55,11 +62,21 @@ sys.path.insert(0, ROOT)
 
 TOLERANCE = 1e-6
 SEED = 1
+METRIC = "time-to-rel-KKT 1e-6 (s)"
 REF_SAMPLE_ITERATIONS = 20
-# Iterations the FP64 restatement of the reference algorithm needs on this workload to reach
-# relative KKT 1e-6 (measured by this bench's FP64 leg on a B200; the CPU reference runs the
-# same algorithm, so its sample is extrapolated to this count when no GPU leg ran first).
+# Iterations the reference's own operator needs on this workload to reach relative KKT 1e-6 in
+# FP64: 160,560, measured by this bench's FP64 reference-operator leg on a B200 (that leg runs
+# the reference's algorithm, src/pdhg/pdhg.cpp:383-644, in FP64; the CPU reference cannot be
+# run to tolerance here, it would take over an hour). The reference arm extrapolates its timed
+# sample to this count; the main arm uses the count its own FP64 reference-operator leg
+# measured in the same run.
 FP64_ITERATIONS_TO_TOLERANCE = 160560
+# DRAM bytes per step of the FP32 Halpern iteration kernel on this workload, from one ncu
+# capture of a 40-step launch (dram__bytes_read.sum + dram__bytes_write.sum over 40; the
+# capture command is `ncu --section SpeedOfLight --section MemoryWorkloadAnalysis --metrics
+# dram__bytes_read.sum,dram__bytes_write.sum --clock-control none -k regex:"iterate_kernel<float"
+# -s 1 -c 1 python bench.py --profile-run single`). Recaptured whenever the kernel changes.
+ITERATE_DRAM_BYTES_PER_STEP = 71.9e6
 WORKLOAD = ("powerlaw LP 200,000 x 500,000, 5,000,000 nonzeros (10 per column), rows "
             "Pareto(1.5), values N(0,1)*10^U(-2,2) per row, equality rows, 0<=x<=u, planted "
             "optimum, seed 1; relative KKT 1e-6")
@@ -288,7 +305,7 @@ def batched_leg(local, world, rank, dist, torch, algorithm="halpern"):
     # one at a time, plain FP64, on every 8th LP (its feasible ones, and its infeasible ones
     # with the certificate test that the single-LP path also runs)
     sample = list(range(0, len(lps), 8))
-    one_rate = one_at_a_time([lps[k] for k in sample], local, algorithm)
+    one_rate, _ = one_at_a_time([lps[k] for k in sample], local, algorithm)
     # the reference operator on the same batch, for comparison
     other = "reference" if algorithm == "halpern" else "halpern"
     t0 = time.perf_counter()
@@ -322,112 +339,164 @@ def batched_leg(local, world, rank, dist, torch, algorithm="halpern"):
     }
 
 
-def served_family(count, seed):
-    """The served family: m log-uniform on [100, 50,000], otherwise as the batched one."""
-    import math
-
-    import numpy as np
-
+def _gen_request(args):
+    """One request of the served stream (runs in a generator process)."""
+    seed, index = args
     from sih26_b200 import lpgen
 
-    rng = np.random.default_rng(seed)
-    out = []
-    for k in range(count):
-        m = int(round(math.exp(rng.uniform(math.log(100), math.log(50000)))))
-        n = int(round(m * rng.uniform(1.5, 3.0)))
-        out.append(lpgen.small_planted(m, n, 5, 15, rng, name=f"served{k}-{m}x{n}"))
-    return out
+    return lpgen.served_request(index, seed)
+
+
+def _size_class(m):
+    return "m<1000" if m < 1000 else ("m<10000" if m < 10000 else "m>=10000")
 
 
 def one_at_a_time(lps, local, algorithm):
-    """LPs/s of the plain FP64 single-LP path, one LP after another (after one warm-up)."""
+    """LPs/s of the plain FP64 single-LP path, one LP after another (after one warm-up), and
+    the seconds each LP took."""
     from sih26_b200 import pdhg
 
     one = pdhg.Options(pdhg_tolerance=TOLERANCE, pdhg_stop_rule="relative_kkt",
                        pdhg_precision="fp64", gpu_device=local, pdhg_algorithm=algorithm)
     pdhg.solve_pdhg(lps[0], one)
+    each = []
     t0 = time.perf_counter()
     for lp in lps:
+        t1 = time.perf_counter()
         pdhg.solve_pdhg(lp, one)
-    return len(lps) / (time.perf_counter() - t0)
+        each.append(time.perf_counter() - t1)
+    return len(lps) / (time.perf_counter() - t0), each
 
 
-def served_leg(local, rates, seconds, chunk, algorithm="halpern", pool_size=24, seed=5,
-               drain_cap=90.0):
-    """A Poisson stream at each rate (LPs/s) for `seconds` into a resident server."""
+def served_leg(local, rates, seconds, chunk, algorithm="halpern", seed=5, drain_cap=15.0,
+               sample=32, max_active=1024, backlog=64, workers=8):
+    """Poisson request streams at each rate (LPs/s) for `seconds` into a resident server.
+
+    Every request is a fresh LP (lpgen.served_request: m log-uniform on [100, 50,000],
+    n = m U(1.5, 3), 5-15 nonzeros per column, 10 % primal-infeasible), drawn by a pool of
+    generator processes ahead of need; a request's content exists when it arrives, so drawing
+    it is not part of its latency. The client hands the server the oldest arrived request
+    whenever fewer than `backlog` wait inside it (host preparation runs on the submitting
+    threads); the server admits waiting LPs between launches as slots (`max_active`) and pool
+    memory (80 % of free HBM) allow, and every active LP advances in every launch (continuous
+    batching). Latency is arrival to verified answer. Requests still unanswered `drain_cap`
+    seconds after the window closes are reported as unfinished, and the latency percentiles
+    then count them at their age (lower bounds)."""
+    import collections
     import concurrent.futures as cf
+    import multiprocessing as mp
 
     import numpy as np
 
     from sih26_b200 import pdhg
 
-    pool = served_family(pool_size, seed)
-    base_rate = one_at_a_time(pool, local, algorithm)
     opts = pdhg.Options(pdhg_tolerance=TOLERANCE, pdhg_stop_rule="relative_kkt",
                         gpu_device=local, pdhg_algorithm=algorithm)
-    # the CPU reference on the pool, one LP per host core, charged the iterations the
-    # reference operator needs (counted on the GPU)
-    ref_sols = pdhg.batch_solve(pool, pdhg.Options(pdhg_tolerance=TOLERANCE,
-                                                   pdhg_stop_rule="relative_kkt",
-                                                   gpu_device=local,
-                                                   pdhg_algorithm="reference"))
-    cpu_pool = cpu_batch_sample(pool, [s.iterations for s in ref_sols], "the pool's LPs")
-    out = []
-    for rate in rates:
-        rng = np.random.default_rng(seed + 1)
-        arrivals = []
-        t = 0.0
-        while True:
-            t += rng.exponential(1.0 / rate)
-            if t > seconds:
-                break
-            arrivals.append(t)
-        picks = rng.integers(0, pool_size, len(arrivals))
-        latency, statuses = {}, {}
-        with pdhg.Server(device=local, chunk_attempts=chunk) as srv, \
-                cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
-            srv.solve_all([pool[0]], opts)  # warm-up
-            futures, tickets = {}, {}
-            nxt = 0
-            t0 = time.perf_counter()
-            while len(latency) < len(arrivals):
-                now = time.perf_counter() - t0
-                if now > seconds + drain_cap:
+    gen = cf.ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn"))
+    try:
+        base = list(gen.map(_gen_request, [(seed, k) for k in range(sample)]))
+        base_rate, base_each = one_at_a_time(base, local, algorithm)
+        by_class_one = collections.defaultdict(list)
+        for lp, t in zip(base, base_each):
+            by_class_one[_size_class(lp.num_rows)].append(t)
+        # the CPU reference on part of the sample, one LP per host core, charged the
+        # iterations the reference operator needs (counted on the GPU)
+        cpu_lps = base[:16]
+        ref_sols = pdhg.batch_solve(cpu_lps, pdhg.Options(
+            pdhg_tolerance=TOLERANCE, pdhg_stop_rule="relative_kkt", gpu_device=local,
+            pdhg_algorithm="reference"))
+        ref_its = [CPU_BATCH_CAP if lp.farkas_star is not None else r.iterations
+                   for lp, r in zip(cpu_lps, ref_sols)]
+        cpu_pool = cpu_batch_sample(cpu_lps, ref_its, "the stream's first LPs")
+        out = []
+        for rate in rates:
+            rseed = seed * 1000 + int(rate)
+            rng = np.random.default_rng(rseed)
+            arrivals = []
+            t = 0.0
+            while True:
+                t += rng.exponential(1.0 / rate)
+                if t > seconds:
                     break
-                while nxt < len(arrivals) and arrivals[nxt] <= now:
-                    futures[nxt] = ex.submit(srv.submit, pool[picks[nxt]], opts)
-                    nxt += 1
-                for k in [k for k, f in futures.items() if f.done()]:
-                    tickets[k] = futures.pop(k).result()
-                active, waiting, _ = srv.step()
-                done_at = time.perf_counter() - t0
-                for k in list(tickets):
-                    r = srv.result(tickets[k])
-                    if r is not None:
-                        latency[k] = done_at - arrivals[k]
-                        statuses[k] = r.status
-                        del tickets[k]
-                if active == 0 and waiting == 0 and not tickets:
-                    time.sleep(0.0005)
-            span = time.perf_counter() - t0
-        done = len(latency)
-        served_rate = done / span if span > 0 else None
-        out.append({
-            "workload": f"Poisson arrivals at {rate:g} LPs/s for {seconds:g} s, LPs drawn from "
-                        f"a pool of {pool_size} of the served family (m log-uniform [100, "
-                        f"50000], n = m U(1.5,3), 5-15 nnz/col, seed {seed}), relative KKT 1e-6",
-            "offered_rate": rate, "requests": len(arrivals), "completed": done,
-            "optimal_or_feasible": sum(1 for v in statuses.values()
-                                       if v in ("optimal", "feasible")),
-            "value": served_rate, "unit": "LPs/s", "span_s": span,
-            "latency_s": _percentiles(list(latency.values())), "chunk_attempts": chunk,
-            "precision": "fp64", "algorithm": algorithm,
-            "one_at_a_time_fp64": {"value": base_rate, "unit": "LPs/s",
-                                   "sample": f"the {pool_size} LPs of the pool, once each"},
-            "speedup_vs_one_at_a_time": (served_rate / base_rate) if served_rate else None,
-            "cpu_reference": cpu_pool,
-        })
-    return out
+                arrivals.append(t)
+            N = len(arrivals)
+            ahead = 256
+            gen_f, sub_f, tickets = {}, {}, {}
+            latency, status, kkt, size = {}, {}, {}, {}
+            next_gen = next_sub = 0
+            with pdhg.Server(device=local, chunk_attempts=chunk, max_active=max_active) as srv, \
+                    cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
+                srv.solve_all([base[0]], opts)  # warm-up
+                waiting = 0
+                t0 = time.perf_counter()
+                while True:
+                    now = time.perf_counter() - t0
+                    if now > seconds + drain_cap:
+                        break
+                    arrived = int(np.searchsorted(arrivals, now, side="right"))
+                    if now > seconds and len(latency) >= arrived:
+                        break
+                    while next_gen < N and next_gen - next_sub < ahead:
+                        gen_f[next_gen] = gen.submit(_gen_request, (rseed, next_gen))
+                        next_gen += 1
+                    while (next_sub < arrived and waiting + len(sub_f) < backlog
+                           and gen_f[next_sub].done()):
+                        lp = gen_f.pop(next_sub).result()
+                        size[next_sub] = lp.num_rows
+                        sub_f[next_sub] = ex.submit(srv.submit, lp, opts)
+                        next_sub += 1
+                    for k in [k for k, f in sub_f.items() if f.done()]:
+                        tickets[k] = sub_f.pop(k).result()
+                    active, waiting, _ = srv.step()
+                    done_at = time.perf_counter() - t0
+                    for k in list(tickets):
+                        r = srv.result(tickets[k])
+                        if r is not None:
+                            latency[k] = done_at - arrivals[k]
+                            status[k] = r.status
+                            kkt[k] = _rel_kkt(r) if r.residuals else None
+                            del tickets[k]
+                    if active == 0 and waiting == 0 and not tickets and not sub_f:
+                        time.sleep(0.0005)
+                span = time.perf_counter() - t0
+                for f in sub_f.values():
+                    f.result()
+            for f in gen_f.values():
+                f.cancel()
+            unfinished = [k for k in range(N) if k not in latency]
+            ages = list(latency.values()) + [span - arrivals[k] for k in unfinished]
+            feasible_ok = sum(1 for k, v in status.items()
+                              if v in ("optimal", "feasible") and kkt[k] is not None
+                              and kkt[k] <= TOLERANCE)
+            classes = {}
+            for cname in ("m<1000", "m<10000", "m>=10000"):
+                ks = [k for k in latency if _size_class(size[k]) == cname]
+                one = by_class_one.get(cname, [])
+                classes[cname] = {
+                    "completed": len(ks), "value": len(ks) / span if span > 0 else None,
+                    "latency_s": _percentiles([latency[k] for k in ks]),
+                    "one_at_a_time_s_per_lp": (sum(one) / len(one)) if one else None}
+            served_rate = len(latency) / span if span > 0 else None
+            out.append({
+                "workload": f"Poisson arrivals at {rate:g} LPs/s for {seconds:g} s, every "
+                            f"request a fresh LP (m log-uniform [100, 50000], n = m U(1.5,3), "
+                            f"5-15 nnz/col, 10% infeasible), relative KKT 1e-6",
+                "offered_rate": rate, "seconds": seconds, "requests": N,
+                "completed": len(latency), "unfinished": len(unfinished),
+                "optimal_or_feasible": feasible_ok,
+                "certified_infeasible": sum(1 for v in status.values() if v == "infeasible"),
+                "value": served_rate, "unit": "LPs/s", "span_s": span,
+                "latency_s": _percentiles(ages), "latency_censored": bool(unfinished),
+                "chunk_attempts": chunk, "max_active": max_active,
+                "precision": "fp64", "algorithm": algorithm,
+                "one_at_a_time_fp64": base_rate,
+                "speedup_vs_one_at_a_time": (served_rate / base_rate) if served_rate else None,
+                "by_size": classes,
+                "cpu_reference": cpu_pool,
+            })
+        return out
+    finally:
+        gen.shutdown(wait=False, cancel_futures=True)
 
 
 def qp_leg(local):
@@ -468,10 +537,133 @@ def make_workload():
     return lpgen.powerlaw_planted(seed=SEED)
 
 
+def parity_of(lp, s):
+    """Parity of a returned answer, checked on the host after the timed region: the oracle's
+    unscaled residuals of the point (two FP64 SpMVs of the C restatement of the reference's
+    evaluate(), src/pdhg/pdhg.cpp:143-263, from x and row_dual alone), and its active-bound
+    pattern on the columns whose planted reduced cost is nonzero. The planted optimum is
+    strictly complementary (|z| >= 0.1), so every optimal point has those columns at the
+    planted bound; the other columns may sit anywhere on the optimal face."""
+    import numpy as np
+
+    import oracle
+
+    sense = -1.0 if lp.maximize else 1.0
+    r = oracle.oracle_evaluate(lp, s.col_value, -sense * s.row_dual)
+    out = {"rel_kkt_oracle": max(r["primal"], r["dual"], r["gap"]),
+           "rel_primal": r["primal"], "rel_dual": r["dual"], "rel_gap": r["gap"],
+           "status": s.status}
+    if lp.x_star is not None and lp.row_dual_star is not None:
+        z = lp.cost - lp.to_scipy_csc().T @ lp.row_dual_star
+        x = s.col_value
+        lo, hi = lp.col_lower, lp.col_upper
+        at_lo = np.abs(x - lo) <= 1e-6 * np.maximum(1.0, np.abs(lo))
+        at_hi = np.abs(x - hi) <= 1e-6 * np.maximum(1.0, np.abs(hi))
+        forced_lo, forced_hi = z > 0.05, z < -0.05
+        out["pattern_checked_columns"] = int(forced_lo.sum() + forced_hi.sum())
+        out["pattern_mismatches"] = int((forced_lo & ~at_lo).sum() + (forced_hi & ~at_hi).sum())
+        out["objective_rel_error"] = (abs(s.objective - lp.optimal_objective)
+                                      / max(1.0, abs(lp.optimal_objective)))
+    return out
+
+
+def _rel_kkt(s):
+    r = s.residuals
+    return max(r["relative_primal"], r["relative_dual"], r["relative_gap"])
+
+
+def config_legs(local, flush, sync, fp64_ref_iterations):
+    """The other single-LP configurations, each solved once outside the timed region, through
+    the C ABI from host arrays, with its answer checked by the oracle:
+
+      c0  2,000 x 5,000 uniform LP (lpgen.uniform_planted, seed 0), relative KKT 1e-6: the GPU
+          (FP64 with the reference's operator, and FP32-mixed Halpern) next to the reference's
+          own solve_pdhg run to the same tolerance on all host threads, for real;
+      c1  the headline LP at relative KKT 1e-4 and 1e-8 (FP32-mixed Halpern; the FP64 polish
+          takes over when the FP32 level stops improving);
+      c2  the block-angular LP (64 blocks of 4,000 x 10,000, 8 nonzeros per column, 2,000
+          linking rows over 2 % of the columns, 30 % '<=' rows; lpgen.block_angular_planted,
+          seed 2, 258,000 x 640,000, 30.7M nonzeros), FP32-mixed Halpern to 1e-6, with the
+          roofline of its iteration kernel."""
+    import oracle
+    from sih26_b200 import lpgen, pdhg
+
+    peak, _ = _peaks()
+    out = {}
+
+    def solve(lp, tol, precision, algorithm, profile=False):
+        flush.random_(0, 255)
+        sync()
+        s = pdhg.solve_pdhg(lp, pdhg.Options(
+            pdhg_tolerance=tol, pdhg_stop_rule="relative_kkt", pdhg_precision=precision,
+            pdhg_algorithm=algorithm, gpu_device=local, pdhg_profile_kernels=profile,
+            pdhg_autotune=True))
+        sync()
+        return s
+
+    def record(lp, s, tol):
+        p = parity_of(lp, s)
+        return {"device_s": s.device_seconds, "e2e_s": s.solve_seconds,
+                "iterations": s.iterations, "fp32_iterations": s.fp32_iterations,
+                "rel_kkt": _rel_kkt(s), "tolerance": tol, **p}
+
+    # c0: small enough for the CPU reference to run to tolerance
+    lp0 = lpgen.uniform_planted(2000, 5000, 10, seed=0)
+    solve(lp0, TOLERANCE, "fp64", "reference")  # warm-up of this shape
+    c0 = {"fp64_reference_operator": record(lp0, solve(lp0, TOLERANCE, "fp64", "reference"),
+                                            TOLERANCE),
+          "mixed_halpern": record(lp0, solve(lp0, TOLERANCE, "mixed", "halpern"), TOLERANCE)}
+    if oracle.ref_available():
+        os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+        oracle.ref_solve(lp0, tolerance=TOLERANCE, iteration_limit=50, stop_at_request=True)
+        t0 = time.perf_counter()
+        r = oracle.ref_solve(lp0, tolerance=TOLERANCE, stop_at_request=True)
+        cpu_s = time.perf_counter() - t0
+        pr = parity_of(lp0, r)
+        c0["cpu_reference"] = {"seconds": cpu_s, "iterations": r.iterations,
+                               "status": r.status, "threads": int(os.environ["OMP_NUM_THREADS"]),
+                               "kind": "reference, run to tolerance (pdhg_stop_at_request)",
+                               "rel_kkt_oracle": pr["rel_kkt_oracle"],
+                               "pattern_mismatches": pr.get("pattern_mismatches")}
+        c0["cpu_over_gpu_e2e"] = cpu_s / c0["fp64_reference_operator"]["e2e_s"]
+    out["c0"] = c0
+
+    # c1 at the survey's other tolerances
+    lp1 = make_workload()
+    for tol in (1e-4, 1e-8):
+        out[f"c1_{tol:g}"] = record(lp1, solve(lp1, tol, "mixed", "halpern"), tol)
+    del lp1
+
+    # c2: the block-angular LP
+    lp2 = lpgen.block_angular_planted()
+    solve(lp2, 1e-2, "mixed", "halpern")  # warm-up and autotune of this shape
+    s2 = solve(lp2, TOLERANCE, "mixed", "halpern", profile=True)
+    c2 = record(lp2, s2, TOLERANCE)
+    share = s2.fp32_iterations / max(1, s2.iterations)
+    m, n, nnz = lp2.num_rows, lp2.num_cols, lp2.num_nonzeros
+    b = (share * algorithmic_bytes(m, n, nnz, 4, "halpern")
+         + (1 - share) * algorithmic_bytes(m, n, nnz, 8, "halpern"))
+    if s2.iterate_kernel_seconds > 0:
+        ach = b * s2.attempts / s2.iterate_kernel_seconds / 1e9
+        c2["roofline"] = {"achieved": ach, "peak": peak, "frac": ach / peak,
+                          "bytes_per_attempt": b,
+                          "us_per_attempt": s2.iterate_kernel_seconds / s2.attempts * 1e6}
+    out["c2"] = c2
+    out["fp64_reference_operator_iterations_c1"] = fp64_ref_iterations
+    return out
+
+
 def run_reference(args):
+    """The reference arm: the reference's own solve_pdhg (oracle/_ref, built from its sources)
+    on the host cores. A step is a bounded sample of the headline solve (setup + 20 iterations)
+    extrapolated to FP64_ITERATIONS_TO_TOLERANCE; the 2,000 x 5,000 LP is also run to
+    tolerance for real once."""
     world, rank = _dist()
     if rank != 0:
         return 0
+    import oracle
+    from sih26_b200 import lpgen
+
     lp = make_workload()
     values = []
     info = None
@@ -483,21 +675,54 @@ def run_reference(args):
             info = (kind, threads, setup, per_it)
     kind, threads, setup, per_it = info
     value = statistics.mean(values)
-    sample = (f"solve_pdhg setup ({setup:.2f} s) + {REF_SAMPLE_ITERATIONS} iterations "
-              f"({per_it * 1e3:.2f} ms each) per step, extrapolated to "
-              f"{FP64_ITERATIONS_TO_TOLERANCE} iterations")
+    c0 = None
+    if oracle.ref_available():
+        lp0 = lpgen.uniform_planted(2000, 5000, 10, seed=0)
+        t0 = time.perf_counter()
+        r = oracle.ref_solve(lp0, tolerance=TOLERANCE, stop_at_request=True)
+        c0 = {"seconds": time.perf_counter() - t0, "iterations": r.iterations,
+              "status": r.status, "kind": "reference, run to tolerance"}
     line = {
-        "impl": "reference", "metric": "time-to-rel-KKT 1e-6 (s)", "value": value, "unit": "s",
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD},
+        "config": {"workload": WORKLOAD, "precision": "fp64", "algorithm": "reference"},
         "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": kind,
-                         "sample": sample},
+                         "extrapolated": True,
+                         "iterations_charged": FP64_ITERATIONS_TO_TOLERANCE,
+                         "sample": f"setup {setup:.2f} s + {REF_SAMPLE_ITERATIONS} its at "
+                                   f"{per_it * 1e3:.2f} ms, extrapolated"},
         "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "c0_to_tolerance": c0,
     }
     print(json.dumps(line))
     return 0
+
+
+def _brief_batched(b):
+    """The batched leg's headline figures, early in the line."""
+    if not b:
+        return None
+    lat = b["latency_s"]
+    return {"value": b["value"], "unit": "LPs/s", "p50_s": lat["p50"], "p99_s": lat["p99"],
+            "p99.9_s": lat["p99.9"], "met_tolerance": b["met_tolerance"],
+            "feasible_lps": b["feasible_lps"], "certified_infeasible": b["certified_infeasible"],
+            "planted_infeasible": b["planted_infeasible"],
+            "one_at_a_time_fp64": b["one_at_a_time_fp64"]["value"],
+            "speedup_vs_one_at_a_time": b["speedup_vs_one_at_a_time"],
+            "cpu_reference": (b["cpu_reference"] or {}).get("value")}
+
+
+def _brief_served(v):
+    lat = v["latency_s"]
+    keep = ("offered_rate", "seconds", "requests", "completed", "optimal_or_feasible",
+            "certified_infeasible", "value", "unfinished", "speedup_vs_one_at_a_time",
+            "one_at_a_time_fp64", "chunk_attempts", "by_size")
+    out = {k: v[k] for k in keep if k in v}
+    out.update({"p50_s": lat["p50"], "p99_s": lat["p99"], "p99.9_s": lat["p99.9"],
+                "latency_censored": v.get("latency_censored")})
+    return out
 
 
 def run_ours(args):
@@ -568,10 +793,8 @@ def run_ours(args):
     for s in sols:
         if s.status not in ("optimal", "feasible"):
             raise SystemExit(f"solve did not converge: {s.status} {s.message}")
-        rel = max(s.residuals["relative_primal"], s.residuals["relative_dual"],
-                  s.residuals["relative_gap"])
-        if rel > TOLERANCE:
-            raise SystemExit(f"solve stopped above the tolerance: {rel}")
+        if _rel_kkt(s) > TOLERANCE:
+            raise SystemExit(f"solve stopped above the tolerance: {_rel_kkt(s)}")
     # roofline of the iteration kernel: attempts are all FP32 unless the polish ran
     attempts = sum(s.attempts for s in sols)
     kern = sum(s.iterate_kernel_seconds for s in sols)
@@ -580,21 +803,23 @@ def run_ours(args):
                      + (1 - fp32_share) * algorithmic_bytes(m, n, nnz, 8, algo))
     achieved = bytes_attempt * attempts / kern / 1e9 if kern > 0 else None
     peak, peak_kind = _peaks()
-    traffic = None
-    summary = os.path.join(ROOT, "profiles", "iterate_kernel_powerlaw_200k.md")
-    if os.path.exists(summary):
-        for line in open(summary):
-            if line.startswith("dram_bytes_per_attempt:"):
-                traffic = float(line.split(":")[1].strip().split()[0])
+    traffic = ITERATE_DRAM_BYTES_PER_STEP if algo == "halpern" else None
+    # the reference's own operator in FP64 is what the CPU reference runs: its iteration count
+    # on this GPU is the count both CPU figures are charged
+    ref_its = alt_fp64.iterations if algo == "halpern" else fp64.iterations
     cpu = None
+    parity = None
     if rank == 0:
         kind, threads, setup, per_it = cpu_reference_sample(lp, REF_SAMPLE_ITERATIONS)
-        cpu = {"value": setup + per_it * fp64.iterations, "unit": "s", "cores": threads,
-               "kind": kind,
-               "sample": (f"solve_pdhg setup ({setup:.2f} s) + {REF_SAMPLE_ITERATIONS} "
-                          f"iterations ({per_it * 1e3:.2f} ms each), extrapolated to the "
-                          f"{fp64.iterations} iterations the FP64 GPU leg needed")}
+        cpu = {"value": setup + per_it * ref_its, "unit": "s", "cores": threads, "kind": kind,
+               "extrapolated": True, "iterations_charged": ref_its,
+               "sample": f"setup {setup:.2f} s + {REF_SAMPLE_ITERATIONS} its at "
+                         f"{per_it * 1e3:.2f} ms, extrapolated"}
+        parity = parity_of(lp, last)
     launches = int(statistics.mean(s.kernel_launches for s in sols))
+    configs = None
+    if rank == 0 and not args.no_configs:
+        configs = config_legs(local, flush, sync, ref_its)
     batched = (None if args.no_batched
                else batched_leg(local, world, rank, dist, torch, args.algorithm))
     served = None
@@ -605,28 +830,20 @@ def run_ours(args):
     qp = qp_leg(local) if rank == 0 and not args.no_qp else None
     if rank == 0:
         line = {
-            "metric": "time-to-rel-KKT 1e-6 (s), FP32-mixed", "value": dev, "unit": "s",
+            "metric": METRIC, "value": dev, "unit": "s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": dev * 1e3, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 iterates, f64 reductions",
             "data": "synthetic (seeded planted-optimum LP)",
+            "gpu_launches": launches,
             "config": {"workload": WORKLOAD, "tolerance": TOLERANCE,
                        "stop_rule": "relative_kkt", "precision": "mixed", "algorithm": algo,
                        "l2": "inputs larger than L2 (A, A' and vectors ~0.3 GB resident) and a "
                              "256 MB L2 flush before every step",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
-            "iterations": last.iterations, "fp32_iterations": last.fp32_iterations,
-            "schedule": {"autotuned": last.autotuned, "stream_row_max_A": last.schedule[0],
-                         "nnz_per_lane_A": last.schedule[1],
-                         "stream_row_max_AT": last.schedule[2],
-                         "nnz_per_lane_AT": last.schedule[3]},
-            "attempts": last.attempts, "restarts": last.restarts,
-            "objective_rel_error": abs(last.objective - lp.optimal_objective)
-            / abs(lp.optimal_objective),
-            "fp64": {"value": fp64_dev, "unit": "s", "iterations": fp64.iterations,
-                     "status": fp64.status},
-            "algorithm": algo,
-            f"{other}_operator": alt,
+            "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": last.h2d_bytes,
+                    "d2h_bytes_per_step": last.d2h_bytes,
+                    "setup_s": statistics.mean(s.setup_seconds for s in sols)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None,
                          "traffic": traffic, "peak_kind": peak_kind,
@@ -634,14 +851,21 @@ def run_ours(args):
                          "bytes_per_attempt": bytes_attempt,
                          "us_per_attempt": kern / attempts * 1e6 if attempts else None},
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": last.h2d_bytes,
-                    "d2h_bytes_per_step": last.d2h_bytes,
-                    "setup_s": statistics.mean(s.setup_seconds for s in sols)},
-            "gpu_launches": launches,
             "clocks": clocks.summary(),
-            "batched": batched,
-            "served": served,
+            "parity": parity,
+            "fp64": {"value": fp64_dev, "unit": "s", "iterations": fp64.iterations,
+                     "status": fp64.status},
+            "iterations": last.iterations, "fp32_iterations": last.fp32_iterations,
+            "attempts": last.attempts, "restarts": last.restarts,
+            "algorithm": algo,
+            f"{other}_operator": alt,
+            "schedule": {"autotuned": last.autotuned, "A": list(last.schedule[:2]),
+                         "AT": list(last.schedule[2:])},
+            "batched": _brief_batched(batched),
+            "served": [_brief_served(v) for v in served] if served else None,
+            "configs": configs,
             "qp": qp,
+            "batched_detail": batched,
         }
         print(json.dumps(line))
     if dist is not None:
@@ -684,10 +908,12 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the 512-LP batched leg")
     ap.add_argument("--no-served", action="store_true", help="skip the served-stream leg")
     ap.add_argument("--no-qp", action="store_true", help="skip the convex-QP leg")
-    ap.add_argument("--served-rates", default="50,200",
-                    help="Poisson rates, LPs/s, comma-separated (the served family's full "
-                         "study is 200,1000,5000 for 60 s)")
-    ap.add_argument("--served-seconds", type=float, default=4.0, help="arrival window, s")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the 2,000 x 5,000, block-angular and 1e-4 / 1e-8 legs")
+    ap.add_argument("--served-rates", default="200,1000,5000",
+                    help="Poisson rates, LPs/s, comma-separated")
+    ap.add_argument("--served-seconds", type=float, default=30.0,
+                    help="arrival window per rate, s (the survey's study is 60)")
     ap.add_argument("--served-chunk", type=int, default=512,
                     help="attempts per LP per server launch")
     ap.add_argument("--profile-run", choices=["single", "batch"], default=None,

@@ -343,6 +343,20 @@ def uneven_batch(count: int = 512, m_lo: int = 50, m_hi: int = 5_000,
     return out
 
 
+def served_request(index: int, seed: int = 5, m_lo: int = 100, m_hi: int = 50_000,
+                   infeasible_fraction: float = 0.1) -> LP:
+    """Request `index` of the served stream: one LP drawn like the batched family but with m
+    log-uniform on [m_lo, m_hi], from its own seeded generator (seed, index), so every request
+    is a fresh LP and any request can be drawn without the ones before it."""
+    rng = np.random.default_rng([seed, index])
+    m = int(round(math.exp(rng.uniform(math.log(m_lo), math.log(m_hi)))))
+    n = int(round(m * rng.uniform(1.5, 3.0)))
+    lp = small_planted(m, n, 5, 15, rng, name=f"request{index}-{m}x{n}")
+    if rng.random() < infeasible_fraction:
+        lp = make_infeasible(lp, rng)
+    return lp
+
+
 def from_dense(rows, row_lower, row_upper, cost, col_lower=None, col_upper=None,
                maximize=False, objective_offset=0.0, name="") -> LP:
     """A tiny LP written out by hand, the way the reference's unit tests build them
