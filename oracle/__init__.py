@@ -20,6 +20,8 @@ from .loader import (  # noqa: F401
     oracle_uniform_draws,
     ref_available,
     ref_farkas_check,
+    ref_kkt_instance,
+    ref_polish_ipm,
     ref_qp_solve,
     ref_ray_check,
     ref_read_model,

@@ -53,6 +53,13 @@ class _RefOut(C.Structure):
                 ("algorithm", C.c_char * 32), ("message", C.c_char * 1024)]
 
 
+class _PolishOut(C.Structure):
+    _fields_ = [("status", C.c_int32), ("polished", C.c_int32), ("iterations", C.c_int64),
+                ("polish_iterations", C.c_int64), ("objective", C.c_double),
+                ("primal_infeasibility", C.c_double), ("dual_infeasibility", C.c_double),
+                ("algorithm", C.c_char * 64), ("message", C.c_char * 1024)]
+
+
 def _p(a, t):
     return a.ctypes.data_as(t)
 
@@ -130,6 +137,11 @@ def _ref():
         lib.ref_read_model.argtypes = [C.c_char_p, C.POINTER(_LP), C.c_char_p, C.c_int]
         lib.ref_recompute_quality.argtypes = [C.POINTER(_LP), _f64p, _f64p, _f64p, C.c_double,
                                               _f64p]
+        lib.ref_kkt_instance.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_int, C.POINTER(_LP),
+                                         C.POINTER(C.c_double)]
+        lib.ref_polish_ipm.argtypes = [C.POINTER(_LP), _f64p, _f64p, _f64p, C.c_int32, C.c_int64,
+                                       C.c_char_p, C.c_double, _f64p, _f64p, _f64p,
+                                       C.POINTER(_PolishOut)]
         _libs["ref"] = lib
     return _libs["ref"]
 
@@ -299,6 +311,61 @@ def ref_read_model(path):
               row_lower=arrs["rl"], row_upper=arrs["ru"], maximize=bool(head.maximize),
               objective_offset=head.objective_offset,
               name=os.path.splitext(os.path.basename(path))[0])
+
+
+STATUS_VALUES = {v: k for k, v in STATUS_NAMES.items()}
+
+
+def ref_polish_ipm(lp, col_value, row_dual, col_dual, status, iterations, algorithm,
+                   scaled_worst) -> dict:
+    """The reference's interior-point polish of a first-order answer (ipm::solve_ipm with a
+    WarmStart, inside the steps of polish_with_the_interior_point, src/core/solve.cpp:184-243):
+    returns the merged answer's status, algorithm, iterations, objective and point."""
+    lib = _ref()
+    pin = _Pinned(lp)
+    x = np.ascontiguousarray(col_value, dtype=np.float64)
+    rd = np.ascontiguousarray(row_dual, dtype=np.float64)
+    cd = np.ascontiguousarray(col_dual, dtype=np.float64)
+    xo, rdo, cdo = np.zeros(lp.num_cols), np.zeros(lp.num_rows), np.zeros(lp.num_cols)
+    out = _PolishOut()
+    rc = lib.ref_polish_ipm(C.byref(pin.s), _p(x, _f64p), _p(rd, _f64p), _p(cd, _f64p),
+                            STATUS_VALUES[status], int(iterations), algorithm.encode(),
+                            float(scaled_worst), _p(xo, _f64p), _p(rdo, _f64p), _p(cdo, _f64p),
+                            C.byref(out))
+    if rc != 0:
+        raise RuntimeError(out.message.decode())
+    return {"status": STATUS_NAMES[out.status], "polished": bool(out.polished),
+            "iterations": out.iterations, "polish_iterations": out.polish_iterations,
+            "objective": out.objective, "primal_infeasibility": out.primal_infeasibility,
+            "dual_infeasibility": out.dual_infeasibility,
+            "algorithm": out.algorithm.decode(), "message": out.message.decode(),
+            "col_value": xo, "row_dual": rdo, "col_dual": cdo}
+
+
+def ref_kkt_instance(seed, max_rows, max_cols, index):
+    """Instance `index` of the reference's kkt_lp sequence from mt19937_64(seed)
+    (tests/oracles/lp_generator.cpp:122-189, converted by oracle::to_model), as an lpgen.LP,
+    with its analytic optimal objective in .optimal_objective."""
+    from sih26_b200.lpgen import LP
+
+    lib = _ref()
+    head = _LP()
+    opt = C.c_double()
+    if lib.ref_kkt_instance(seed, max_rows, max_cols, index, C.byref(head), C.byref(opt)) != 0:
+        raise RuntimeError("ref_kkt_instance failed")
+    m, n, nnz = head.num_rows, head.num_cols, head.num_nonzeros
+    arrs = dict(cs=np.zeros(n + 1, np.int32), ri=np.zeros(nnz, np.int32), v=np.zeros(nnz),
+                c=np.zeros(n), cl=np.zeros(n), cu=np.zeros(n), rl=np.zeros(m), ru=np.zeros(m))
+    full = _LP(m, n, nnz, _p(arrs["cs"], _i32p), _p(arrs["ri"], _i32p), _p(arrs["v"], _f64p),
+               _p(arrs["c"], _f64p), _p(arrs["cl"], _f64p), _p(arrs["cu"], _f64p),
+               _p(arrs["rl"], _f64p), _p(arrs["ru"], _f64p), 0, 0.0)
+    if lib.ref_kkt_instance(seed, max_rows, max_cols, index, C.byref(full), C.byref(opt)) != 0:
+        raise RuntimeError("ref_kkt_instance failed")
+    return LP(num_rows=m, num_cols=n, col_starts=arrs["cs"], row_indices=arrs["ri"],
+              values=arrs["v"], cost=arrs["c"], col_lower=arrs["cl"], col_upper=arrs["cu"],
+              row_lower=arrs["rl"], row_upper=arrs["ru"], maximize=bool(head.maximize),
+              objective_offset=head.objective_offset, name=f"kkt{index}",
+              optimal_objective=float(opt.value))
 
 
 QUALITY_KEYS = ("primal_infeasibility", "primal_infeasibility_scaled", "dual_infeasibility",

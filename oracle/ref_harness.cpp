@@ -14,6 +14,9 @@
 //   sankhya::io::read_model              include/sankhya/io.hpp:53  (MPS/LP files, for pins)
 //   sankhya::qp::solve_convex_qp         src/qp/qp_condat_vu.cpp:150 include/sankhya/qp.hpp:20
 //   sankhya::Solution::recompute_quality src/core/model.cpp:228      include/sankhya/model.hpp:373
+//   sankhya::ipm::solve_ipm (warm start) src/ipm/ipm.cpp            include/sankhya/ipm.hpp:41,
+//     inside a restatement of its caller polish_with_the_interior_point
+//     (src/core/solve.cpp:184-243), which sits among the whole solve() machinery
 #include <algorithm>
 #include <cstdint>
 #include <cstdio>
@@ -24,6 +27,7 @@
 
 #include "sankhya/certificate.hpp"
 #include "sankhya/io.hpp"
+#include "sankhya/ipm.hpp"
 #include "sankhya/logging.hpp"
 #include "sankhya/model.hpp"
 #include "sankhya/options.hpp"
@@ -325,6 +329,82 @@ int ref_recompute_quality(const ref_lp* lp, const double* col_value, const doubl
     out[7] = s.relative_gap;
     return 0;
   } catch (const std::exception&) {
+    return 1;
+  }
+}
+
+}  // extern "C"
+
+// ---- the interior-point polish of a first-order answer ------------------------------------
+//
+// polish_with_the_interior_point (src/core/solve.cpp:184-243) runs right after the PDHG
+// engine at the call site the GPU library replaces (src/core/solve.cpp:392-393). This entry
+// point repeats its few steps -- the options it sets, the warm start it builds, the "better"
+// rule and the "+ipm" algorithm name -- around the reference's own interior point.
+extern "C" {
+
+struct ref_polish_out {
+  std::int32_t status;    // sankhya::SolveStatus of the merged answer
+  std::int32_t polished;  // 1 when the interior point's answer replaced the first one
+  std::int64_t iterations;
+  std::int64_t polish_iterations;
+  double objective;
+  double primal_infeasibility;
+  double dual_infeasibility;
+  char algorithm[64];
+  char message[1024];
+};
+
+/// first_status is the first answer's sankhya::SolveStatus value; first_algorithm its
+/// Solution::algorithm (e.g. "pdhg-gpu"); first_scaled_worst its max(primal, dual)
+/// infeasibility over the recompute_quality scales. col_value / row_dual / col_dual are the
+/// first answer in the reference's units and signs; polished outputs may be NULL.
+int ref_polish_ipm(const ref_lp* lp, const double* col_value, const double* row_dual,
+                   const double* col_dual, std::int32_t first_status, std::int64_t first_iterations,
+                   const char* first_algorithm, double first_scaled_worst, double* x_out,
+                   double* rd_out, double* cd_out, ref_polish_out* out) {
+  using namespace sankhya;
+  try {
+    const Model model = to_model(*lp);
+    const auto n = static_cast<std::size_t>(lp->num_cols);
+    const auto m = static_cast<std::size_t>(lp->num_rows);
+    Options options;
+    // solve.cpp:196-214: the polish's own iteration cap and clock
+    Options polish = options;
+    polish.set_int("iteration_limit", options.get_int("polish_iteration_limit"));
+    polish.set_double("time_limit", options.get_double("polish_max_seconds"));
+    Logger logger(stdout, LogLevel::kWarning);
+    const ipm::WarmStart warm{std::vector<double>(col_value, col_value + n),
+                              std::vector<double>(row_dual, row_dual + m),
+                              std::vector<double>(col_dual, col_dual + n)};
+    Solution polished = ipm::solve_ipm(model, polish, logger, &warm);
+    // solve.cpp:218-231: kept only when better
+    const double worst = std::max(polished.primal_infeasibility_scaled,
+                                  polished.dual_infeasibility_scaled);
+    const bool better = polished.status == SolveStatus::kOptimal ||
+                        (polished.status == SolveStatus::kFeasible && worst < first_scaled_worst);
+    out->polished = better ? 1 : 0;
+    out->polish_iterations = polished.iterations;
+    std::string algorithm = first_algorithm ? first_algorithm : "";
+    if (better) {
+      algorithm += "+ipm";  // solve.cpp:237
+      out->status = static_cast<std::int32_t>(polished.status);
+      out->iterations = polished.iterations + first_iterations;
+      out->objective = polished.objective;
+      out->primal_infeasibility = polished.primal_infeasibility;
+      out->dual_infeasibility = polished.dual_infeasibility;
+      if (x_out && polished.col_value.size() == n) std::memcpy(x_out, polished.col_value.data(), n * 8);
+      if (rd_out && polished.row_dual.size() == m) std::memcpy(rd_out, polished.row_dual.data(), m * 8);
+      if (cd_out && polished.col_dual.size() == n) std::memcpy(cd_out, polished.col_dual.data(), n * 8);
+    } else {
+      out->status = first_status;
+      out->iterations = first_iterations;
+    }
+    std::snprintf(out->algorithm, sizeof out->algorithm, "%s", algorithm.c_str());
+    std::snprintf(out->message, sizeof out->message, "%s", polished.message.c_str());
+    return 0;
+  } catch (const std::exception& e) {
+    std::snprintf(out->message, sizeof out->message, "%s", e.what());
     return 1;
   }
 }

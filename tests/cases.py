@@ -50,3 +50,45 @@ def generated_cases():
         out.append((f"uniform_60x150_s{seed}", lpgen.uniform_planted(60, 150, 4, seed=seed)))
     out.append(("uniform_200x500_s7", lpgen.uniform_planted(200, 500, 5, seed=7)))
     return out
+
+
+def netlib_cases():
+    """The Netlib LPs of the reference tree (data/netlib/*.mps) as read by the reference's MPS
+    reader, from tests/golden/netlib.npz (made by tests/golden/make_netlib.py): (LP, published
+    optimum, the reference solve_pdhg's status and objective at pdhg_tolerance 1e-8)."""
+    import os
+
+    import numpy as np
+
+    from sih26_b200.lpgen import LP
+
+    d = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "netlib.npz"))
+    names = sorted({k.split("/")[0] for k in d.files},
+                   key=lambda nm: int(d[nm + "/meta"][0]) * int(d[nm + "/meta"][1]))
+    out = []
+    for nm in names:
+        m, n, mx = (int(v) for v in d[nm + "/meta"])
+        lp = LP(num_rows=m, num_cols=n, col_starts=d[nm + "/col_starts"],
+                row_indices=d[nm + "/row_indices"], values=d[nm + "/values"],
+                cost=d[nm + "/cost"], col_lower=d[nm + "/col_lower"],
+                col_upper=d[nm + "/col_upper"], row_lower=d[nm + "/row_lower"],
+                row_upper=d[nm + "/row_upper"], maximize=bool(mx),
+                objective_offset=float(d[nm + "/objective_offset"]), name=nm)
+        out.append((lp, float(d[nm + "/published_optimal"]), str(d[nm + "/ref_status"]),
+                    float(d[nm + "/ref_objective"])))
+    return out
+
+
+def kkt_fuzz_cases():
+    """The 120 instances of the reference's cross-engine gate (tests/unit/test_pdhg.cpp:178-222)
+    from tests/golden/kkt_fuzz_120.npz: (LP with its analytic optimum, the reference
+    solve_pdhg's status and objective at pdhg_tolerance 1e-9)."""
+    import os
+    import sys
+
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    if here not in sys.path:
+        sys.path.insert(0, here)
+    import make_kkt_fuzz
+
+    return make_kkt_fuzz.load()
