@@ -417,6 +417,40 @@ def from_wire(buffer) -> LP:
     return lp
 
 
+class WireRequest:
+    """A request held in its wire form: the 8-byte-aligned buffer and the problem struct that
+    sankhya_pdhg_wire_view points into it. The solves below read the LP in place; nothing is
+    copied out of the buffer on the host."""
+
+    def __init__(self, buffer):
+        lib = load_library()
+        _bind_wire(lib)
+        raw = np.frombuffer(buffer, dtype=np.uint8)
+        self.buffer = np.zeros((raw.size + 7) // 8, dtype=np.uint64).view(np.uint8)[:raw.size]
+        self.buffer[:] = raw
+        self.problem = _Problem()
+        code = lib.sankhya_pdhg_wire_view(self.buffer.ctypes.data, self.buffer.size,
+                                          C.byref(self.problem))
+        if code != 0:
+            raise GpuError(code, lib.sankhya_pdhg_gpu_last_error().decode())
+        self.num_rows = self.problem.num_rows
+        self.num_cols = self.problem.num_cols
+
+
+def solve_wire(request: WireRequest, options: Optional[Options] = None) -> Solution:
+    """sankhya_pdhg_gpu_solve on an LP read in place from its wire buffer."""
+    opt = options or Options()
+    lib = load_library()
+    prm = _params(opt, lib)
+    out = _Outputs(request)
+    code = lib.sankhya_pdhg_gpu_solve(C.byref(request.problem), C.byref(prm), C.byref(out.res))
+    if code != 0:
+        raise GpuError(code, lib.sankhya_pdhg_gpu_last_error().decode())
+    sol = out.solution(request)
+    sol.algorithm = "pdhg-gpu"
+    return sol
+
+
 # ---- many LPs at once (the served / batched engine) ---------------------------------------
 
 class _ServerConfig(C.Structure):
@@ -569,6 +603,17 @@ class Server:
         if code != 0:
             raise GpuError(code, self.lib.sankhya_pdhg_gpu_last_error().decode())
         self.pending[ticket.value] = model
+        return ticket.value
+
+    def submit_wire(self, request: WireRequest, options: Optional[Options] = None) -> int:
+        """Queues an LP read in place from its wire buffer (the server copies what it keeps)."""
+        prm = _params(options or Options(), self.lib)
+        ticket = C.c_int64()
+        code = self.lib.sankhya_pdhg_server_submit(self.handle, C.byref(request.problem),
+                                                   C.byref(prm), C.byref(ticket))
+        if code != 0:
+            raise GpuError(code, self.lib.sankhya_pdhg_gpu_last_error().decode())
+        self.pending[ticket.value] = request
         return ticket.value
 
     def step(self):
