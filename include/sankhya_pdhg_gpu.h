@@ -60,7 +60,10 @@ enum {
   SANKHYA_PDHG_ITERATION_LIMIT = 5,
   SANKHYA_PDHG_TIME_LIMIT = 6,
   SANKHYA_PDHG_NUMERICAL_ERROR = 8,
-  SANKHYA_PDHG_MODEL_ERROR = 9
+  SANKHYA_PDHG_MODEL_ERROR = 9,
+  /* a certified primal ray (the LP has no bounded optimum) without a point shown to be
+     feasible, so unboundedness is not claimed (SANKHYA_INFEASIBLE_OR_UNBOUNDED) */
+  SANKHYA_PDHG_INFEASIBLE_OR_UNBOUNDED = 10
 };
 
 /* Arithmetic of the iteration. */
@@ -189,11 +192,11 @@ typedef struct sankhya_pdhg_quality {
 } sankhya_pdhg_quality;
 
 typedef struct sankhya_pdhg_result {
-  double* col_value;   /* [n] */
+  double* col_value;   /* [n]; for UNBOUNDED a feasible point the ray starts from */
   double* row_dual;    /* [m] */
   double* col_dual;    /* [n] */
   double* farkas_dual; /* [m] filled when status is INFEASIBLE (row_dual sign) */
-  double* primal_ray;  /* [n] filled when status is UNBOUNDED */
+  double* primal_ray;  /* [n] filled when status is UNBOUNDED or INFEASIBLE_OR_UNBOUNDED */
   int32_t status;      /* SANKHYA_PDHG_* solve status */
   int32_t converged;
   int64_t iterations;  /* accepted iterations, all phases */

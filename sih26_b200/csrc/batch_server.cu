@@ -507,7 +507,11 @@ void finish_job(Server& s, Job& J, const Ctrl& c) {
   if (c.state == kInfeasible) {
     J.status = SANKHYA_PDHG_INFEASIBLE;
   } else if (c.state == kUnbounded) {
-    J.status = SANKHYA_PDHG_UNBOUNDED;
+    // a ray is certified; unboundedness also claims a feasible point for it to start from,
+    // which the batched engine does not search for: claimed only when the reported point is
+    // feasible to the project's standard (its largest bound violation, measured on the device)
+    J.status = c.primal_violation <= 1e-7 ? SANKHYA_PDHG_UNBOUNDED
+                                          : SANKHYA_PDHG_INFEASIBLE_OR_UNBOUNDED;
   } else if (c.converged) {
     J.status = standard ? SANKHYA_PDHG_OPTIMAL : SANKHYA_PDHG_FEASIBLE;
   } else {
@@ -524,6 +528,12 @@ void finish_job(Server& s, Job& J, const Ctrl& c) {
                   "unbounded: primal ray from the last step after %lld iterations, checked on "
                   "the original model",
                   c.iteration);
+  } else if (J.status == SANKHYA_PDHG_INFEASIBLE_OR_UNBOUNDED) {
+    std::snprintf(msg, sizeof msg,
+                  "primal ray from the last step after %lld iterations, checked on the original "
+                  "model; the point is not feasible (largest violation %.3e), so unboundedness "
+                  "is not claimed",
+                  c.iteration, c.primal_violation);
   } else {
     std::snprintf(msg, sizeof msg,
                   "%lld iterations and %lld restarts; relative primal %.3e, dual %.3e, gap %.3e",

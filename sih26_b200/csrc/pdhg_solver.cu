@@ -1247,6 +1247,82 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
   return SANKHYA_GPU_SUCCESS;
 }
 
+// An UNBOUNDED verdict claims two things: a feasible point, and a ray along which the
+// objective improves without limit from it (the reference's solution files carry both, and its
+// checker verifies the point before the ray, src/io/writer.cpp:195-216). The ray is certified;
+// the point the loop stopped at is an iterate running off along the ray and need not be
+// feasible. So the same constraints are solved once more with zero cost under the reference's
+// stop rule: its optimum meets the absolute standard (primal residual <= 1e-7), i.e. it is a
+// feasible point, and it is reported with the ray. If that solve proves the constraints
+// infeasible, the verdict is INFEASIBLE with its certificate; if it ends without a feasible
+// point, the verdict is INFEASIBLE_OR_UNBOUNDED: the ray alone, no point claimed.
+static void start_point_for_ray(const sankhya_pdhg_problem& prob, const sankhya_pdhg_params& prm,
+                                sankhya_pdhg_result* res) {
+  const int m = prob.num_rows, n = prob.num_cols;
+  std::vector<double> zero(n, 0.0), x(n), rd(m), cd(n), fk(m), ray(n);
+  sankhya_pdhg_problem feas = prob;
+  feas.cost = zero.data();
+  feas.maximize = 0;
+  feas.objective_offset = 0.0;
+  sankhya_pdhg_params fp = prm;
+  fp.tolerance = std::min(prm.tolerance, 1e-9);
+  fp.stop_rule = SANKHYA_PDHG_STOP_REFERENCE;
+  fp.stop_at_request = 0;
+  fp.precision = SANKHYA_PDHG_FP64;
+  fp.algorithm = SANKHYA_PDHG_ALGORITHM_HALPERN;
+  fp.detect_infeasibility = 1;
+  fp.verbose = 0;
+  fp.autotune = 0;
+  fp.profile_kernels = 0;
+  const long long cap = prm.iteration_limit < 0 ? 1000000ll : prm.iteration_limit;
+  fp.iteration_limit = std::max<long long>(1000, cap - res->iterations);
+  sankhya_pdhg_result r{};
+  r.col_value = x.data();
+  r.row_dual = rd.data();
+  r.col_dual = cd.data();
+  r.farkas_dual = fk.data();
+  r.primal_ray = ray.data();
+  const long long launches = g_launches;
+  int rc = SANKHYA_GPU_SUCCESS;
+  try {
+    rc = solve_impl(feas, fp, &r);
+  } catch (const Failure& f) {
+    rc = f.code;
+  }
+  g_launches += launches;
+  res->kernel_launches = g_launches;
+  res->iterations += r.iterations;
+  res->attempts += r.attempts;
+  res->total_seconds += r.total_seconds;
+  res->h2d_bytes += r.h2d_bytes;
+  res->d2h_bytes += r.d2h_bytes;
+  char msg[512];
+  if (rc == SANKHYA_GPU_SUCCESS && r.status == SANKHYA_PDHG_OPTIMAL) {
+    if (res->col_value) std::memcpy(res->col_value, x.data(), n * sizeof(double));
+    if (res->row_dual) std::fill(res->row_dual, res->row_dual + m, 0.0);
+    if (res->col_dual) std::memcpy(res->col_dual, prob.cost, n * sizeof(double));
+    double obj = prob.objective_offset;
+    for (int j = 0; j < n; ++j) obj += prob.cost[j] * x[j];
+    res->objective = obj;
+    res->primal_infeasibility = r.primal_infeasibility;
+    res->quality.primal_infeasibility = r.quality.primal_infeasibility;
+    res->quality.primal_infeasibility_scaled = r.quality.primal_infeasibility_scaled;
+    std::snprintf(msg, sizeof msg, "%s; the ray starts from a feasible point found by a "
+                  "zero-cost solve of the constraints in %lld iterations", res->message,
+                  static_cast<long long>(r.iterations));
+  } else if (rc == SANKHYA_GPU_SUCCESS && r.status == SANKHYA_PDHG_INFEASIBLE) {
+    res->status = SANKHYA_PDHG_INFEASIBLE;
+    if (res->farkas_dual) std::memcpy(res->farkas_dual, fk.data(), m * sizeof(double));
+    std::snprintf(msg, sizeof msg, "primal infeasible (a primal ray exists too): %s", r.message);
+  } else {
+    res->status = SANKHYA_PDHG_INFEASIBLE_OR_UNBOUNDED;
+    std::snprintf(msg, sizeof msg, "%s; no feasible point was found for the ray to start from "
+                  "(zero-cost solve: %s), so unboundedness is not claimed", res->message,
+                  rc == SANKHYA_GPU_SUCCESS ? r.message : "failed");
+  }
+  fill_message(res, msg);
+}
+
 }  // namespace sih26
 
 extern "C" {
@@ -1278,7 +1354,11 @@ int sankhya_pdhg_gpu_solve(const sankhya_pdhg_problem* problem, const sankhya_pd
   sankhya_pdhg_gpu_default_params(&defaults);
   DeviceGuard guard;
   try {
-    return solve_impl(*problem, params ? *params : defaults, result);
+    const sankhya_pdhg_params& prm = params ? *params : defaults;
+    const int rc = solve_impl(*problem, prm, result);
+    if (rc == SANKHYA_GPU_SUCCESS && result->status == SANKHYA_PDHG_UNBOUNDED)
+      start_point_for_ray(*problem, prm, result);
+    return rc;
   } catch (const Failure& f) {
     g_last_error = f.message;
     std::snprintf(result->message, sizeof result->message, "%s", f.message.c_str());

@@ -303,7 +303,7 @@ def solve_pdhg(model: LP, options: Optional[Options] = None) -> Solution:
         solve_seconds=res.total_seconds, algorithm="pdhg-gpu",
         message=res.message.decode(errors="replace"),
         farkas_dual=fk if status == "infeasible" else None,
-        primal_ray=ray if status == "unbounded" else None,
+        primal_ray=ray if status in ("unbounded", "infeasible_or_unbounded") else None,
         attempts=res.attempts, restarts=res.restarts, evaluations=res.evaluations,
         fp32_iterations=res.fp32_iterations, spectral_norm=res.spectral_norm,
         residuals={k: getattr(r, k) for k, _ in _Residuals._fields_},
@@ -312,8 +312,9 @@ def solve_pdhg(model: LP, options: Optional[Options] = None) -> Solution:
         iterate_kernel_seconds=res.iterate_kernel_seconds, iterate_launches=res.iterate_launches,
         kernel_launches=res.kernel_launches, autotuned=res.autotuned,
         schedule=tuple(res.schedule))
-    if status not in ("model_error", "infeasible", "unbounded"):
-        sol.primal_infeasibility = res.primal_infeasibility  # computed on the device
+    if status not in ("model_error", "infeasible"):
+        # computed on the device; for UNBOUNDED, of the feasible point the ray starts from
+        sol.primal_infeasibility = res.primal_infeasibility
         sol.quality = _quality(res)
     return sol
 
@@ -539,13 +540,13 @@ class _Outputs:
             solve_seconds=res.total_seconds, algorithm="pdhg-gpu-batch",
             message=res.message.decode(errors="replace"),
             farkas_dual=self.fk if status == "infeasible" else None,
-            primal_ray=self.ray if status == "unbounded" else None,
+            primal_ray=self.ray if status in ("unbounded", "infeasible_or_unbounded") else None,
             attempts=res.attempts, restarts=res.restarts, evaluations=res.evaluations,
             spectral_norm=res.spectral_norm,
             residuals={k: getattr(r, k) for k, _ in _Residuals._fields_},
             setup_seconds=res.setup_seconds, device_seconds=res.solve_seconds,
             kernel_launches=res.kernel_launches)
-        if status not in ("model_error", "infeasible", "unbounded"):
+        if status not in ("model_error", "infeasible"):
             sol.primal_infeasibility = res.primal_infeasibility  # computed on the device
             sol.quality = _quality(res)
         return sol

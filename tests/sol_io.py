@@ -136,7 +136,7 @@ def write_sol(lp, sol, path: str) -> None:
         body.append(f"begin rows {m}")
         body += [f"R{i} {_num(act[i])} {_num(sol.row_dual[i])} unknown" for i in range(m)]
         body.append("end rows")
-        if sol.status == "unbounded" and cert == "ray":
+        if sol.status in ("unbounded", "infeasible_or_unbounded") and cert == "ray":
             body.append(f"begin ray {n}")
             body += [f"C{j} {_num(v)}" for j, v in enumerate(sol.primal_ray)]
             body.append("end ray")

@@ -60,6 +60,9 @@ def test_unbounded_lp_returns_a_checked_primal_ray(lp, precision):
     assert s.primal_ray is not None and s.primal_ray.shape == (lp.num_cols,)
     ok, why = ray_ok(lp, s.primal_ray)
     assert ok, (lp.name, why)
+    # the ray starts from a feasible point (a zero-cost solve of the constraints found it)
+    assert s.primal_infeasibility <= 1e-7, (lp.name, s.primal_infeasibility)
+    assert "feasible point" in s.message
     if lp.ray_star is not None:  # the planted direction, up to scale
         r = s.primal_ray / np.max(np.abs(s.primal_ray))
         assert np.allclose(r, lp.ray_star / np.max(np.abs(lp.ray_star)), atol=1e-6)
@@ -91,6 +94,11 @@ def test_batched_engine_certifies_both_kinds_next_to_feasible_lps():
             ok, why = farkas_ok(lp, s.farkas_dual)
             assert ok, (lp.name, why)
         else:
-            assert s.status == "unbounded", (lp.name, s.status, s.message)
+            # the batched engine claims unboundedness only when its point is feasible too;
+            # otherwise the certified ray comes back alone
+            assert s.status in ("unbounded", "infeasible_or_unbounded"), (lp.name, s.status,
+                                                                          s.message)
             ok, why = ray_ok(lp, s.primal_ray)
             assert ok, (lp.name, why)
+            if s.status == "unbounded":
+                assert s.primal_infeasibility <= 1e-7, (lp.name, s.primal_infeasibility)

@@ -7,7 +7,8 @@ include/sankhya/ipm.hpp:24-34). The GPU engine drops in before that step, so its
 be a warm start the reference's interior point accepts: here the GPU stops early (an
 iteration limit, or the relative-KKT rule at a loose tolerance), the reference's polish
 (oracle/_ref: the reference's src/ipm/ipm.cpp in the polish's own steps) takes over, and the
-result must be optimal at the planted optimum with the algorithm "pdhg-gpu+ipm".
+result must be optimal at the LP's optimum (the planted one; for the maximised LP the
+reference solver's own) with the algorithm "pdhg-gpu+ipm".
 """
 import pytest
 
@@ -50,5 +51,8 @@ def test_gpu_answer_polished_by_the_reference_interior_point(name, lp, stop, pre
     assert p["status"] == "optimal", (name, p["status"], p["message"])
     assert p["algorithm"] == "pdhg-gpu+ipm"
     assert p["iterations"] == s.iterations + p["polish_iterations"]
-    want = lp.optimal_objective
+    # the optimum: the planted one, or for the maximised LP (whose planted point was built for
+    # the minimise sense) what the reference's own solve_pdhg reaches at 1e-9
+    want = (lp.optimal_objective if not lp.maximize
+            else oracle.ref_solve(lp, tolerance=1e-9, iteration_limit=1000000).objective)
     assert abs(p["objective"] - want) <= 1e-6 * max(1.0, abs(want)), (name, p["objective"], want)
