@@ -580,7 +580,8 @@ def config_legs(local, flush, sync, fp64_ref_iterations):
           (FP64 with the reference's operator, and FP32-mixed Halpern) next to the reference's
           own solve_pdhg run to the same tolerance on all host threads, for real;
       c1  the headline LP at relative KKT 1e-4 and 1e-8 (FP32-mixed Halpern; the FP64 polish
-          takes over when the FP32 level stops improving);
+          takes over when the FP32 level stops improving), and at 1e-8 with the hand-over to
+          the FP64 polish forced at 1e-6;
       c2  the block-angular LP (64 blocks of 4,000 x 10,000, 8 nonzeros per column, 2,000
           linking rows over 2 % of the columns, 30 % '<=' rows; lpgen.block_angular_planted,
           seed 2, 258,000 x 640,000, 30.7M nonzeros), FP32-mixed Halpern to 1e-6, with the
@@ -591,13 +592,13 @@ def config_legs(local, flush, sync, fp64_ref_iterations):
     peak, _ = _peaks()
     out = {}
 
-    def solve(lp, tol, precision, algorithm, profile=False):
+    def solve(lp, tol, precision, algorithm, profile=False, switch=0.0):
         flush.random_(0, 255)
         sync()
         s = pdhg.solve_pdhg(lp, pdhg.Options(
             pdhg_tolerance=tol, pdhg_stop_rule="relative_kkt", pdhg_precision=precision,
             pdhg_algorithm=algorithm, gpu_device=local, pdhg_profile_kernels=profile,
-            pdhg_autotune=True))
+            pdhg_autotune=True, pdhg_mixed_switch_tolerance=switch))
         sync()
         return s
 
@@ -632,6 +633,10 @@ def config_legs(local, flush, sync, fp64_ref_iterations):
     lp1 = make_workload()
     for tol in (1e-4, 1e-8):
         out[f"c1_{tol:g}"] = record(lp1, solve(lp1, tol, "mixed", "halpern"), tol)
+    # the anchored FP32 level reaches 1e-8 by itself; with the hand-over forced at 1e-6 the FP64
+    # polish finishes the solve, for comparison
+    out["c1_1e-08_polish_from_1e-06"] = record(lp1, solve(lp1, 1e-8, "mixed", "halpern",
+                                                          switch=1e-6), 1e-8)
     del lp1
 
     # c2: the block-angular LP
