@@ -123,8 +123,9 @@ struct Part {
 };
 
 // Unrolled loads per lane and round in a slice: every round issues this many independent
-// gathers before it sums them.
-constexpr int kSliceUnroll = 8;
+// gathers before it sums them (4 measured fastest of 4, 6, 8, 12 and 16 on the 5M-nonzero LP:
+// fewer dead slots on short rows, fewer registers).
+constexpr int kSliceUnroll = 4;
 
 template <class T>
 struct Csr {
@@ -231,6 +232,25 @@ __device__ __forceinline__ double ro(const T* p) {
   return static_cast<double>(__ldg(p));
 }
 
+
+// Streamed matrix loads of the sliced phases (the iteration kernel's): each entry is read once
+// per phase, so they bypass L1 (no_allocate) and leave it to the gathered vector.
+__device__ __forceinline__ int ld_stream(const int* p) {
+  int v;
+  asm("ld.global.nc.L1::no_allocate.b32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ float ld_stream(const float* p) {
+  float v;
+  asm("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ double ld_stream(const double* p) {
+  double v;
+  asm("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
+  return v;
+}
+
 // ---- generic fused SpMV phase ----------------------------------------------------------
 //
 // For every row r of the matrix owned by this block: s = sum_k val[k] * gather(idx[k])
@@ -267,7 +287,12 @@ __device__ __forceinline__ void run_phase(const int* __restrict__ ptr, const int
 #pragma unroll
     for (int t = 0; t < kSegment / 32; ++t) {
       const int k = sg.y + lane + 32 * t;
-      if (k < sg.z) g.add(s, ro(val + k), __ldg(idx + k));
+      if (k < sg.z) {
+        if constexpr (kSliced)
+          g.add(s, static_cast<double>(ld_stream(val + k)), ld_stream(idx + k));
+        else
+          g.add(s, ro(val + k), __ldg(idx + k));
+      }
     }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
@@ -305,42 +330,46 @@ __device__ __forceinline__ void run_phase(const int* __restrict__ ptr, const int
         prefetch_range(idx, val, __ldg(ptr + next.x), __ldg(ptr + next.y), lane);
     }
     if (kSliced && item.z < 0) {
-      // slice: lane l sums row item.x + l over the slice arrays
-      const int rows = item.y - item.x, L = -item.z;
-      const int r = item.x + lane;
-      const bool mine = lane < rows;
-      typename Epi::In in{};
-      int len = 0;
-      if (mine) {
-        in = epi.load(r);
-        len = __ldg(ptr + r + 1) - __ldg(ptr + r);
-      }
-      const int* __restrict__ si = p.sell_idx + item.w + lane;
-      const V* __restrict__ sv = static_cast<const V*>(p.sell_val) + item.w + lane;
-      double s[NV];
-#pragma unroll
-      for (int v = 0; v < NV; ++v) s[v] = 0.0;
-      for (int k0 = 0; k0 < L; k0 += kUnroll) {
-        int j[kUnroll];
-        double a[kUnroll];
-#pragma unroll
-        for (int t = 0; t < kUnroll; ++t) {
-          const bool live = mine && k0 + t < len;
-          j[t] = live ? __ldg(si + (size_t)(k0 + t) * rows) : 0;
-          a[t] = live ? ro(sv + (size_t)(k0 + t) * rows) : 0.0;
+      if constexpr (kSliced) {
+        // slice: lane l sums row item.x + l over the slice arrays
+        const int rows = item.y - item.x, L = -item.z;
+        const int r = item.x + lane;
+        const bool mine = lane < rows;
+        typename Epi::In in{};
+        int len = 0;
+        if (mine) {
+          in = epi.load(r);
+          len = __ldg(ptr + r + 1) - __ldg(ptr + r);
         }
+        const int* __restrict__ si = p.sell_idx + item.w + lane;
+        const V* __restrict__ sv = static_cast<const V*>(p.sell_val) + item.w + lane;
+        double s[NV];
 #pragma unroll
-        for (int v = 0; v < NV; ++v) {
-          double pr[kUnroll];
+        for (int v = 0; v < NV; ++v) s[v] = 0.0;
+        // values and gathered entries stay in their stored width until the multiply; a
+        // product of two FP32 numbers is exact in FP64, so the sum is the stream item's
+        for (int k0 = 0; k0 < L; k0 += kUnroll) {
+          int j[kUnroll];
+          V a[kUnroll];
 #pragma unroll
-          for (int t = 0; t < kUnroll; ++t)
-            pr[t] = (mine && k0 + t < len) ? g.product(v, a[t], j[t]) : 0.0;
+          for (int t = 0; t < kUnroll; ++t) {
+            const bool live = mine && k0 + t < len;
+            j[t] = live ? ld_stream(si + (size_t)(k0 + t) * rows) : 0;
+            a[t] = live ? ld_stream(sv + (size_t)(k0 + t) * rows) : V(0);
+          }
 #pragma unroll
-          for (int t = 0; t < kUnroll; ++t)
-            if (k0 + t < len) s[v] += pr[t];
+          for (int v = 0; v < NV; ++v) {
+            typename Gather::Raw gv[kUnroll];
+#pragma unroll
+            for (int t = 0; t < kUnroll; ++t)
+              gv[t] = (mine && k0 + t < len) ? g.raw(v, j[t]) : typename Gather::Raw(0);
+#pragma unroll
+            for (int t = 0; t < kUnroll; ++t)
+              if (k0 + t < len) s[v] += static_cast<double>(a[t]) * static_cast<double>(gv[t]);
+          }
         }
+        if (mine) epi.apply(r, s, in, acc);
       }
-      if (mine) epi.apply(r, s, in, acc);
     } else if (kSliced && item.z == 0) {
       // never produced by a sliced partition
     } else if (!kSliced && item.z == 0) {
@@ -387,7 +416,12 @@ __device__ __forceinline__ void run_phase(const int* __restrict__ ptr, const int
         if (gl == 0) in = epi.load(r);
         const int kb = __ldg(ptr + r), ke = __ldg(ptr + r + 1);
 #pragma unroll 16
-        for (int k = kb + gl; k < ke; k += lanes) g.add(s, ro(val + k), __ldg(idx + k));
+        for (int k = kb + gl; k < ke; k += lanes) {
+          if constexpr (kSliced)
+            g.add(s, static_cast<double>(ld_stream(val + k)), ld_stream(idx + k));
+          else
+            g.add(s, ro(val + k), __ldg(idx + k));
+        }
       }
       for (int off = lanes >> 1; off > 0; off >>= 1) {
 #pragma unroll
@@ -428,8 +462,10 @@ __device__ __forceinline__ void run_phase(const int* __restrict__ ptr, const int
 template <class T>
 struct Gather1 {
   const T* v;
+  using Raw = T;  // the gathered entry as stored (sliced phases)
   __device__ __forceinline__ void add(double (&s)[1], double a, int k) const { s[0] += a * ld(v + k); }
   __device__ __forceinline__ double product(int, double a, int k) const { return a * ld(v + k); }
+  __device__ __forceinline__ T raw(int, int k) const { return v[k]; }
 };
 
 template <class T, class U>
