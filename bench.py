@@ -72,11 +72,11 @@ REF_SAMPLE_ITERATIONS = 20
 # measured in the same run.
 FP64_ITERATIONS_TO_TOLERANCE = 160560
 # DRAM bytes per step of the FP32 Halpern iteration kernel on this workload, from one ncu
-# capture of a 40-step launch (dram__bytes_read.sum + dram__bytes_write.sum over 40; the
-# capture command is `ncu --section SpeedOfLight --section MemoryWorkloadAnalysis --metrics
-# dram__bytes_read.sum,dram__bytes_write.sum --clock-control none -k regex:"iterate_kernel<float"
-# -s 1 -c 1 python bench.py --profile-run single`). Recaptured whenever the kernel changes.
-ITERATE_DRAM_BYTES_PER_STEP = 71.9e6
+# capture of a 40-step launch (dram__bytes_read.sum + dram__bytes_write.sum = 1.780 + 0.044 GB
+# over 40 steps; captured with `ncu --set full --clock-control none --kernel-name-base demangled
+# -k regex:"iterate_kernel<float" -s 1 -c 1 python bench.py --profile-run single`). Recaptured
+# whenever the kernel changes.
+ITERATE_DRAM_BYTES_PER_STEP = 45.6e6
 WORKLOAD = ("powerlaw LP 200,000 x 500,000, 5,000,000 nonzeros (10 per column), rows "
             "Pareto(1.5), values N(0,1)*10^U(-2,2) per row, equality rows, 0<=x<=u, planted "
             "optimum, seed 1; relative KKT 1e-6")
@@ -369,7 +369,7 @@ def one_at_a_time(lps, local, algorithm):
 
 
 def served_leg(local, rates, seconds, chunk, algorithm="halpern", seed=5, drain_cap=15.0,
-               sample=32, max_active=1024, backlog=64, workers=8):
+               sample=64, max_active=1024, backlog=64, workers=8):
     """Poisson request streams at each rate (LPs/s) for `seconds` into a resident server.
 
     Every request is a fresh LP (lpgen.served_request: m log-uniform on [100, 50,000],

@@ -294,7 +294,12 @@ typedef struct sankhya_pdhg_server_config {
   int32_t clusters;        /* clusters for those LPs; 0 (default): chosen every round from
                               the large LPs' share of the active nonzeros (the rest of the GPU
                               runs the small LPs on single blocks) */
-  int32_t reserved[7];
+  int32_t solo_min_nnz;    /* LPs with at least this many nonzeros are solved one at a time on
+                              the whole GPU by the single-LP engine (sankhya_pdhg_gpu_solve with
+                              the LP's own params), one per step between the batched launches:
+                              at that size one LP already fills the GPU, and a cluster of 8
+                              blocks would take far longer per LP. Default 200,000; 0 = never */
+  int32_t reserved[6];
 } sankhya_pdhg_server_config;
 
 void sankhya_pdhg_server_default_config(sankhya_pdhg_server_config* config);

@@ -91,6 +91,9 @@ struct Job {
   bool model_error = false;
   std::string message;
   double submit_time = 0.0, admit_time = 0.0, finish_time = 0.0;
+  // solved alone on the whole GPU by the single-LP engine; its result as that engine filled it
+  bool solo = false;
+  sankhya_pdhg_result solo_result{};
   // result
   int status = SANKHYA_PDHG_NOT_SOLVED;
   Ctrl last{};
@@ -111,7 +114,7 @@ std::vector<T> gathered(const std::vector<T>& v, const std::vector<int>& perm) {
 
 // Host preparation of one LP (the setup half of the single-LP solve, with G = 1).
 void prepare(Job& J, const sankhya_pdhg_problem& p, const sankhya_pdhg_params& prm,
-             long long cluster_min_nnz) {
+             long long cluster_min_nnz, long long solo_min_nnz) {
   check_structure(p);
   const int m = p.num_rows, n = p.num_cols;
   J.m = m;
@@ -133,6 +136,10 @@ void prepare(Job& J, const sankhya_pdhg_problem& p, const sankhya_pdhg_params& p
   if (!why.empty()) {
     J.model_error = true;
     J.message = why;
+    return;
+  }
+  if (solo_min_nnz > 0 && J.nnz >= solo_min_nnz) {
+    J.solo = true;  // the single-LP engine prepares it itself
     return;
   }
   const double sense = p.maximize ? -1.0 : 1.0;
@@ -319,6 +326,7 @@ struct Server {
   std::vector<int> active;  // slot indices, largest LP first
   std::vector<int> active_big;  // the same for the cluster class
   std::deque<std::shared_ptr<Job>> waiting;
+  std::deque<std::shared_ptr<Job>> solo_waiting;  // LPs the single-LP engine solves alone
   std::map<int64_t, std::shared_ptr<Job>> jobs;
   int64_t next_ticket = 1;
   std::mutex mu;
@@ -548,6 +556,45 @@ void finish_job(Server& s, Job& J, const Ctrl& c) {
 
 // ---- server operations (called under the server mutex) -----------------------------------
 
+// The oldest LP routed to the single-LP engine: solved now, on the whole GPU, with its own
+// params, between two batched launches (the same stream order as the batched work, so the two
+// never share the GPU at once).
+static void run_solo(Server& s) {
+  if (s.solo_waiting.empty()) return;
+  std::shared_ptr<Job> J = s.solo_waiting.front();
+  s.solo_waiting.pop_front();
+  SIH26_SCUDA(cudaStreamSynchronize(s.stream), SANKHYA_GPU_SYNC_FAILED);
+  J->admit_time = s.now();
+  J->x.assign(J->n, 0.0);
+  J->col_dual.assign(J->n, 0.0);
+  J->row_dual.assign(J->m, 0.0);
+  J->farkas.assign(J->m, 0.0);
+  J->ray.assign(J->n, 0.0);
+  sankhya_pdhg_result& r = J->solo_result;
+  r = sankhya_pdhg_result{};
+  r.col_value = J->x.data();
+  r.row_dual = J->row_dual.data();
+  r.col_dual = J->col_dual.data();
+  r.farkas_dual = J->farkas.data();
+  r.primal_ray = J->ray.data();
+  sankhya_pdhg_params prm = J->prm;
+  prm.device = s.cfg.device;
+  const int rc = sankhya_pdhg_gpu_solve(&J->view, &prm, &r);
+  if (rc != SANKHYA_GPU_SUCCESS) {
+    r.status = SANKHYA_PDHG_NUMERICAL_ERROR;
+    std::snprintf(r.message, sizeof r.message, "single-LP engine failed: %s",
+                  sankhya_pdhg_gpu_last_error());
+  }
+  if (r.status != SANKHYA_PDHG_INFEASIBLE) J->farkas.clear();
+  if (r.status != SANKHYA_PDHG_UNBOUNDED && r.status != SANKHYA_PDHG_INFEASIBLE_OR_UNBOUNDED)
+    J->ray.clear();
+  J->status = r.status;
+  J->message = r.message;
+  J->finished = true;
+  J->finish_time = s.now();
+  s.launches += r.kernel_launches;
+}
+
 static void admit(Server& s) {
   bool changed = false;
   while (!s.waiting.empty() && !s.free_slots.empty()) {
@@ -690,6 +737,7 @@ void sankhya_pdhg_server_default_config(sankhya_pdhg_server_config* c) {
   c->chunk_attempts = 2048;
   c->cluster_min_nnz = 16384;
   c->clusters = 0;  // adaptive: the large class's share of the active nonzeros
+  c->solo_min_nnz = 200000;
 }
 
 int sankhya_pdhg_server_create(const sankhya_pdhg_server_config* config,
@@ -792,8 +840,8 @@ int sankhya_pdhg_server_submit(sankhya_pdhg_server* server, const sankhya_pdhg_p
   auto J = std::make_shared<sih26::Job>();
   try {
     J->submit_time = s->now();
-    sih26::prepare(*J, *problem, params ? *params : defaults,
-                   s->cfg.cluster_min_nnz);  // host work, outside the lock
+    sih26::prepare(*J, *problem, params ? *params : defaults, s->cfg.cluster_min_nnz,
+                   s->cfg.solo_min_nnz);  // host work, outside the lock
   } catch (const Failure& f) {
     sih26::g_last_error = f.message;
     return f.code;
@@ -809,6 +857,8 @@ int sankhya_pdhg_server_submit(sankhya_pdhg_server* server, const sankhya_pdhg_p
     J->status = SANKHYA_PDHG_MODEL_ERROR;
     J->finished = true;
     J->finish_time = J->submit_time;
+  } else if (J->solo) {
+    s->solo_waiting.push_back(J);
   } else if (J->image.size() > s->pool_bytes) {
     J->status = SANKHYA_PDHG_NUMERICAL_ERROR;
     J->message = "the LP does not fit the server's device pool";
@@ -833,12 +883,13 @@ int sankhya_pdhg_server_step(sankhya_pdhg_server* server, int32_t* active, int32
     sih26::admit(*s);
     sih26::run_round(*s);
     sih26::admit(*s);
+    sih26::run_solo(*s);
   } catch (const Failure& f) {
     sih26::g_last_error = f.message;
     return f.code;
   }
   if (active) *active = static_cast<int32_t>(s->active.size() + s->active_big.size());
-  if (waiting) *waiting = static_cast<int32_t>(s->waiting.size());
+  if (waiting) *waiting = static_cast<int32_t>(s->waiting.size() + s->solo_waiting.size());
   if (finished) {
     int32_t k = 0;
     for (auto& kv : s->jobs) k += kv.second->finished ? 1 : 0;
@@ -862,6 +913,26 @@ int sankhya_pdhg_server_result(sankhya_pdhg_server* server, int64_t ticket,
   }
   sih26::Job& J = *it->second;
   if (!J.finished) return SANKHYA_GPU_NOT_READY;
+  if (J.solo) {
+    // the single-LP engine's own result, with the caller's arrays and the served times
+    sankhya_pdhg_result out = J.solo_result;
+    out.col_value = r->col_value;
+    out.row_dual = r->row_dual;
+    out.col_dual = r->col_dual;
+    out.farkas_dual = r->farkas_dual;
+    out.primal_ray = r->primal_ray;
+    if (out.col_value && !J.x.empty()) std::memcpy(out.col_value, J.x.data(), J.n * 8);
+    if (out.col_dual && !J.col_dual.empty()) std::memcpy(out.col_dual, J.col_dual.data(), J.n * 8);
+    if (out.row_dual && !J.row_dual.empty()) std::memcpy(out.row_dual, J.row_dual.data(), J.m * 8);
+    if (out.farkas_dual && !J.farkas.empty()) std::memcpy(out.farkas_dual, J.farkas.data(), J.m * 8);
+    if (out.primal_ray && !J.ray.empty()) std::memcpy(out.primal_ray, J.ray.data(), J.n * 8);
+    out.setup_seconds = std::max(0.0, J.admit_time - J.submit_time);
+    out.solve_seconds = std::max(0.0, J.finish_time - J.admit_time);
+    out.total_seconds = std::max(0.0, J.finish_time - J.submit_time);
+    *r = out;
+    s->jobs.erase(it);
+    return SANKHYA_GPU_SUCCESS;
+  }
   r->status = J.status;
   const sih26::Ctrl& c = J.last;
   r->converged = c.converged;

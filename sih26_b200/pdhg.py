@@ -458,7 +458,8 @@ class _ServerConfig(C.Structure):
     _fields_ = [("device", C.c_int32), ("memory_fraction", C.c_double),
                 ("pool_bytes", C.c_int64), ("max_active", C.c_int32),
                 ("chunk_attempts", C.c_int64), ("cluster_min_nnz", C.c_int64),
-                ("clusters", C.c_int32), ("reserved", C.c_int32 * 7)]
+                ("clusters", C.c_int32), ("solo_min_nnz", C.c_int32),
+                ("reserved", C.c_int32 * 6)]
 
 
 def _bind_server(lib):
@@ -577,11 +578,13 @@ class Server:
     step() admits what fits and runs one launch over every active LP, result() collects.
     LPs with at least `cluster_min_nnz` nonzeros run on an 8-block thread-block cluster
     (`clusters` of them; 0 = chosen every round from the large LPs' share of the active
-    nonzeros), the others on one block each."""
+    nonzeros), the others on one block each; LPs with at least `solo_min_nnz` nonzeros are
+    solved one per step on the whole GPU by the single-LP engine."""
 
     def __init__(self, device: int = 0, memory_fraction: float = 0.8, pool_bytes: int = 0,
                  max_active: int = 4096, chunk_attempts: int = 2048,
-                 cluster_min_nnz: int = 16384, clusters: int = 0):
+                 cluster_min_nnz: int = 16384, clusters: int = 0,
+                 solo_min_nnz: int = 200000):
         self.lib = load_library()
         _bind_server(self.lib)
         cfg = _ServerConfig()
@@ -589,6 +592,7 @@ class Server:
         cfg.device, cfg.memory_fraction, cfg.pool_bytes = device, memory_fraction, pool_bytes
         cfg.max_active, cfg.chunk_attempts = max_active, chunk_attempts
         cfg.cluster_min_nnz, cfg.clusters = cluster_min_nnz, clusters
+        cfg.solo_min_nnz = solo_min_nnz
         self.handle = C.c_void_p()
         code = self.lib.sankhya_pdhg_server_create(C.byref(cfg), C.byref(self.handle))
         if code != 0:
