@@ -369,7 +369,7 @@ def one_at_a_time(lps, local, algorithm):
 
 
 def served_leg(local, rates, seconds, chunk, algorithm="halpern", seed=5, drain_cap=15.0,
-               sample=64, max_active=1024, backlog=64, workers=8):
+               sample=64, max_active=1024, backlog=64, workers=8, solo_min_nnz=200000):
     """Poisson request streams at each rate (LPs/s) for `seconds` into a resident server.
 
     Every request is a fresh LP (lpgen.served_request: m log-uniform on [100, 50,000],
@@ -424,7 +424,8 @@ def served_leg(local, rates, seconds, chunk, algorithm="halpern", seed=5, drain_
             gen_f, sub_f, tickets = {}, {}, {}
             latency, status, kkt, size = {}, {}, {}, {}
             next_gen = next_sub = 0
-            with pdhg.Server(device=local, chunk_attempts=chunk, max_active=max_active) as srv, \
+            with pdhg.Server(device=local, chunk_attempts=chunk, max_active=max_active,
+                             solo_min_nnz=solo_min_nnz) as srv, \
                     cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
                 srv.solve_all([base[0]], opts)  # warm-up
                 waiting = 0
@@ -487,7 +488,7 @@ def served_leg(local, rates, seconds, chunk, algorithm="halpern", seed=5, drain_
                 "certified_infeasible": sum(1 for v in status.values() if v == "infeasible"),
                 "value": served_rate, "unit": "LPs/s", "span_s": span,
                 "latency_s": _percentiles(ages), "latency_censored": bool(unfinished),
-                "chunk_attempts": chunk, "max_active": max_active,
+                "chunk_attempts": chunk, "max_active": max_active, "solo_min_nnz": solo_min_nnz,
                 "precision": "fp64", "algorithm": algorithm,
                 "one_at_a_time_fp64": base_rate,
                 "speedup_vs_one_at_a_time": (served_rate / base_rate) if served_rate else None,
@@ -831,7 +832,8 @@ def run_ours(args):
     if rank == 0 and not args.no_served:
         rates = [float(r) for r in args.served_rates.split(",") if r]
         served = served_leg(local, rates, args.served_seconds, args.served_chunk,
-                            args.algorithm)
+                            args.algorithm, max_active=args.served_max_active,
+                            solo_min_nnz=args.served_solo_nnz)
     qp = qp_leg(local) if rank == 0 and not args.no_qp else None
     if rank == 0:
         line = {
@@ -921,6 +923,10 @@ def main():
                     help="arrival window per rate, s (the survey's study is 60)")
     ap.add_argument("--served-chunk", type=int, default=512,
                     help="attempts per LP per server launch")
+    ap.add_argument("--served-max-active", type=int, default=1024,
+                    help="LP slots of the server in the served leg")
+    ap.add_argument("--served-solo-nnz", type=int, default=200000,
+                    help="served LPs from this many nonzeros go to the single-LP engine (0: never)")
     ap.add_argument("--profile-run", choices=["single", "batch"], default=None,
                     help="a bounded run for an ncu capture (prints no bench line)")
     args = ap.parse_args()

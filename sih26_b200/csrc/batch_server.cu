@@ -333,6 +333,7 @@ struct Server {
   Clock::time_point t0 = Clock::now();
   long long launches = 0;
   unsigned long long device_clock0 = 0;
+  double last_round_seconds = 0.0;  // wall time of the last batched launch
 
   double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
 };
@@ -556,11 +557,24 @@ void finish_job(Server& s, Job& J, const Ctrl& c) {
 
 // ---- server operations (called under the server mutex) -----------------------------------
 
-// The oldest LP routed to the single-LP engine: solved now, on the whole GPU, with its own
-// params, between two batched launches (the same stream order as the batched work, so the two
-// never share the GPU at once).
+// LPs routed to the single-LP engine, oldest first, each on the whole GPU with its own params,
+// between two batched launches (in stream order with the batched work, so the two never share
+// the GPU at once): at least one per step and then as many as fit in the time the last batched
+// launch took, so either class gets about half of the GPU while both have work; with no
+// batched work, up to 16 per step.
+static void solve_one_solo(Server& s);
+
 static void run_solo(Server& s) {
-  if (s.solo_waiting.empty()) return;
+  const bool batch_idle = s.active.empty() && s.active_big.empty() && s.waiting.empty();
+  const double budget = batch_idle ? 1e30 : s.last_round_seconds;
+  const double start = s.now();
+  for (int k = 0; k < 16 && !s.solo_waiting.empty(); ++k) {
+    if (k > 0 && s.now() - start >= budget) break;
+    solve_one_solo(s);
+  }
+}
+
+static void solve_one_solo(Server& s) {
   std::shared_ptr<Job> J = s.solo_waiting.front();
   s.solo_waiting.pop_front();
   SIH26_SCUDA(cudaStreamSynchronize(s.stream), SANKHYA_GPU_SYNC_FAILED);
@@ -706,6 +720,7 @@ static void run_round(Server& s) {
                               s.stream), SANKHYA_GPU_COPY_FAILED);
   SIH26_SCUDA(cudaMemcpyAsync(s.d_count[1], &s.h_counts[1], sizeof(int), cudaMemcpyHostToDevice,
                               s.stream), SANKHYA_GPU_COPY_FAILED);
+  const double started = s.now();
   SIH26_SCUDA(cudaGraphLaunch(s.graph, s.stream), SANKHYA_GPU_KERNEL_LAUNCH_FAILED);
   ++s.launches;
   if (c0)
@@ -715,6 +730,7 @@ static void run_round(Server& s) {
     SIH26_SCUDA(cudaMemcpyAsync(s.h_compact2, s.d_compact2, c1 * sizeof(Ctrl),
                                 cudaMemcpyDeviceToHost, s.stream), SANKHYA_GPU_COPY_FAILED);
   SIH26_SCUDA(cudaStreamSynchronize(s.stream), SANKHYA_GPU_SYNC_FAILED);
+  s.last_round_seconds = s.now() - started;
   s.active = settle(s, s.active, s.h_compact);
   s.active_big = settle(s, s.active_big, s.h_compact2);
 }
