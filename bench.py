@@ -27,7 +27,7 @@ FP64, unscaled) through the library's C ABI.
           the same LPs solved one at a time by the plain FP64 single-LP path (a sample of every
           8th LP) for the LPs/s ratio. Under torchrun the 512 LPs are sharded by nonzeros
           (sih26_b200.shard) and the time is the maximum over ranks.
-  served  Poisson request streams at 200, 1,000 and 5,000 LPs/s for 30 s each (--served-seconds 60
+  served  Poisson request streams at 200, 1,000 and 5,000 LPs/s for 20 s each (--served-seconds 60
           for the survey's full windows), every request a fresh LP of the served family (m
           log-uniform on [100, 50,000], 10 % infeasible; lpgen.served_request), into a resident
           server that admits requests between launches of its persistent kernels (continuous
@@ -65,12 +65,12 @@ SEED = 1
 METRIC = "time-to-rel-KKT 1e-6 (s)"
 REF_SAMPLE_ITERATIONS = 20
 # Iterations the reference's own operator needs on this workload to reach relative KKT 1e-6 in
-# FP64: 160,560, measured by this bench's FP64 reference-operator leg on a B200 (that leg runs
+# FP64: 169,080, measured by this bench's FP64 reference-operator leg on a B200 (that leg runs
 # the reference's algorithm, src/pdhg/pdhg.cpp:383-644, in FP64; the CPU reference cannot be
 # run to tolerance here, it would take over an hour). The reference arm extrapolates its timed
 # sample to this count; the main arm uses the count its own FP64 reference-operator leg
 # measured in the same run.
-FP64_ITERATIONS_TO_TOLERANCE = 160560
+FP64_ITERATIONS_TO_TOLERANCE = 169080
 # DRAM bytes per step of the FP32 Halpern iteration kernel on this workload, from one ncu
 # capture of a 40-step launch (dram__bytes_read.sum + dram__bytes_write.sum = 1.780 + 0.044 GB
 # over 40 steps; captured with `ncu --set full --clock-control none --kernel-name-base demangled
@@ -919,7 +919,7 @@ def main():
                     help="skip the 2,000 x 5,000, block-angular and 1e-4 / 1e-8 legs")
     ap.add_argument("--served-rates", default="200,1000,5000",
                     help="Poisson rates, LPs/s, comma-separated")
-    ap.add_argument("--served-seconds", type=float, default=30.0,
+    ap.add_argument("--served-seconds", type=float, default=20.0,
                     help="arrival window per rate, s (the survey's study is 60)")
     ap.add_argument("--served-chunk", type=int, default=512,
                     help="attempts per LP per server launch")
