@@ -352,24 +352,29 @@ def _size_class(m):
 
 
 def one_at_a_time(lps, local, algorithm):
-    """LPs/s of the plain FP64 single-LP path, one LP after another (after one warm-up), and
-    the seconds each LP took."""
+    """LPs/s of the plain FP64 single-LP path, one LP after another (after one warm-up; the
+    faster of two passes), and the seconds each LP took."""
     from sih26_b200 import pdhg
 
     one = pdhg.Options(pdhg_tolerance=TOLERANCE, pdhg_stop_rule="relative_kkt",
                        pdhg_precision="fp64", gpu_device=local, pdhg_algorithm=algorithm)
     pdhg.solve_pdhg(lps[0], one)
-    each = []
-    t0 = time.perf_counter()
-    for lp in lps:
-        t1 = time.perf_counter()
-        pdhg.solve_pdhg(lp, one)
-        each.append(time.perf_counter() - t1)
-    return len(lps) / (time.perf_counter() - t0), each
+    best = None
+    for _ in range(2):  # the faster of two passes: the host's load varies between them
+        each = []
+        t0 = time.perf_counter()
+        for lp in lps:
+            t1 = time.perf_counter()
+            pdhg.solve_pdhg(lp, one)
+            each.append(time.perf_counter() - t1)
+        total = time.perf_counter() - t0
+        if best is None or total < best[0]:
+            best = (total, each)
+    return len(lps) / best[0], best[1]
 
 
 def served_leg(local, rates, seconds, chunk, algorithm="halpern", seed=5, drain_cap=15.0,
-               sample=64, max_active=1024, backlog=64, workers=8, solo_min_nnz=200000):
+               sample=64, max_active=1024, backlog=64, workers=8, solo_min_nnz=0):
     """Poisson request streams at each rate (LPs/s) for `seconds` into a resident server.
 
     Every request is a fresh LP (lpgen.served_request: m log-uniform on [100, 50,000],
@@ -925,7 +930,7 @@ def main():
                     help="attempts per LP per server launch")
     ap.add_argument("--served-max-active", type=int, default=1024,
                     help="LP slots of the server in the served leg")
-    ap.add_argument("--served-solo-nnz", type=int, default=200000,
+    ap.add_argument("--served-solo-nnz", type=int, default=0,
                     help="served LPs from this many nonzeros go to the single-LP engine (0: never)")
     ap.add_argument("--profile-run", choices=["single", "batch"], default=None,
                     help="a bounded run for an ncu capture (prints no bench line)")

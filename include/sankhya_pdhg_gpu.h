@@ -296,9 +296,9 @@ typedef struct sankhya_pdhg_server_config {
                               runs the small LPs on single blocks) */
   int32_t solo_min_nnz;    /* LPs with at least this many nonzeros are solved one at a time on
                               the whole GPU by the single-LP engine (sankhya_pdhg_gpu_solve with
-                              the LP's own params), one per step between the batched launches:
-                              at that size one LP already fills the GPU, and a cluster of 8
-                              blocks would take far longer per LP. Default 200,000; 0 = never */
+                              the LP's own params) between the batched launches, for as long as
+                              the last batched launch took; 0 (default) = never: on the served
+                              family the batched engine's clusters served the large LPs faster */
   int32_t reserved[6];
 } sankhya_pdhg_server_config;
 

@@ -753,7 +753,7 @@ void sankhya_pdhg_server_default_config(sankhya_pdhg_server_config* c) {
   c->chunk_attempts = 2048;
   c->cluster_min_nnz = 16384;
   c->clusters = 0;  // adaptive: the large class's share of the active nonzeros
-  c->solo_min_nnz = 200000;
+  c->solo_min_nnz = 0;  // never: routing measured slower on the served family
 }
 
 int sankhya_pdhg_server_create(const sankhya_pdhg_server_config* config,

@@ -584,7 +584,7 @@ class Server:
     def __init__(self, device: int = 0, memory_fraction: float = 0.8, pool_bytes: int = 0,
                  max_active: int = 4096, chunk_attempts: int = 2048,
                  cluster_min_nnz: int = 16384, clusters: int = 0,
-                 solo_min_nnz: int = 200000):
+                 solo_min_nnz: int = 0):
         self.lib = load_library()
         _bind_server(self.lib)
         cfg = _ServerConfig()
