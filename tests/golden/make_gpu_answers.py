@@ -51,7 +51,7 @@ def cases():
         base = lpgen.uniform_planted(60, 150, 4, seed=seed)
         out.append((f"infeasible_{seed}", lpgen.make_infeasible(base, rng), "fp64"))
         out.append((f"unbounded_{seed}", lpgen.make_unbounded(base, rng), "fp64"))
-    batch = lpgen.uneven_batch(count=40, m_lo=50, m_hi=400, infeasible_fraction=0.1, seed=8)
+    batch = lpgen.uneven_batch(count=40, m_lo=50, m_hi=200, infeasible_fraction=0.1, seed=8)
     for k, lp in enumerate(batch):
         out.append((f"batch_{k:02d}", lp, "batch"))
     return out
