@@ -732,7 +732,8 @@ def _brief_served(v):
             "one_at_a_time_fp64", "chunk_attempts", "by_size")
     out = {k: v[k] for k in keep if k in v}
     out.update({"p50_s": lat["p50"], "p99_s": lat["p99"], "p99.9_s": lat["p99.9"],
-                "latency_censored": v.get("latency_censored")})
+                "latency_censored": v.get("latency_censored"),
+                "cpu_reference": (v.get("cpu_reference") or {}).get("value")})
     return out
 
 
