@@ -415,12 +415,34 @@ __device__ __forceinline__ void run_phase(const int* __restrict__ ptr, const int
       if (valid) {
         if (gl == 0) in = epi.load(r);
         const int kb = __ldg(ptr + r), ke = __ldg(ptr + r + 1);
+        if constexpr (kSliced) {
+          // the lane's entries kb + gl, kb + gl + lanes, ... in rounds of kUnroll independent
+          // raw-width gathers, summed in that same order (so the sums are those of the plain
+          // loop below, bit for bit)
+          for (int k0 = kb + gl; k0 < ke; k0 += lanes * kUnroll) {
+            int j[kUnroll];
+            V a[kUnroll];
+#pragma unroll
+            for (int t = 0; t < kUnroll; ++t) {
+              const int k = k0 + t * lanes;
+              j[t] = k < ke ? ld_stream(idx + k) : 0;
+              a[t] = k < ke ? ld_stream(val + k) : V(0);
+            }
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+              typename Gather::Raw gv[kUnroll];
+#pragma unroll
+              for (int t = 0; t < kUnroll; ++t)
+                gv[t] = k0 + t * lanes < ke ? g.raw(v, j[t]) : typename Gather::Raw(0);
+#pragma unroll
+              for (int t = 0; t < kUnroll; ++t)
+                if (k0 + t * lanes < ke)
+                  s[v] += static_cast<double>(a[t]) * static_cast<double>(gv[t]);
+            }
+          }
+        } else {
 #pragma unroll 16
-        for (int k = kb + gl; k < ke; k += lanes) {
-          if constexpr (kSliced)
-            g.add(s, static_cast<double>(ld_stream(val + k)), ld_stream(idx + k));
-          else
-            g.add(s, ro(val + k), __ldg(idx + k));
+          for (int k = kb + gl; k < ke; k += lanes) g.add(s, ro(val + k), __ldg(idx + k));
         }
       }
       for (int off = lanes >> 1; off > 0; off >>= 1) {
