@@ -39,6 +39,7 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 
 #include "device_common.cuh"
 
@@ -141,6 +142,7 @@ struct Prob {
   Csr<T> A, AT;
   Part pa, pat;
   Part pai, pati;  // the iteration kernel's sliced partitions (slice values of type T)
+  Part pae, pate;  // the evaluation's: the same slices with FP64 values (the FP64 level's)
   // scaled problem, permuted (src/la/scaling.hpp:36-58)
   const T* c;
   const T* cl;
@@ -181,10 +183,14 @@ struct State {
   double* axr;    // [m] A xr (the Halpern operator needs it on the FP64 level too)
   T* xt;          // Halpern: the PDHG output T(z_k), primal part (a delta on the FP32 level)
   T* yt;          // and dual part
-  double* xfull;  // [n] evaluation scratch: xr + dx
+  double* xfull;  // [n] evaluation scratch (batched engine): xr + dx
   double* yfull;  // [m] yr + dy
   double* xavg;
   double* yavg;
+  // single-LP evaluation: both candidates of every column / row side by side (the current
+  // point in FP64, then the second candidate), so one 16-byte gather reads both
+  double2* xc;  // [n]
+  double2* yc;  // [m]
   double* best_x;  // scaled, FP64
   double* best_y;
   double* cert_row;  // [m] Farkas candidate (reference sign, max-normalised), permuted
@@ -250,6 +256,12 @@ __device__ __forceinline__ double ld_stream(const double* p) {
   asm("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
   return v;
 }
+
+// Whether a gather reads its NV vectors with one load (GatherPair).
+template <class G, class = void>
+struct paired_gather : std::false_type {};
+template <class G>
+struct paired_gather<G, std::void_t<decltype(G::kPaired)>> : std::bool_constant<G::kPaired> {};
 
 // ---- generic fused SpMV phase ----------------------------------------------------------
 //
@@ -357,15 +369,29 @@ __device__ __forceinline__ void run_phase(const int* __restrict__ ptr, const int
             j[t] = live ? ld_stream(si + (size_t)(k0 + t) * rows) : 0;
             a[t] = live ? ld_stream(sv + (size_t)(k0 + t) * rows) : V(0);
           }
-#pragma unroll
-          for (int v = 0; v < NV; ++v) {
-            typename Gather::Raw gv[kUnroll];
-#pragma unroll
-            for (int t = 0; t < kUnroll; ++t)
-              gv[t] = (mine && k0 + t < len) ? g.raw(v, j[t]) : typename Gather::Raw(0);
+          if constexpr (paired_gather<Gather>::value) {
+            static_assert(NV == 2, "a paired gather reads two vectors");
+            double2 gv[kUnroll];
 #pragma unroll
             for (int t = 0; t < kUnroll; ++t)
-              if (k0 + t < len) s[v] += static_cast<double>(a[t]) * static_cast<double>(gv[t]);
+              gv[t] = (mine && k0 + t < len) ? g.pair(j[t]) : make_double2(0.0, 0.0);
+#pragma unroll
+            for (int t = 0; t < kUnroll; ++t)
+              if (k0 + t < len) {
+                s[0] += static_cast<double>(a[t]) * gv[t].x;
+                s[1] += static_cast<double>(a[t]) * gv[t].y;
+              }
+          } else {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+              typename Gather::Raw gv[kUnroll];
+#pragma unroll
+              for (int t = 0; t < kUnroll; ++t)
+                gv[t] = (mine && k0 + t < len) ? g.raw(v, j[t]) : typename Gather::Raw(0);
+#pragma unroll
+              for (int t = 0; t < kUnroll; ++t)
+                if (k0 + t < len) s[v] += static_cast<double>(a[t]) * static_cast<double>(gv[t]);
+            }
           }
         }
         if (mine) epi.apply(r, s, in, acc);
@@ -428,16 +454,29 @@ __device__ __forceinline__ void run_phase(const int* __restrict__ ptr, const int
               j[t] = k < ke ? ld_stream(idx + k) : 0;
               a[t] = k < ke ? ld_stream(val + k) : V(0);
             }
-#pragma unroll
-            for (int v = 0; v < NV; ++v) {
-              typename Gather::Raw gv[kUnroll];
-#pragma unroll
-              for (int t = 0; t < kUnroll; ++t)
-                gv[t] = k0 + t * lanes < ke ? g.raw(v, j[t]) : typename Gather::Raw(0);
+            if constexpr (paired_gather<Gather>::value) {
+              double2 gv[kUnroll];
 #pragma unroll
               for (int t = 0; t < kUnroll; ++t)
-                if (k0 + t * lanes < ke)
-                  s[v] += static_cast<double>(a[t]) * static_cast<double>(gv[t]);
+                gv[t] = k0 + t * lanes < ke ? g.pair(j[t]) : make_double2(0.0, 0.0);
+#pragma unroll
+              for (int t = 0; t < kUnroll; ++t)
+                if (k0 + t * lanes < ke) {
+                  s[0] += static_cast<double>(a[t]) * gv[t].x;
+                  s[1] += static_cast<double>(a[t]) * gv[t].y;
+                }
+            } else {
+#pragma unroll
+              for (int v = 0; v < NV; ++v) {
+                typename Gather::Raw gv[kUnroll];
+#pragma unroll
+                for (int t = 0; t < kUnroll; ++t)
+                  gv[t] = k0 + t * lanes < ke ? g.raw(v, j[t]) : typename Gather::Raw(0);
+#pragma unroll
+                for (int t = 0; t < kUnroll; ++t)
+                  if (k0 + t * lanes < ke)
+                    s[v] += static_cast<double>(a[t]) * static_cast<double>(gv[t]);
+              }
             }
           }
         } else {
@@ -502,6 +541,24 @@ struct Gather2 {
     return which == 0 ? a * ld(v0 + k) : a * ld(v1 + k);
   }
 };
+
+// Two FP64 vectors stored side by side: one 16-byte load gathers both entries. Each sum is
+// formed in the same order as with two separate gathers (Gather2), so the sums are the same.
+struct GatherPair {
+  const double2* v;
+  static constexpr bool kPaired = true;
+  __device__ __forceinline__ void add(double (&s)[2], double a, int k) const {
+    const double2 t = v[k];
+    s[0] += a * t.x;
+    s[1] += a * t.y;
+  }
+  __device__ __forceinline__ double product(int which, double a, int k) const {
+    const double2 t = v[k];
+    return a * (which == 0 ? t.x : t.y);
+  }
+  __device__ __forceinline__ double2 pair(int k) const { return v[k]; }
+};
+
 
 // ---- epilogues of the iteration ---------------------------------------------------------
 
@@ -1230,6 +1287,7 @@ struct RowEval {
   const double* yavg;  // candidate 1 (scaled)
   const double* ycand; // when non-null: candidate 0 in FP64 (the report)
   double* y_out;       // report: unscaled multipliers
+  const double2* pair; // when non-null: both candidates side by side (State::yc)
   struct In {
     double dr, lo, hi, y0, y1;
   };
@@ -1238,8 +1296,14 @@ struct RowEval {
     v.dr = __ldg(dr + i);
     v.lo = __ldg(rl0 + i);
     v.hi = __ldg(ru0 + i);
-    v.y0 = ycand ? __ldcg(ycand + i) : ld(y + i);
-    v.y1 = NC > 1 ? __ldcg(yavg + i) : 0.0;
+    if (pair) {
+      const double2 t = __ldcg(pair + i);
+      v.y0 = t.x;
+      v.y1 = t.y;
+    } else {
+      v.y0 = ycand ? __ldcg(ycand + i) : ld(y + i);
+      v.y1 = NC > 1 ? __ldcg(yavg + i) : 0.0;
+    }
     return v;
   }
   __device__ __forceinline__ void apply(int i, const double (&s)[NC], const In& v,
@@ -1283,6 +1347,7 @@ struct ColEval {
   const double* xcand;  // report: candidate 0 in FP64
   double* x_out;        // report outputs (unscaled, permuted order)
   double* reduced_out;
+  const double2* pair;  // when non-null: both candidates side by side (State::xc)
   struct In {
     double dc, lo, hi, c, x0, x1;
   };
@@ -1292,8 +1357,14 @@ struct ColEval {
     v.lo = __ldg(cl0 + j);
     v.hi = __ldg(cu0 + j);
     v.c = __ldg(c0 + j);
-    v.x0 = xcand ? __ldcg(xcand + j) : ld(x + j);
-    v.x1 = NC > 1 ? __ldcg(xavg + j) : 0.0;
+    if (pair) {
+      const double2 t = __ldcg(pair + j);
+      v.x0 = t.x;
+      v.x1 = t.y;
+    } else {
+      v.x0 = xcand ? __ldcg(xcand + j) : ld(x + j);
+      v.x1 = NC > 1 ? __ldcg(xavg + j) : 0.0;
+    }
     return v;
   }
   __device__ __forceinline__ void apply(int j, const double (&s)[NC], const In& v,
@@ -1462,11 +1533,10 @@ __global__ void __launch_bounds__(kThreads, 2) evaluate_kernel(Prob<T> P, State<
     double d;
     if constexpr (kDelta<T>) {
       const double r = S.xr[j];
-      S.xfull[j] = r + xo;
-      S.xavg[j] = has_average ? r + (halpern ? ld(S.xt + j) : xs / count) : 0.0;
+      S.xc[j] = make_double2(r + xo, has_average ? r + (halpern ? ld(S.xt + j) : xs / count) : 0.0);
       d = xo;
     } else {
-      S.xavg[j] = has_average ? (halpern ? ld(S.xt + j) : xs / count) : 0.0;
+      S.xc[j] = make_double2(xo, has_average ? (halpern ? ld(S.xt + j) : xs / count) : 0.0);
       d = xo - ld(S.xr + j);
     }
     acc1[0] += d * d;
@@ -1482,11 +1552,10 @@ __global__ void __launch_bounds__(kThreads, 2) evaluate_kernel(Prob<T> P, State<
     double d;
     if constexpr (kDelta<T>) {
       const double r = S.yr[i];
-      S.yfull[i] = r + yo;
-      S.yavg[i] = has_average ? r + (halpern ? ld(S.yt + i) : ys / count) : 0.0;
+      S.yc[i] = make_double2(r + yo, has_average ? r + (halpern ? ld(S.yt + i) : ys / count) : 0.0);
       d = yo;
     } else {
-      S.yavg[i] = has_average ? (halpern ? ld(S.yt + i) : ys / count) : 0.0;
+      S.yc[i] = make_double2(yo, has_average ? (halpern ? ld(S.yt + i) : ys / count) : 0.0);
       d = yo - ld(S.yr + i);
     }
     acc1[1] += d * d;
@@ -1501,25 +1570,17 @@ __global__ void __launch_bounds__(kThreads, 2) evaluate_kernel(Prob<T> P, State<
   if (!grid_barrier(S.bar)) goto device_error;
 
   {
-    // E2: both candidates' residual terms in one pass over each matrix (FP64 values).
+    // E2: both candidates' residual terms in one pass over each matrix (FP64 values, the
+    // FP64 slices): one 16-byte gather per entry reads both candidates.
     double acc[kEvalSlots];
 #pragma unroll
     for (int s = 0; s < kEvalSlots; ++s) acc[s] = 0.0;
-    if constexpr (kDelta<T>) {
-      RowEval<T, 2> re{P.dr, P.rl0, P.ru0, nullptr, S.yavg, S.yfull, nullptr};
-      run_phase<2, kEvalSlots>(P.A.ptr, P.A.idx, P.A.val64, P.pa,
-                               Gather2<double, double>{S.xfull, S.xavg}, re, acc, stream);
-      ColEval<T, 2> ce{P.dc, P.cl0, P.cu0, P.c0, nullptr, S.xavg, S.xfull, nullptr, nullptr};
-      run_phase<2, kEvalSlots>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pat,
-                               Gather2<double, double>{S.yfull, S.yavg}, ce, acc, stream);
-    } else {
-      RowEval<T, 2> re{P.dr, P.rl0, P.ru0, S.y[cur], S.yavg, nullptr, nullptr};
-      run_phase<2, kEvalSlots>(P.A.ptr, P.A.idx, P.A.val64, P.pa,
-                               Gather2<T, double>{S.x[cur], S.xavg}, re, acc, stream);
-      ColEval<T, 2> ce{P.dc, P.cl0, P.cu0, P.c0, S.x[cur], S.xavg, nullptr, nullptr, nullptr};
-      run_phase<2, kEvalSlots>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pat,
-                               Gather2<T, double>{S.y[cur], S.yavg}, ce, acc, stream);
-    }
+    RowEval<T, 2> re{P.dr, P.rl0, P.ru0, nullptr, nullptr, nullptr, nullptr, S.yc};
+    run_phase<2, kEvalSlots, false, true>(P.A.ptr, P.A.idx, P.A.val64, P.pae, GatherPair{S.xc},
+                                          re, acc, stream);
+    ColEval<T, 2> ce{P.dc, P.cl0, P.cu0, P.c0, nullptr, nullptr, nullptr, nullptr, nullptr, S.xc};
+    run_phase<2, kEvalSlots, false, true>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pate,
+                                          GatherPair{S.yc}, ce, acc, stream);
     block_reduce<kEvalSlots, kEvalMaxMask>(acc, sh);
     write_partials(part, 2, acc, kEvalSlots);
     if (test_cert) {
@@ -1593,8 +1654,9 @@ __global__ void __launch_bounds__(kThreads, 2) evaluate_kernel(Prob<T> P, State<
   // E3: keep the best point (scaled, FP64) and reset the average at a restart.
   if (flags[0] || flags[1]) {
     for (int j = gt; j < P.n; j += stride) {
-      const double xo = kDelta<T> ? S.xfull[j] : ld(S.x[cur] + j);
-      if (flags[0]) S.best_x[j] = flags[2] ? S.xavg[j] : xo;
+      const double2 xcj = S.xc[j];
+      const double xo = xcj.x;
+      if (flags[0]) S.best_x[j] = flags[2] ? xcj.y : xo;
       if (flags[1]) {
         S.xr[j] = xo;
         S.xsum[j] = 0.0;
@@ -1602,8 +1664,9 @@ __global__ void __launch_bounds__(kThreads, 2) evaluate_kernel(Prob<T> P, State<
       }
     }
     for (int i = gt; i < P.m; i += stride) {
-      const double yo = kDelta<T> ? S.yfull[i] : ld(S.y[cur] + i);
-      if (flags[0]) S.best_y[i] = flags[2] ? S.yavg[i] : yo;
+      const double2 yci = S.yc[i];
+      const double yo = yci.x;
+      if (flags[0]) S.best_y[i] = flags[2] ? yci.y : yo;
       if (flags[1]) {
         S.yr[i] = yo;
         S.ysum[i] = 0.0;

@@ -269,8 +269,8 @@ static Level<T> make_level(Arena& a, const Common& cm, const PermutedLp& q,
   S.ysum = a.zeros<double>(m);
   S.xr = a.zeros<double>(n);
   S.yr = a.zeros<double>(m);
-  S.xavg = a.zeros<double>(n);
-  S.yavg = a.zeros<double>(m);
+  S.xc = a.zeros<double2>(n);
+  S.yc = a.zeros<double2>(m);
   S.axr = a.zeros<double>(m);
   S.xt = a.zeros<T>(n);
   S.yt = a.zeros<T>(m);
@@ -278,8 +278,6 @@ static Level<T> make_level(Arena& a, const Common& cm, const PermutedLp& q,
     S.cg = a.zeros<double>(n);
     S.dl = a.zeros<float>(n);
     S.du = a.zeros<float>(n);
-    S.xfull = a.zeros<double>(n);
-    S.yfull = a.zeros<double>(m);
   }
   S.best_x = cm.best_x;
   S.best_y = cm.best_y;
@@ -952,6 +950,9 @@ static int solve_impl(const sankhya_pdhg_problem& prob, const sankhya_pdhg_param
       L32.P.pati = upload_sliced<float>(a, hati, cm.at_ptr, cm.at_idx, cm.at_val64, stream,
                                         const_cast<int*>(L64.P.pati.sell_idx));
     }
+    // both levels evaluate over the FP64 slices
+    L64.P.pae = L32.P.pae = L64.P.pai;
+    L64.P.pate = L32.P.pate = L64.P.pati;
   }
   mark("schedules");
   // ||A||_2 by power iteration (scaling.cpp:161-194), seed random_seed + 1
