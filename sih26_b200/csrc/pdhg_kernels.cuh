@@ -359,15 +359,34 @@ __device__ __forceinline__ void run_phase(const int* __restrict__ ptr, const int
 #pragma unroll
         for (int v = 0; v < NV; ++v) s[v] = 0.0;
         // values and gathered entries stay in their stored width until the multiply; a
-        // product of two FP32 numbers is exact in FP64, so the sum is the stream item's
+        // product of two FP32 numbers is exact in FP64, so the sum is the stream item's.
+        // FP32 slices load the next round's column indices while this round's entries are
+        // gathered (kPipe; measured faster there, slower with FP64 values).
+        constexpr bool kPipe = sizeof(V) == 4;
+        int jn[kUnroll];
+        if constexpr (kPipe) {
+#pragma unroll
+          for (int t = 0; t < kUnroll; ++t)
+            jn[t] = (mine && t < len) ? ld_stream(si + (size_t)t * rows) : 0;
+        }
         for (int k0 = 0; k0 < L; k0 += kUnroll) {
           int j[kUnroll];
           V a[kUnroll];
 #pragma unroll
           for (int t = 0; t < kUnroll; ++t) {
             const bool live = mine && k0 + t < len;
-            j[t] = live ? ld_stream(si + (size_t)(k0 + t) * rows) : 0;
+            if constexpr (kPipe)
+              j[t] = jn[t];
+            else
+              j[t] = live ? ld_stream(si + (size_t)(k0 + t) * rows) : 0;
             a[t] = live ? ld_stream(sv + (size_t)(k0 + t) * rows) : V(0);
+          }
+          if constexpr (kPipe) {
+#pragma unroll
+            for (int t = 0; t < kUnroll; ++t) {
+              const int k = k0 + kUnroll + t;
+              jn[t] = (mine && k < len) ? ld_stream(si + (size_t)k * rows) : 0;
+            }
           }
           if constexpr (paired_gather<Gather>::value) {
             static_assert(NV == 2, "a paired gather reads two vectors");
@@ -445,14 +464,35 @@ __device__ __forceinline__ void run_phase(const int* __restrict__ ptr, const int
           // the lane's entries kb + gl, kb + gl + lanes, ... in rounds of kUnroll independent
           // raw-width gathers, summed in that same order (so the sums are those of the plain
           // loop below, bit for bit)
+          // FP32 values: the next round's column indices are loaded while this round's
+          // entries are gathered, as in a slice
+          constexpr bool kPipe = sizeof(V) == 4;
+          int jn[kUnroll];
+          if constexpr (kPipe) {
+#pragma unroll
+            for (int t = 0; t < kUnroll; ++t) {
+              const int k = kb + gl + t * lanes;
+              jn[t] = k < ke ? ld_stream(idx + k) : 0;
+            }
+          }
           for (int k0 = kb + gl; k0 < ke; k0 += lanes * kUnroll) {
             int j[kUnroll];
             V a[kUnroll];
 #pragma unroll
             for (int t = 0; t < kUnroll; ++t) {
               const int k = k0 + t * lanes;
-              j[t] = k < ke ? ld_stream(idx + k) : 0;
+              if constexpr (kPipe)
+                j[t] = jn[t];
+              else
+                j[t] = k < ke ? ld_stream(idx + k) : 0;
               a[t] = k < ke ? ld_stream(val + k) : V(0);
+            }
+            if constexpr (kPipe) {
+#pragma unroll
+              for (int t = 0; t < kUnroll; ++t) {
+                const int k = k0 + (kUnroll + t) * lanes;
+                jn[t] = k < ke ? ld_stream(idx + k) : 0;
+              }
             }
             if constexpr (paired_gather<Gather>::value) {
               double2 gv[kUnroll];
@@ -1306,8 +1346,11 @@ struct RowEval {
     }
     return v;
   }
+  // acc holds slots 0 .. NS-1 (the row pass of the evaluation keeps only its own 8)
+  template <int NS>
   __device__ __forceinline__ void apply(int i, const double (&s)[NC], const In& v,
-                                        double (&acc)[kEvalSlots]) const {
+                                        double (&acc)[NS]) const {
+    static_assert(NS >= 8, "the row terms fill slots 0-7");
     const double lo = v.lo, hi = v.hi;
 #pragma unroll
     for (int q = 0; q < NC; ++q) {
@@ -1335,8 +1378,9 @@ struct RowEval {
 
 // Column terms (pdhg.cpp:172-199, 239-256). slots: 8/9 dual violation^2, 10/11 bound
 // contribution, 12/13 complementarity, 14/15 primal objective. The report variant also
-// writes the unscaled point and reduced costs.
-template <class T, int NC>
+// writes the unscaled point and reduced costs. acc[0] is slot kBase: the column pass of the
+// evaluation keeps only slots 8-15 (kBase 8), the others the whole 16.
+template <class T, int NC, int kBase = 0>
 struct ColEval {
   const double* dc;
   const double* cl0;
@@ -1367,8 +1411,10 @@ struct ColEval {
     }
     return v;
   }
+  template <int NS>
   __device__ __forceinline__ void apply(int j, const double (&s)[NC], const In& v,
-                                        double (&acc)[kEvalSlots]) const {
+                                        double (&acc)[NS]) const {
+    static_assert(kBase + NS >= 16 && kBase <= 8, "the column terms fill slots 8-15");
     const double lo = v.lo, hi = v.hi;
 #pragma unroll
     for (int q = 0; q < NC; ++q) {
@@ -1378,20 +1424,20 @@ struct ColEval {
         x_out[j] = xj;
         reduced_out[j] = d;
         // report: largest column bound violation
-        if (finite_bound(lo)) acc[9] = dmax(acc[9], lo - xj);
-        if (finite_bound(hi)) acc[9] = dmax(acc[9], xj - hi);
+        if (finite_bound(lo)) acc[9 - kBase] = dmax(acc[9 - kBase], lo - xj);
+        if (finite_bound(hi)) acc[9 - kBase] = dmax(acc[9 - kBase], xj - hi);
       }
       if (d > 0.0) {
-        if (finite_bound(lo)) acc[10 + q] += d * lo; else acc[8 + q] += d * d;
+        if (finite_bound(lo)) acc[10 + q - kBase] += d * lo; else acc[8 + q - kBase] += d * d;
       } else if (d < 0.0) {
-        if (finite_bound(hi)) acc[10 + q] += d * hi; else acc[8 + q] += d * d;
+        if (finite_bound(hi)) acc[10 + q - kBase] += d * hi; else acc[8 + q - kBase] += d * d;
       }
       if (lo != hi) {
         const double ls = finite_bound(lo) ? xj - lo : INFINITY;
         const double us = finite_bound(hi) ? hi - xj : INFINITY;
-        acc[12 + q] = dmax(acc[12 + q], fabs(d) * dmin(ls, us));
+        acc[12 + q - kBase] = dmax(acc[12 + q - kBase], fabs(d) * dmin(ls, us));
       }
-      acc[14 + q] += v.c * xj;
+      acc[14 + q - kBase] += v.c * xj;
     }
   }
 };
@@ -1572,17 +1618,30 @@ __global__ void __launch_bounds__(kThreads, 2) evaluate_kernel(Prob<T> P, State<
   {
     // E2: both candidates' residual terms in one pass over each matrix (FP64 values, the
     // FP64 slices): one 16-byte gather per entry reads both candidates.
-    double acc[kEvalSlots];
+    // Each pass keeps only its own 8 slots live (rows 0-7, columns 8-15); every slot is
+    // reduced on its own, so the split changes no sum. Two paired gathers per round
+    // (measured a little faster than four here).
+    {
+      double acc[8];
 #pragma unroll
-    for (int s = 0; s < kEvalSlots; ++s) acc[s] = 0.0;
-    RowEval<T, 2> re{P.dr, P.rl0, P.ru0, nullptr, nullptr, nullptr, nullptr, S.yc};
-    run_phase<2, kEvalSlots, false, true>(P.A.ptr, P.A.idx, P.A.val64, P.pae, GatherPair{S.xc},
-                                          re, acc, stream);
-    ColEval<T, 2> ce{P.dc, P.cl0, P.cu0, P.c0, nullptr, nullptr, nullptr, nullptr, nullptr, S.xc};
-    run_phase<2, kEvalSlots, false, true>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pate,
-                                          GatherPair{S.yc}, ce, acc, stream);
-    block_reduce<kEvalSlots, kEvalMaxMask>(acc, sh);
-    write_partials(part, 2, acc, kEvalSlots);
+      for (int s = 0; s < 8; ++s) acc[s] = 0.0;
+      RowEval<T, 2> re{P.dr, P.rl0, P.ru0, nullptr, nullptr, nullptr, nullptr, S.yc};
+      run_phase<2, 8, false, true, 2>(P.A.ptr, P.A.idx, P.A.val64, P.pae, GatherPair{S.xc}, re, acc,
+                                   stream);
+      block_reduce<8, kEvalMaxMask & 0xffu>(acc, sh);
+      write_partials(part, 2, acc, 8);
+    }
+    {
+      double acc[8];
+#pragma unroll
+      for (int s = 0; s < 8; ++s) acc[s] = 0.0;
+      ColEval<T, 2, 8> ce{P.dc, P.cl0, P.cu0, P.c0, nullptr, nullptr, nullptr, nullptr, nullptr,
+                          S.xc};
+      run_phase<2, 8, false, true, 2>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pate, GatherPair{S.yc}, ce,
+                                   acc, stream);
+      block_reduce<8, (kEvalMaxMask >> 8)>(acc, sh);
+      write_partials(part, 10, acc, 8);
+    }
     if (test_cert) {
       // the certificates' matrix terms: A'(y - y_r) for the Farkas test, A (x_k - x_{k-1})
       // for the ray test
