@@ -281,8 +281,11 @@ struct paired_gather<G, std::void_t<decltype(G::kPaired)>> : std::bool_constant<
 // lane l of the warp owns row row_begin + l and sums it in its stored order from the slice
 // arrays, kUnroll independent gathers in flight per round; the products are summed in the
 // row's order, as in a stream item. Such a phase uses no shared-memory stream buffer.
+//
+// kLateIn: slices and grouped rows load the epilogue's inputs after the row's sum instead of
+// before it, so they hold no registers during the sum (for epilogues with many inputs).
 template <int NV, int NS, bool kShared = false, bool kSliced = false, int kUnroll = kSliceUnroll,
-          class V, class Gather, class Epi>
+          bool kLateIn = false, class V, class Gather, class Epi>
 __device__ __forceinline__ void run_phase(const int* __restrict__ ptr, const int* __restrict__ idx,
                                           const V* __restrict__ val, const Part& p,
                                           const Gather& g, const Epi& epi, double (&acc)[NS],
@@ -350,7 +353,7 @@ __device__ __forceinline__ void run_phase(const int* __restrict__ ptr, const int
         typename Epi::In in{};
         int len = 0;
         if (mine) {
-          in = epi.load(r);
+          if constexpr (!kLateIn) in = epi.load(r);
           len = __ldg(ptr + r + 1) - __ldg(ptr + r);
         }
         const int* __restrict__ si = p.sell_idx + item.w + lane;
@@ -413,7 +416,10 @@ __device__ __forceinline__ void run_phase(const int* __restrict__ ptr, const int
             }
           }
         }
-        if (mine) epi.apply(r, s, in, acc);
+        if (mine) {
+          if constexpr (kLateIn) in = epi.load(r);
+          epi.apply(r, s, in, acc);
+        }
       }
     } else if (kSliced && item.z == 0) {
       // never produced by a sliced partition
@@ -458,7 +464,7 @@ __device__ __forceinline__ void run_phase(const int* __restrict__ ptr, const int
 #pragma unroll
       for (int v = 0; v < NV; ++v) s[v] = 0.0;
       if (valid) {
-        if (gl == 0) in = epi.load(r);
+        if (!kLateIn && gl == 0) in = epi.load(r);
         const int kb = __ldg(ptr + r), ke = __ldg(ptr + r + 1);
         if constexpr (kSliced) {
           // the lane's entries kb + gl, kb + gl + lanes, ... in rounds of kUnroll independent
@@ -528,7 +534,10 @@ __device__ __forceinline__ void run_phase(const int* __restrict__ ptr, const int
 #pragma unroll
         for (int v = 0; v < NV; ++v) s[v] += __shfl_xor_sync(0xffffffffu, s[v], off);
       }
-      if (valid && gl == 0) epi.apply(r, s, in, acc);
+      if (valid && gl == 0) {
+        if constexpr (kLateIn) in = epi.load(r);
+        epi.apply(r, s, in, acc);
+      }
     }
     item = next;
     it = nit;
@@ -1564,7 +1573,8 @@ __global__ void __launch_bounds__(kThreads, 2) evaluate_kernel(Prob<T> P, State<
   // E1: fold the pending running-sum term, form the scaled averages, and measure the
   // movement since the last restart (pdhg.cpp:519-528, 613-624).
   // On the FP32 level the iterates and sums are deltas from the anchor: the movement is the
-  // delta itself, and the full FP64 iterate goes to xfull / yfull for the passes below.
+  // delta itself, and the full FP64 iterate goes to xc / yc (beside the second candidate)
+  // for the passes below.
   double acc1[2] = {0.0, 0.0};
   double ec[kCertSlots];
 #pragma unroll
@@ -1619,15 +1629,16 @@ __global__ void __launch_bounds__(kThreads, 2) evaluate_kernel(Prob<T> P, State<
     // E2: both candidates' residual terms in one pass over each matrix (FP64 values, the
     // FP64 slices): one 16-byte gather per entry reads both candidates.
     // Each pass keeps only its own 8 slots live (rows 0-7, columns 8-15); every slot is
-    // reduced on its own, so the split changes no sum. Two paired gathers per round
-    // (measured a little faster than four here).
+    // reduced on its own, so the split changes no sum. The epilogue's inputs (five or six
+    // FP64 values a row) are loaded after the row's sum (kLateIn), which leaves the registers
+    // to four paired gathers per round (measured fastest of 2 / 4, early / late).
     {
       double acc[8];
 #pragma unroll
       for (int s = 0; s < 8; ++s) acc[s] = 0.0;
       RowEval<T, 2> re{P.dr, P.rl0, P.ru0, nullptr, nullptr, nullptr, nullptr, S.yc};
-      run_phase<2, 8, false, true, 2>(P.A.ptr, P.A.idx, P.A.val64, P.pae, GatherPair{S.xc}, re, acc,
-                                   stream);
+      run_phase<2, 8, false, true, 4, true>(P.A.ptr, P.A.idx, P.A.val64, P.pae, GatherPair{S.xc},
+                                            re, acc, stream);
       block_reduce<8, kEvalMaxMask & 0xffu>(acc, sh);
       write_partials(part, 2, acc, 8);
     }
@@ -1637,8 +1648,8 @@ __global__ void __launch_bounds__(kThreads, 2) evaluate_kernel(Prob<T> P, State<
       for (int s = 0; s < 8; ++s) acc[s] = 0.0;
       ColEval<T, 2, 8> ce{P.dc, P.cl0, P.cu0, P.c0, nullptr, nullptr, nullptr, nullptr, nullptr,
                           S.xc};
-      run_phase<2, 8, false, true, 2>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pate, GatherPair{S.yc}, ce,
-                                   acc, stream);
+      run_phase<2, 8, false, true, 4, true>(P.AT.ptr, P.AT.idx, P.AT.val64, P.pate,
+                                            GatherPair{S.yc}, ce, acc, stream);
       block_reduce<8, (kEvalMaxMask >> 8)>(acc, sh);
       write_partials(part, 10, acc, 8);
     }
