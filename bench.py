@@ -65,18 +65,18 @@ SEED = 1
 METRIC = "time-to-rel-KKT 1e-6 (s)"
 REF_SAMPLE_ITERATIONS = 20
 # Iterations the reference's own operator needs on this workload to reach relative KKT 1e-6 in
-# FP64: 169,080, measured by this bench's FP64 reference-operator leg on a B200 (that leg runs
+# FP64: 167,280, measured by this bench's FP64 reference-operator leg on a B200 (that leg runs
 # the reference's algorithm, src/pdhg/pdhg.cpp:383-644, in FP64; the CPU reference cannot be
 # run to tolerance here, it would take over an hour). The reference arm extrapolates its timed
 # sample to this count; the main arm uses the count its own FP64 reference-operator leg
 # measured in the same run.
-FP64_ITERATIONS_TO_TOLERANCE = 169080
+FP64_ITERATIONS_TO_TOLERANCE = 167280
 # DRAM bytes per step of the FP32 Halpern iteration kernel on this workload, from one ncu
-# capture of a 40-step launch (dram__bytes_read.sum + dram__bytes_write.sum = 1.780 + 0.044 GB
+# capture of a 40-step launch (dram__bytes_read.sum + dram__bytes_write.sum = 1.620 + 0.032 GB
 # over 40 steps; captured with `ncu --set full --clock-control none --kernel-name-base demangled
 # -k regex:"iterate_kernel<float" -s 1 -c 1 python bench.py --profile-run single`). Recaptured
 # whenever the kernel changes.
-ITERATE_DRAM_BYTES_PER_STEP = 45.6e6
+ITERATE_DRAM_BYTES_PER_STEP = 41.3e6
 WORKLOAD = ("powerlaw LP 200,000 x 500,000, 5,000,000 nonzeros (10 per column), rows "
             "Pareto(1.5), values N(0,1)*10^U(-2,2) per row, equality rows, 0<=x<=u, planted "
             "optimum, seed 1; relative KKT 1e-6")
