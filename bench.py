@@ -465,6 +465,7 @@ def served_leg(local, rates, seconds, chunk, algorithm="halpern", seed=5, drain_
                     if active == 0 and waiting == 0 and not tickets and not sub_f:
                         time.sleep(0.0005)
                 span = time.perf_counter() - t0
+                launch_settings = srv.stats()
                 for f in sub_f.values():
                     f.result()
             for f in gen_f.values():
@@ -494,6 +495,7 @@ def served_leg(local, rates, seconds, chunk, algorithm="halpern", seed=5, drain_
                 "value": served_rate, "unit": "LPs/s", "span_s": span,
                 "latency_s": _percentiles(ages), "latency_censored": bool(unfinished),
                 "chunk_attempts": chunk, "max_active": max_active, "solo_min_nnz": solo_min_nnz,
+                "launch_settings": launch_settings,
                 "precision": "fp64", "algorithm": algorithm,
                 "one_at_a_time_fp64": base_rate,
                 "speedup_vs_one_at_a_time": (served_rate / base_rate) if served_rate else None,
@@ -729,7 +731,7 @@ def _brief_served(v):
     lat = v["latency_s"]
     keep = ("offered_rate", "seconds", "requests", "completed", "optimal_or_feasible",
             "certified_infeasible", "value", "unfinished", "speedup_vs_one_at_a_time",
-            "one_at_a_time_fp64", "chunk_attempts", "by_size")
+            "one_at_a_time_fp64", "chunk_attempts", "launch_settings", "by_size")
     out = {k: v[k] for k in keep if k in v}
     out.update({"p50_s": lat["p50"], "p99_s": lat["p99"], "p99.9_s": lat["p99.9"],
                 "latency_censored": v.get("latency_censored"),
@@ -927,8 +929,9 @@ def main():
                     help="Poisson rates, LPs/s, comma-separated")
     ap.add_argument("--served-seconds", type=float, default=20.0,
                     help="arrival window per rate, s (the survey's study is 60)")
-    ap.add_argument("--served-chunk", type=int, default=512,
-                    help="attempts per LP per server launch")
+    ap.add_argument("--served-chunk", type=int, default=-1,
+                    help="attempts per LP per server launch (-1, the default: the server's "
+                         "autotuner)")
     ap.add_argument("--served-max-active", type=int, default=1024,
                     help="LP slots of the server in the served leg")
     ap.add_argument("--served-solo-nnz", type=int, default=0,

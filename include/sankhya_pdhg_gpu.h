@@ -288,7 +288,15 @@ typedef struct sankhya_pdhg_server_config {
   int64_t chunk_attempts;  /* attempts per LP per step for LPs with at most 16,384 nonzeros
                               per block; larger LPs get proportionally fewer (at least 8), so
                               a step lasts about as long for every LP; 0 = run each LP to its
-                              end */
+                              end; -1 (default) = autotuned: a search over powers of two
+                              (16-8,192) for the most LPs finished per second (over windows of
+                              at least 8 launches and 1 s), starting from 512 or, once 32 LPs
+                              have been admitted, from the value the autotune cache (see
+                              sankhya_pdhg_params.autotune) holds for their family (keyed on
+                              the SM count, the launch slots and the LPs' median nonzeros and
+                              nonzeros per row); the value it settles on is stored there.
+                              Chunking only pauses an LP between launches: its answer is the
+                              same for every chunk length */
   int64_t cluster_min_nnz; /* LPs with at least this many nonzeros run on an 8-block thread
                               block cluster instead of one block (default 16384; 0 = never) */
   int32_t clusters;        /* clusters for those LPs; 0 (default): chosen every round from
@@ -301,6 +309,19 @@ typedef struct sankhya_pdhg_server_config {
                               family the batched engine's clusters served the large LPs faster */
   int32_t reserved[6];
 } sankhya_pdhg_server_config;
+
+/* A server's current launch settings. */
+typedef struct sankhya_pdhg_server_stats {
+  int64_t chunk_attempts; /* attempts per LP per launch in use now (0 = each LP to its end) */
+  int32_t chunk_source;   /* 0 configured, 1 tuned by this server (searching or settled),
+                             2 read from the cache */
+  int32_t clusters;       /* 8-block clusters of the current launch graph */
+  int64_t rounds;         /* batched launches so far */
+  double last_round_ms;   /* wall time of the last batched launch */
+  char family[192];       /* chunk_attempts = -1: the autotune cache key of the admitted LPs'
+                             family, once 32 have been admitted ("" before) */
+  int32_t reserved[4];
+} sankhya_pdhg_server_stats;
 
 void sankhya_pdhg_server_default_config(sankhya_pdhg_server_config* config);
 int sankhya_pdhg_server_create(const sankhya_pdhg_server_config* config,
@@ -318,6 +339,8 @@ int sankhya_pdhg_server_step(sankhya_pdhg_server* server, int32_t* active, int32
 int sankhya_pdhg_server_result(sankhya_pdhg_server* server, int64_t ticket,
                                sankhya_pdhg_result* result);
 void sankhya_pdhg_server_free(sankhya_pdhg_server* server);
+/* Fills *stats with the server's current launch settings. */
+int sankhya_pdhg_server_get_stats(sankhya_pdhg_server* server, sankhya_pdhg_server_stats* stats);
 
 /* Solves `count` independent LPs concurrently on one GPU (a server, every LP submitted, run
  * to the end, results collected). results[k] is filled like sankhya_pdhg_gpu_solve's. */

@@ -334,6 +334,26 @@ struct Server {
   long long launches = 0;
   unsigned long long device_clock0 = 0;
   double last_round_seconds = 0.0;  // wall time of the last batched launch
+  long long rounds = 0;             // batched launches so far
+  // attempts per LP per launch (LPs of at most 16,384 nonzeros per block; larger ones get
+  // proportionally fewer): the configured value, or the autotuner's (chunk_attempts = -1)
+  long long chunk = 0;
+  long long graph_chunk = -1;  // the chunk the current graph was built with
+  bool auto_chunk = false;
+  int chunk_source = 0;        // 0 configured, 1 tuned here, 2 read from the cache
+  std::string chunk_family;    // cache key, once enough LPs have been admitted
+  std::vector<long long> family_nnz;
+  std::vector<double> family_per_row;
+  // the chunk search: LPs finished per second over windows of at least kChunkWindow launches
+  // and kChunkWindowSeconds, for every chunk tried
+  double round_work = 0.0;     // LPs the last launch finished
+  double window_work = 0.0, window_time = 0.0;
+  int window_rounds = 0;
+  std::map<long long, double> chunk_rate;
+  long long best_chunk = 0;
+  double best_rate = 0.0;
+  int direction = 1;           // 1 doubling, -1 halving
+  bool chunk_settled = false;
 
   double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
 };
@@ -437,7 +457,8 @@ void query_capacity(Server& s) {
 void build_graph(Server& s, int clusters) {
   clusters = std::max(1, std::min(clusters, s.max_clusters));
   const int small_grid = std::max(1, s.slots_total - clusters * kClusterSize);
-  if (s.graph && clusters == s.clusters && small_grid == s.small_grid) return;
+  if (s.graph && clusters == s.clusters && small_grid == s.small_grid && s.chunk == s.graph_chunk)
+    return;
   if (s.graph) {
     cudaGraphExecDestroy(s.graph);
     s.graph = nullptr;
@@ -448,7 +469,7 @@ void build_graph(Server& s, int clusters) {
   cudaEvent_t fork, join;
   SIH26_SCUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), SANKHYA_GPU_INIT_FAILED);
   SIH26_SCUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming), SANKHYA_GPU_INIT_FAILED);
-  const long long chunk = s.cfg.chunk_attempts > 0 ? s.cfg.chunk_attempts : (1ll << 40);
+  const long long chunk = s.chunk;
   cudaGraph_t g;
   SIH26_SCUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal), SANKHYA_GPU_INIT_FAILED);
   cudaMemsetAsync(s.d_head[0], 0, sizeof(int), cap);
@@ -472,6 +493,65 @@ void build_graph(Server& s, int clusters) {
   cudaStreamDestroy(cap);
   s.clusters = clusters;
   s.small_grid = small_grid;
+  s.graph_chunk = chunk;
+}
+
+// The chunk autotuner (chunk_attempts = -1). Chunking only decides where an LP pauses between
+// launches, never what it computes, so the chunk is free to follow measurement. A launch has
+// a fixed cost (control blocks, the LPs' start-up, the host round trip) besides its attempts,
+// so longer chunks cost less per attempt; but an LP that finishes early in a launch leaves its
+// slot idle until the launch ends, so longer chunks also refill the slots of the small LPs
+// later. The search measures what a served stream is judged by, LPs finished per second, over
+// windows of at least kChunkWindow launches and kChunkWindowSeconds, starting at kChunkStart
+// and moving by factors of two from the best chunk so far while a step gains more than 3 %;
+// when neither neighbour of the best is untried, the best is kept and stored in the autotune
+// cache under the family of the first kChunkFamilySample admitted LPs. A chunk cached for the
+// family is used as it is.
+constexpr long long kChunkMin = 16, kChunkMax = 8192, kChunkStart = 512;
+constexpr int kChunkFamilySample = 32, kChunkWindow = 8;
+constexpr double kChunkWindowSeconds = 1.0;
+
+void note_family(Server& s, const Job& J) {
+  if (!s.auto_chunk || !s.chunk_family.empty()) return;
+  s.family_nnz.push_back(J.nnz);
+  s.family_per_row.push_back(J.m > 0 ? static_cast<double>(J.nnz) / J.m : 0.0);
+  if (static_cast<int>(s.family_nnz.size()) < kChunkFamilySample) return;
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s.cfg.device);
+  s.chunk_family = chunk_key(sms, s.slots_total, s.family_nnz, s.family_per_row);
+  long long cached = 0;
+  if (chunk_lookup(autotune_cache_path(), s.chunk_family, &cached)) {
+    s.chunk = std::max(kChunkMin, std::min(kChunkMax, cached));
+    s.chunk_source = 2;
+    s.chunk_settled = true;
+  }
+}
+
+void tune_chunk(Server& s) {
+  if (!s.auto_chunk || s.chunk_settled || s.last_round_seconds <= 0.0) return;
+  s.window_work += s.round_work;
+  s.window_time += s.last_round_seconds;
+  if (++s.window_rounds < kChunkWindow || s.window_time < kChunkWindowSeconds) return;
+  const double rate = s.window_work / s.window_time;
+  s.window_work = s.window_time = 0.0;
+  s.window_rounds = 0;
+  s.chunk_rate[s.chunk] = rate;
+  if (s.best_chunk == 0 || rate > 1.03 * s.best_rate) {
+    s.best_chunk = s.chunk;
+    s.best_rate = rate;
+  }
+  for (int turn = 0; turn < 2; ++turn) {
+    const long long next = s.direction > 0 ? s.best_chunk * 2 : s.best_chunk / 2;
+    if (next >= kChunkMin && next <= kChunkMax && !s.chunk_rate.count(next)) {
+      s.chunk = next;
+      return;
+    }
+    s.direction = -s.direction;
+  }
+  s.chunk = s.best_chunk;
+  s.chunk_settled = true;
+  if (!s.chunk_family.empty())
+    chunk_store(autotune_cache_path(), s.chunk_family, s.chunk, s.best_rate);  // LPs/s
 }
 
 // Clusters for this round: the large class's share of the active nonzeros (its work per
@@ -640,6 +720,7 @@ static void admit(Server& s) {
     J->image.shrink_to_fit();
     s.slot_job[slot] = J;
     (J->group > 1 ? s.active_big : s.active).push_back(slot);
+    note_family(s, *J);
     changed = true;
   }
   if (changed) {
@@ -685,6 +766,7 @@ static std::vector<int> settle(Server& s, const std::vector<int>& list, const Ct
       }
     }
     if (done) {
+      s.round_work += 1.0;
       finish_job(s, J, c);
       s.alloc->release(J.pool_offset, J.pool_bytes);
       s.slot_job[slot].reset();
@@ -723,6 +805,7 @@ static void run_round(Server& s) {
   const double started = s.now();
   SIH26_SCUDA(cudaGraphLaunch(s.graph, s.stream), SANKHYA_GPU_KERNEL_LAUNCH_FAILED);
   ++s.launches;
+  ++s.rounds;
   if (c0)
     SIH26_SCUDA(cudaMemcpyAsync(s.h_compact, s.d_compact, c0 * sizeof(Ctrl),
                                 cudaMemcpyDeviceToHost, s.stream), SANKHYA_GPU_COPY_FAILED);
@@ -731,8 +814,10 @@ static void run_round(Server& s) {
                                 cudaMemcpyDeviceToHost, s.stream), SANKHYA_GPU_COPY_FAILED);
   SIH26_SCUDA(cudaStreamSynchronize(s.stream), SANKHYA_GPU_SYNC_FAILED);
   s.last_round_seconds = s.now() - started;
+  s.round_work = 0.0;
   s.active = settle(s, s.active, s.h_compact);
   s.active_big = settle(s, s.active_big, s.h_compact2);
+  tune_chunk(s);
 }
 
 }  // namespace sih26
@@ -750,7 +835,7 @@ void sankhya_pdhg_server_default_config(sankhya_pdhg_server_config* c) {
   c->memory_fraction = 0.8;
   c->pool_bytes = 0;
   c->max_active = 4096;
-  c->chunk_attempts = 2048;
+  c->chunk_attempts = -1;  // the autotuner's (measured against fixed lengths on the served family)
   c->cluster_min_nnz = 16384;
   c->clusters = 0;  // adaptive: the large class's share of the active nonzeros
   c->solo_min_nnz = 0;  // never: routing measured slower on the served family
@@ -765,6 +850,10 @@ int sankhya_pdhg_server_create(const sankhya_pdhg_server_config* config,
   *out = nullptr;
   auto s = std::make_unique<Server>();
   if (config) s->cfg = *config; else sankhya_pdhg_server_default_config(&s->cfg);
+  s->auto_chunk = s->cfg.chunk_attempts < 0;
+  s->chunk = s->auto_chunk ? sih26::kChunkStart
+                           : (s->cfg.chunk_attempts > 0 ? s->cfg.chunk_attempts : (1ll << 40));
+  s->chunk_source = s->auto_chunk ? 1 : 0;
   sih26::DeviceGuard guard;
   try {
     int devices = 0;
@@ -911,6 +1000,23 @@ int sankhya_pdhg_server_step(sankhya_pdhg_server* server, int32_t* active, int32
     for (auto& kv : s->jobs) k += kv.second->finished ? 1 : 0;
     *finished = k;
   }
+  return SANKHYA_GPU_SUCCESS;
+}
+
+int sankhya_pdhg_server_get_stats(sankhya_pdhg_server* server, sankhya_pdhg_server_stats* st) {
+  Server* s = reinterpret_cast<Server*>(server);
+  if (!s || !st) {
+    sih26::g_last_error = "server and stats must not be NULL";
+    return SANKHYA_GPU_INVALID_ARGUMENT;
+  }
+  std::lock_guard<std::mutex> lock(s->mu);
+  std::memset(st, 0, sizeof *st);
+  st->chunk_attempts = s->chunk >= (1ll << 40) ? 0 : s->chunk;
+  st->chunk_source = s->chunk_source;
+  st->clusters = s->clusters;
+  st->rounds = s->rounds;
+  st->last_round_ms = s->last_round_seconds * 1e3;
+  std::snprintf(st->family, sizeof st->family, "%s", s->chunk_family.c_str());
   return SANKHYA_GPU_SUCCESS;
 }
 

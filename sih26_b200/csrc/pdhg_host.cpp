@@ -710,6 +710,50 @@ void autotune_store(const std::string& path, const std::string& key, const Sched
   std::fclose(f);
 }
 
+bool chunk_lookup(const std::string& path, const std::string& key, long long* chunk) {
+  std::FILE* f = std::fopen(path.c_str(), "r");
+  if (!f) return false;
+  bool found = false;
+  char line[1024];
+  while (std::fgets(line, sizeof line, f)) {
+    char* tab = std::strchr(line, '\t');
+    if (!tab) continue;
+    if (std::string(line, tab - line) != key) continue;
+    long long v = 0;
+    if (std::sscanf(tab + 1, "%lld", &v) == 1 && v > 0) {
+      *chunk = v;
+      found = true;
+    }
+  }
+  std::fclose(f);
+  return found;
+}
+
+void chunk_store(const std::string& path, const std::string& key, long long chunk, double rate) {
+  const size_t slash = path.find_last_of('/');
+  if (slash != std::string::npos) {
+    for (size_t k = path.find('/', 1); k != std::string::npos && k <= slash; k = path.find('/', k + 1))
+      ::mkdir(path.substr(0, k).c_str(), 0755);
+  }
+  std::FILE* f = std::fopen(path.c_str(), "a");
+  if (!f) return;
+  std::fprintf(f, "%s\t%lld\t%.4g\n", key.c_str(), chunk, rate);
+  std::fclose(f);
+}
+
+std::string chunk_key(int sms, int slots, std::vector<long long> nnz, std::vector<double> per_row) {
+  const auto median = [](auto v) {
+    if (v.empty()) return 0.0;
+    std::nth_element(v.begin(), v.begin() + v.size() / 2, v.end());
+    return static_cast<double>(v[v.size() / 2]);
+  };
+  const double mn = median(nnz), mr = median(per_row);
+  int b = 0;
+  while (std::ldexp(1.0, b) < mn) ++b;
+  return "served|sm" + std::to_string(sms) + "|slots" + std::to_string(slots) + "|nnz2^" +
+         std::to_string(b) + "|perrow" + sig2(mr);
+}
+
 // mt19937 (Matsumoto & Nishimura) and libstdc++'s generate_canonical<double, 53> for a
 // 32-bit engine: (g0 + g1 * 2^32) / 2^64, clamped below 1.
 void uniform_draws(uint32_t seed, double lo, double hi, size_t count, double* out) {

@@ -86,6 +86,13 @@ HostPart partition(const std::vector<int>& ptr, int G, int warps_per_block, int 
 std::string autotune_key(const PermutedLp& q, int G, int sms, int value_bytes);
 std::string autotune_cache_path();
 bool autotune_lookup(const std::string& path, const std::string& key, Schedule* a, Schedule* at);
+// The served engine's chunk length for an LP family (one line per key: key, chunk, the LPs
+// per second it measured; the last line of a key wins).
+bool chunk_lookup(const std::string& path, const std::string& key, long long* chunk);
+void chunk_store(const std::string& path, const std::string& key, long long chunk, double rate);
+// Key of a family of served LPs: the SM count, the launch slots, and the median nonzeros and
+// median nonzeros per row of a sample of its LPs (power-of-two and two-digit buckets).
+std::string chunk_key(int sms, int slots, std::vector<long long> nnz, std::vector<double> per_row);
 void autotune_store(const std::string& path, const std::string& key, const Schedule& a,
                     const Schedule& at, double us_a, double us_at);
 

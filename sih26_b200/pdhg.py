@@ -113,6 +113,7 @@ EXPORTED_SYMBOLS = ("sankhya_pdhg_gpu_default_params", "sankhya_pdhg_gpu_solve",
                     "sankhya_pdhg_server_default_config", "sankhya_pdhg_server_create",
                     "sankhya_pdhg_server_submit", "sankhya_pdhg_server_step",
                     "sankhya_pdhg_server_result", "sankhya_pdhg_server_free",
+                    "sankhya_pdhg_server_get_stats",
                     "sankhya_pdhg_gpu_batch_solve", "sankhya_pdhg_wire_size",
                     "sankhya_pdhg_wire_write", "sankhya_pdhg_wire_view",
                     "sankhya_qp_gpu_solve")
@@ -462,6 +463,12 @@ class _ServerConfig(C.Structure):
                 ("reserved", C.c_int32 * 6)]
 
 
+class _ServerStats(C.Structure):
+    _fields_ = [("chunk_attempts", C.c_int64), ("chunk_source", C.c_int32),
+                ("clusters", C.c_int32), ("rounds", C.c_int64), ("last_round_ms", C.c_double),
+                ("family", C.c_char * 192), ("reserved", C.c_int32 * 4)]
+
+
 def _bind_server(lib):
     if getattr(lib, "_server_bound", False):
         return
@@ -473,6 +480,7 @@ def _bind_server(lib):
                                              C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
     lib.sankhya_pdhg_server_result.argtypes = [C.c_void_p, C.c_int64, C.POINTER(_Result)]
     lib.sankhya_pdhg_server_free.argtypes = [C.c_void_p]
+    lib.sankhya_pdhg_server_get_stats.argtypes = [C.c_void_p, C.POINTER(_ServerStats)]
     lib.sankhya_pdhg_gpu_batch_solve.argtypes = [C.POINTER(_Problem), C.c_int32,
                                                  C.POINTER(_Params), C.POINTER(_Result)]
     lib._server_bound = True
@@ -579,10 +587,14 @@ class Server:
     LPs with at least `cluster_min_nnz` nonzeros run on an 8-block thread-block cluster
     (`clusters` of them; 0 = chosen every round from the large LPs' share of the active
     nonzeros), the others on one block each; LPs with at least `solo_min_nnz` nonzeros are
-    solved one per step on the whole GPU by the single-LP engine."""
+    solved one per step on the whole GPU by the single-LP engine. `chunk_attempts` = -1 lets
+    the server search the attempts per launch for the most LPs finished per second itself (the
+    choice changes when an LP pauses, not its answer); stats() reports the setting."""
+
+    CHUNK_SOURCES = ("configured", "tuned", "cache")
 
     def __init__(self, device: int = 0, memory_fraction: float = 0.8, pool_bytes: int = 0,
-                 max_active: int = 4096, chunk_attempts: int = 2048,
+                 max_active: int = 4096, chunk_attempts: int = -1,
                  cluster_min_nnz: int = 16384, clusters: int = 0,
                  solo_min_nnz: int = 0):
         self.lib = load_library()
@@ -653,6 +665,18 @@ class Server:
             if active == 0 and waiting == 0 and len(done) < len(tickets):
                 raise GpuError(1, "server idle with unfinished tickets")
         return [done[t] for t in tickets]
+
+    def stats(self) -> dict:
+        """The current launch settings: chunk_attempts (0 = each LP to its end), where it
+        came from, the clusters of the launch graph, launches so far, the last launch's ms."""
+        st = _ServerStats()
+        code = self.lib.sankhya_pdhg_server_get_stats(self.handle, C.byref(st))
+        if code != 0:
+            raise GpuError(code, self.lib.sankhya_pdhg_gpu_last_error().decode())
+        return {"chunk_attempts": st.chunk_attempts,
+                "chunk_source": self.CHUNK_SOURCES[st.chunk_source],
+                "clusters": st.clusters, "rounds": st.rounds, "last_round_ms": st.last_round_ms,
+                "family": st.family.decode()}
 
     def close(self):
         if self.handle:

@@ -118,7 +118,7 @@ def test_python_mirrors_match_the_header_layout(tmp_path):
     pairs = [("sankhya_pdhg_problem", P._Problem), ("sankhya_pdhg_params", P._Params),
              ("sankhya_pdhg_residuals", P._Residuals), ("sankhya_pdhg_quality", P._Quality),
              ("sankhya_pdhg_result", P._Result), ("sankhya_pdhg_server_config", P._ServerConfig),
-             ("sankhya_qp_hessian", P._Hessian)]
+             ("sankhya_pdhg_server_stats", P._ServerStats), ("sankhya_qp_hessian", P._Hessian)]
     lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "sankhya_pdhg_gpu.h"',
              "int main(void) {"]
     for cname, py in pairs:
