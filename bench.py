@@ -616,12 +616,18 @@ def config_legs(local, flush, sync, fp64_ref_iterations):
                 "iterations": s.iterations, "fp32_iterations": s.fp32_iterations,
                 "rel_kkt": _rel_kkt(s), "tolerance": tol, **p}
 
-    # c0: small enough for the CPU reference to run to tolerance
+    # c0: small enough for the CPU reference to run to tolerance. Its GPU solves last ~10-20 ms,
+    # where host jitter shows, so each keeps the faster of two (same answer both times).
     lp0 = lpgen.uniform_planted(2000, 5000, 10, seed=0)
     solve(lp0, TOLERANCE, "fp64", "reference")  # warm-up of this shape
-    c0 = {"fp64_reference_operator": record(lp0, solve(lp0, TOLERANCE, "fp64", "reference"),
-                                            TOLERANCE),
-          "mixed_halpern": record(lp0, solve(lp0, TOLERANCE, "mixed", "halpern"), TOLERANCE)}
+
+    def best_of_two(precision, algorithm):
+        a = solve(lp0, TOLERANCE, precision, algorithm)
+        b = solve(lp0, TOLERANCE, precision, algorithm)
+        return a if a.solve_seconds <= b.solve_seconds else b
+
+    c0 = {"fp64_reference_operator": record(lp0, best_of_two("fp64", "reference"), TOLERANCE),
+          "mixed_halpern": record(lp0, best_of_two("mixed", "halpern"), TOLERANCE)}
     if oracle.ref_available():
         os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
         oracle.ref_solve(lp0, tolerance=TOLERANCE, iteration_limit=50, stop_at_request=True)
