@@ -501,12 +501,12 @@ void build_graph(Server& s, int clusters) {
 // a fixed cost (control blocks, the LPs' start-up, the host round trip) besides its attempts,
 // so longer chunks cost less per attempt; but an LP that finishes early in a launch leaves its
 // slot idle until the launch ends, so longer chunks also refill the slots of the small LPs
-// later. The search measures what a served stream is judged by, LPs finished per second, over
-// windows of at least kChunkWindow launches and kChunkWindowSeconds, starting at kChunkStart
-// and moving by factors of two from the best chunk so far while a step gains more than 3 %;
-// when neither neighbour of the best is untried, the best is kept and stored in the autotune
-// cache under the family of the first kChunkFamilySample admitted LPs. A chunk cached for the
-// family is used as it is.
+// later. The search measures the served stream's own figure of merit, LPs finished per
+// second, over windows of at least kChunkWindow launches and kChunkWindowSeconds, starting at
+// kChunkStart and moving by factors of two from the best chunk so far while a step gains more
+// than 3 %; when neither neighbour of the best is untried, the best is kept and stored in the
+// autotune cache under the family of the first kChunkFamilySample admitted LPs. A chunk cached
+// for the family is used as it is.
 constexpr long long kChunkMin = 16, kChunkMax = 8192, kChunkStart = 512;
 constexpr int kChunkFamilySample = 32, kChunkWindow = 8;
 constexpr double kChunkWindowSeconds = 1.0;
