@@ -232,30 +232,57 @@ void check_structure(const sankhya_pdhg_problem& p) {
   if (p.col_starts[0] != 0) bad("col_starts[0] != 0");
   if (p.col_starts[n] != p.num_nonzeros)
     bad(fmtd("col_starts[n] = %lld but num_nonzeros = %lld", p.col_starts[n], p.num_nonzeros));
-  for (int j = 0; j < n; ++j) {
-    const int b = p.col_starts[j], e = p.col_starts[j + 1];
-    if (e < b) bad(fmtd("col_starts decreases at column %lld", j));
-    for (int k = b; k < e; ++k) {
-      const int i = p.row_indices[k];
-      if (i < 0 || i >= m) bad(fmtd("row index %lld out of range in column %lld", i, j));
-      if (k > b && i <= p.row_indices[k - 1])
-        bad(fmtd("row indices of column %lld are not strictly ascending (entry %lld)", j, k));
+  // col_starts first: once it never decreases, every column's range lies in [0, nnz], so the
+  // entry checks below read nothing outside the arrays
+  for (int j = 0; j < n; ++j)
+    if (p.col_starts[j + 1] < p.col_starts[j]) bad(fmtd("col_starts decreases at column %lld", j));
+  // the entries, in column ranges on host threads; the first bad column in column order is
+  // reported, with the message a single pass would give
+  const int parts = host_parts(p.num_nonzeros);
+  std::vector<std::string> why(parts);
+  parallel_parts(parts, [&](int t, int T) {
+    for (int j = split(n, t, T), j1 = split(n, t + 1, T); j < j1; ++j) {
+      const int b = p.col_starts[j], e = p.col_starts[j + 1];
+      for (int k = b; k < e; ++k) {
+        const int i = p.row_indices[k];
+        if (i < 0 || i >= m) {
+          why[t] = fmtd("row index %lld out of range in column %lld", i, j);
+          return;
+        }
+        if (k > b && i <= p.row_indices[k - 1]) {
+          why[t] = fmtd("row indices of column %lld are not strictly ascending (entry %lld)", j, k);
+          return;
+        }
+      }
     }
-  }
+  });
+  for (const std::string& w : why)
+    if (!w.empty()) bad(w);
 }
 
 std::string validate_model(const sankhya_pdhg_problem& p) {
   char buf[256];
   const int m = p.num_rows, n = p.num_cols;
-  for (int j = 0; j < n; ++j) {
-    for (int k = p.col_starts[j]; k < p.col_starts[j + 1]; ++k) {
+  // the values, in column ranges on host threads; the first bad entry in column order wins
+  const int parts = host_parts(p.num_nonzeros);
+  std::vector<long long> first(parts, -1);
+  parallel_parts(parts, [&](int t, int T) {
+    const long long k0 = p.col_starts[split(n, t, T)], k1 = p.col_starts[split(n, t + 1, T)];
+    for (long long k = k0; k < k1; ++k) {
       if (!std::isfinite(p.values[k])) {
-        std::snprintf(buf, sizeof buf,
-                      "matrix entry (%d, %d) is %g, which is not a usable coefficient",
-                      p.row_indices[k], j, p.values[k]);
-        return buf;
+        first[t] = k;
+        return;
       }
     }
+  });
+  for (int t = 0; t < parts; ++t) {
+    if (first[t] < 0) continue;
+    const long long k = first[t];
+    const int j = static_cast<int>(std::upper_bound(p.col_starts, p.col_starts + n + 1,
+                                                    static_cast<int>(k)) - p.col_starts) - 1;
+    std::snprintf(buf, sizeof buf, "matrix entry (%d, %d) is %g, which is not a usable coefficient",
+                  p.row_indices[k], j, p.values[k]);
+    return buf;
   }
   for (int j = 0; j < n; ++j) {
     const double lo = p.col_lower[j], hi = p.col_upper[j];

@@ -34,6 +34,7 @@ bool repair_ray(const sankhya_pdhg_problem& p, std::vector<double>& d);
 void check_structure(const sankhya_pdhg_problem& p);
 
 // Model::validate for an LP (src/core/model.cpp:125-210): returns "" or the first problem.
+// Runs after check_structure has passed (it reads each column's range of the arrays).
 std::string validate_model(const sankhya_pdhg_problem& p);
 
 // build_scaling (src/la/scaling.cpp:111-158): 10 Ruiz rounds then one Pock-Chambolle round,

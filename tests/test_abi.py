@@ -1,6 +1,7 @@
 """The C-ABI library: it loads, exports every symbol include/*.h declares, mirrors the
 reference's option names and defaults, and rejects bad input before touching a GPU."""
 import ctypes as C
+import dataclasses
 import math
 import os
 import re
@@ -75,6 +76,35 @@ def test_malformed_matrix_is_an_argument_error(lib):
     with pytest.raises(P.GpuError) as e:
         P.solve_pdhg(lp)
     assert e.value.code == 10 and "out of range" in str(e.value)
+
+
+def test_col_starts_are_checked_before_any_column_is_read(lib):
+    # col_starts rises past num_nonzeros and then falls back to it: reading column 0's entries
+    # first would run past the arrays, so the decrease must be found before any entry is read
+    lp = lpgen.from_dense([[1, 1, 1]], [3], [math.inf], [1, 1, 1])
+    lp.col_starts = np.array([0, 1000, 1001, 3], dtype=np.int32)
+    with pytest.raises(P.GpuError) as e:
+        P.solve_pdhg(lp)
+    assert e.value.code == 10 and "col_starts decreases at column 2" in str(e.value)
+
+
+def test_the_first_bad_column_is_reported_when_the_checks_run_in_parallel(lib):
+    # 1M nonzeros: the entry checks run in several column ranges at once; the message must name
+    # the first bad column in column order, as one pass would
+    lp = lpgen.uniform_planted(40000, 100000, 10, seed=3)
+    ri = lp.row_indices.copy()
+    ri[lp.col_starts[90000]] = lp.num_rows  # out of range, late
+    ri[lp.col_starts[20001] + 3] = -1       # out of range, earlier
+    bad = dataclasses.replace(lp, row_indices=ri)
+    with pytest.raises(P.GpuError) as e:
+        P.solve_pdhg(bad)
+    assert e.value.code == 10 and "in column 20001" in str(e.value)
+    vals = lp.values.copy()
+    vals[lp.col_starts[99000]] = math.inf
+    vals[lp.col_starts[5000] + 1] = math.nan
+    s = P.solve_pdhg(dataclasses.replace(lp, values=vals))
+    row = int(lp.row_indices[lp.col_starts[5000] + 1])
+    assert s.status == "model_error" and f"matrix entry ({row}, 5000) is nan" in s.message
 
 
 def test_unsorted_column_is_an_argument_error(lib):
