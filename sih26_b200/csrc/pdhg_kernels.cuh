@@ -183,10 +183,8 @@ struct State {
   double* axr;    // [m] A xr (the Halpern operator needs it on the FP64 level too)
   T* xt;          // Halpern: the PDHG output T(z_k), primal part (a delta on the FP32 level)
   T* yt;          // and dual part
-  double* xfull;  // [n] evaluation scratch (batched engine): xr + dx
-  double* yfull;  // [m] yr + dy
-  double* xavg;
-  double* yavg;
+  double* xavg;   // [n] batched engine: the evaluation's second candidate
+  double* yavg;   // [m]
   // single-LP evaluation: both candidates of every column / row side by side (the current
   // point in FP64, then the second candidate), so one 16-byte gather reads both
   double2* xc;  // [n]
