@@ -170,3 +170,17 @@ def test_python_mirrors_match_the_header_layout(tmp_path):
         assert got[(cname, "size")] == C.sizeof(py), cname
         for field, _ in py._fields_:
             assert got[(cname, field)] == getattr(py, field).offset, (cname, field)
+
+
+def test_server_defaults_and_stats_arguments(lib):
+    """The served engine's defaults (chunk length autotuned, 8-block clusters from 16,384
+    nonzeros, no solo routing) and the stats entry point's argument check, without a GPU."""
+    P._bind_server(lib)
+    cfg = P._ServerConfig()
+    lib.sankhya_pdhg_server_default_config(C.byref(cfg))
+    assert cfg.chunk_attempts == -1
+    assert cfg.cluster_min_nnz == 16384 and cfg.clusters == 0 and cfg.solo_min_nnz == 0
+    assert cfg.max_active == 4096 and abs(cfg.memory_fraction - 0.8) < 1e-12
+    st = P._ServerStats()
+    assert lib.sankhya_pdhg_server_get_stats(None, C.byref(st)) == 10
+    assert "must not be NULL" in lib.sankhya_pdhg_gpu_last_error().decode()
