@@ -51,7 +51,9 @@ def test_two_gloo_ranks_gather_every_answer_exactly_once():
     nnz = [int(v) for v in (17, 4000, 250, 250, 90, 3100, 12, 800, 5, 5, 60)]
     world = 2
     port = _free_port()
-    with mp.Manager() as mgr:
+    # the manager's server process is spawned too: forking a multi-threaded test process
+    # (torch starts threads) can deadlock the child
+    with mp.get_context("spawn").Manager() as mgr:
         out = mgr.dict()
         mp.start_processes(_rank_main, args=(world, port, nnz, out), nprocs=world,
                            join=True, start_method="spawn")
