@@ -892,11 +892,12 @@ int sankhya_pdhg_server_create(const sankhya_pdhg_server_config* config,
     sih26::build_graph(*s, s->cfg.clusters > 0 ? s->cfg.clusters : 16);
     unsigned long long* d_clock = nullptr;
     SIH26_SCUDA(cudaMalloc(&d_clock, sizeof *d_clock), SANKHYA_GPU_OUT_OF_MEMORY);
+    // freed on every way out of this block, the failing ones included
+    std::unique_ptr<unsigned long long, cudaError_t (*)(void*)> clock_owner(d_clock, cudaFree);
     sih26::read_clock<<<1, 1, 0, s->stream>>>(d_clock);
     SIH26_SCUDA(cudaMemcpyAsync(&s->device_clock0, d_clock, sizeof *d_clock,
                                 cudaMemcpyDeviceToHost, s->stream), SANKHYA_GPU_COPY_FAILED);
     SIH26_SCUDA(cudaStreamSynchronize(s->stream), SANKHYA_GPU_SYNC_FAILED);
-    cudaFree(d_clock);
     s->t0 = sih26::Clock::now();
   } catch (const Failure& f) {
     sih26::g_last_error = f.message;
@@ -968,6 +969,7 @@ int sankhya_pdhg_server_submit(sankhya_pdhg_server* server, const sankhya_pdhg_p
     J->status = SANKHYA_PDHG_NUMERICAL_ERROR;
     J->message = "the LP does not fit the server's device pool";
     J->finished = true;
+    J->finish_time = J->submit_time;
   } else {
     s->waiting.push_back(J);
   }
