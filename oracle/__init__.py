@@ -13,7 +13,10 @@ this package, and only as the checker or the timed CPU baseline -- never as the 
 from .loader import (  # noqa: F401
     OracleResult,
     oracle_available,
+    oracle_csc_multiply,
+    oracle_csc_transpose_multiply,
     oracle_evaluate,
+    oracle_primal_step,
     oracle_scaling,
     oracle_solve,
     oracle_spectral_norm,

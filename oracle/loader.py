@@ -105,6 +105,11 @@ def _oracle():
         lib.oracle_build_scaling.argtypes = [C.POINTER(_LP), _f64p, C.c_int] + [_f64p] * 8
         lib.oracle_uniform_draws.argtypes = [C.c_uint32, C.c_double, C.c_double, C.c_int64,
                                              _f64p]
+        lib.oracle_csc_multiply.argtypes = [C.c_int32, C.c_int32, _i32p, _i32p, _f64p, _f64p,
+                                            _f64p]
+        lib.oracle_csc_transpose_multiply.argtypes = [C.c_int32, _i32p, _i32p, _f64p, _f64p,
+                                                      _f64p]
+        lib.oracle_primal_step.argtypes = [C.c_int32, C.c_double] + [_f64p] * 7
         _libs["oracle"] = lib
     return _libs["oracle"]
 
@@ -205,6 +210,42 @@ def oracle_uniform_draws(seed, lo, hi, count) -> np.ndarray:
     out = np.zeros(count)
     _oracle().oracle_uniform_draws(seed, lo, hi, count, _p(out, _f64p))
     return out
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def oracle_csc_multiply(num_rows, col_starts, row_indices, values, x) -> np.ndarray:
+    """y = A x over a CSC matrix, as the oracle's solve computes it (src/la/sparse.cpp:202-212)."""
+    cs = np.ascontiguousarray(col_starts, dtype=np.int32)
+    ri = np.ascontiguousarray(row_indices, dtype=np.int32)
+    v, xv = _f64(values), _f64(x)
+    y = np.zeros(num_rows)
+    _oracle().oracle_csc_multiply(num_rows, len(cs) - 1, _p(cs, _i32p), _p(ri, _i32p),
+                                  _p(v, _f64p), _p(xv, _f64p), _p(y, _f64p))
+    return y
+
+
+def oracle_csc_transpose_multiply(col_starts, row_indices, values, x) -> np.ndarray:
+    """y = A' x over a CSC matrix (per-column gather, src/la/sparse.cpp:214-229)."""
+    cs = np.ascontiguousarray(col_starts, dtype=np.int32)
+    ri = np.ascontiguousarray(row_indices, dtype=np.int32)
+    v, xv = _f64(values), _f64(x)
+    y = np.zeros(len(cs) - 1)
+    _oracle().oracle_csc_transpose_multiply(len(cs) - 1, _p(cs, _i32p), _p(ri, _i32p),
+                                            _p(v, _f64p), _p(xv, _f64p), _p(y, _f64p))
+    return y
+
+
+def oracle_primal_step(tau, x, cost, at_y, lower, upper):
+    """The primal step of src/pdhg/pdhg.cpp:393-400: (x', 2x' - x)."""
+    x, cost, at_y, lower, upper = (_f64(a) for a in (x, cost, at_y, lower, upper))
+    n = len(x)
+    x_next, extrapolated = np.zeros(n), np.zeros(n)
+    _oracle().oracle_primal_step(n, tau, *(_p(a, _f64p) for a in (x, cost, at_y, lower, upper,
+                                                                    x_next, extrapolated)))
+    return x_next, extrapolated
 
 
 def _scaling(fn, lp, min_cost, ruiz):

@@ -94,6 +94,36 @@ static void csc_transpose_multiply_add(int32_t n, const int32_t* cs, const int32
   }
 }
 
+/* primal step (src/pdhg/pdhg.cpp:393-400): x' = proj(x - tau (c + A'y)), x_bar = 2x' - x */
+static void primal_step(int32_t n, double tau, const double* x, const double* cost,
+                        const double* at_y, const double* lower, const double* upper,
+                        double* x_next, double* extrapolated) {
+  for (int32_t j = 0; j < n; ++j) {
+    const double gradient = cost[j] + at_y[j];
+    x_next[j] = project(x[j] - tau * gradient, lower[j], upper[j]);
+    extrapolated[j] = 2.0 * x_next[j] - x[j];
+  }
+}
+
+/* Exported single steps, so the known answers of the reference's GPU-slot tests
+ * (tests/unit/test_gpu.cpp:107-177) can be checked against the code the solve runs. */
+void oracle_csc_multiply(int32_t m, int32_t n, const int32_t* cs, const int32_t* ri,
+                         const double* v, const double* x, double* y) {
+  csc_multiply(m, n, cs, ri, v, x, y);
+}
+
+void oracle_csc_transpose_multiply(int32_t n, const int32_t* cs, const int32_t* ri,
+                                   const double* v, const double* x, double* y) {
+  for (int32_t j = 0; j < n; ++j) y[j] = 0.0;
+  csc_transpose_multiply_add(n, cs, ri, v, x, y);
+}
+
+void oracle_primal_step(int32_t n, double tau, const double* x, const double* cost,
+                        const double* at_y, const double* lower, const double* upper,
+                        double* x_next, double* extrapolated) {
+  primal_step(n, tau, x, cost, at_y, lower, upper, x_next, extrapolated);
+}
+
 /* ---- scaling: src/la/scaling.cpp:14-158 ----------------------------------------------- */
 
 /* apply_pass (:14-40): the rebuild through add_entry + finalize(0.0) keeps the pattern and
@@ -411,11 +441,7 @@ int oracle_pdhg_solve(const oracle_lp* lp, double tolerance, int64_t iteration_o
     /* primal (:393-400) */
     for (int32_t j = 0; j < cols; ++j) at_y[j] = 0.0;
     if (rows > 0) csc_transpose_multiply_add(cols, cs, ri, sv, y, at_y);
-    for (int32_t j = 0; j < cols; ++j) {
-      const double gradient = s_cost[j] + at_y[j];
-      x_next[j] = project(x[j] - tau * gradient, s_cl[j], s_cu[j]);
-      extrapolated[j] = 2.0 * x_next[j] - x[j];
-    }
+    primal_step(cols, tau, x, s_cost, at_y, s_cl, s_cu, x_next, extrapolated);
     /* dual (:403-408) */
     if (rows > 0) csc_multiply(rows, cols, cs, ri, sv, extrapolated, a_x);
     for (int32_t i = 0; i < rows; ++i) {

@@ -79,6 +79,18 @@ double oracle_spectral_norm(int32_t num_rows, int32_t num_cols, const int32_t* c
                             const int32_t* row_indices, const double* values, int iterations,
                             uint32_t seed);
 
+/* The CSC products of src/la/sparse.cpp:202-229 (y = A x; y = A' x, y zeroed first) and the
+ * primal step of src/pdhg/pdhg.cpp:393-400, as the solve below runs them. */
+void oracle_csc_multiply(int32_t num_rows, int32_t num_cols, const int32_t* col_starts,
+                         const int32_t* row_indices, const double* values, const double* x,
+                         double* y);
+void oracle_csc_transpose_multiply(int32_t num_cols, const int32_t* col_starts,
+                                   const int32_t* row_indices, const double* values,
+                                   const double* x, double* y);
+void oracle_primal_step(int32_t n, double tau, const double* x, const double* cost,
+                        const double* at_y, const double* lower, const double* upper,
+                        double* x_next, double* extrapolated);
+
 /* src/pdhg/pdhg.cpp:143-263: unscaled residuals of (x, y) in PDHG sign (y = -multiplier),
  * min-space cost. activity[m] and reduced[n] are outputs (may be NULL). */
 oracle_residuals oracle_evaluate(const oracle_lp* lp, const double* x, const double* y,

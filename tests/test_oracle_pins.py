@@ -119,3 +119,26 @@ def test_oracle_on_netlib_matches_reference(name):
     assert a.objective == b.objective
     ref = json.load(open(os.path.join(NETLIB, "reference.json")))["instances"][name]
     assert abs(a.objective - ref["published_optimal"]) <= 1e-6 * abs(ref["published_optimal"])
+
+
+def test_oracle_steps_meet_the_reference_gpu_slot_known_answers():
+    """The known answers of the reference's GPU-slot tests, on the oracle's own primal step and
+    CSC products (the code its solve runs): the 4-coordinate primal step with a box, a free, a
+    lower-bounded and an interior column (tests/unit/test_gpu.cpp:107-140), and the 2 x 3 CSC
+    product in both orientations (:142-177). The reference allows 1e-12; every value here is
+    exact in binary, so equality is required."""
+    inf = math.inf
+    x_next, extrapolated = oracle.oracle_primal_step(
+        0.5, x=[2.0, 0.0, -4.0, 0.5], cost=[1.0, -2.0, 2.0, 3.0], at_y=[0.0, 1.0, 0.0, 0.0],
+        lower=[-1.0, 0.0, -inf, 0.0], upper=[1.0, 2.0, inf, inf])
+    assert x_next.tolist() == [1.0, 0.5, -5.0, 0.0]
+    assert extrapolated.tolist() == [0.0, 1.0, -6.0, -0.5]
+
+    cs, ri, val = [0, 1, 2, 4], [0, 1, 0, 1], [1.0, 3.0, 2.0, 4.0]  # [[1 0 2] [0 3 4]]
+    assert oracle.oracle_csc_multiply(2, cs, ri, val, [1.0, 2.0, 3.0]).tolist() == [7.0, 18.0]
+    assert oracle.oracle_csc_transpose_multiply(cs, ri, val, [2.0, 5.0]).tolist() == [2.0, 15.0,
+                                                                                       24.0]
+    # an absent bound given as a large finite value (|v| >= 1e30) projects like an infinite one
+    x_next, _ = oracle.oracle_primal_step(1.0, x=[0.0, 0.0], cost=[1e3, -1e3], at_y=[0.0, 0.0],
+                                          lower=[-1e30, -1e31], upper=[1e30, 2e30])
+    assert x_next.tolist() == [-1e3, 1e3]
