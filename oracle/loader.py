@@ -146,7 +146,7 @@ def _ref():
                                          C.POINTER(C.c_double)]
         lib.ref_polish_ipm.argtypes = [C.POINTER(_LP), _f64p, _f64p, _f64p, C.c_int32, C.c_int64,
                                        C.c_char_p, C.c_double, _f64p, _f64p, _f64p,
-                                       C.POINTER(_PolishOut)]
+                                       C.POINTER(_PolishOut), C.c_char_p]
         _libs["ref"] = lib
     return _libs["ref"]
 
@@ -358,10 +358,11 @@ STATUS_VALUES = {v: k for k, v in STATUS_NAMES.items()}
 
 
 def ref_polish_ipm(lp, col_value, row_dual, col_dual, status, iterations, algorithm,
-                   scaled_worst) -> dict:
+                   scaled_worst, message="") -> dict:
     """The reference's interior-point polish of a first-order answer (ipm::solve_ipm with a
     WarmStart, inside the steps of polish_with_the_interior_point, src/core/solve.cpp:184-243):
-    returns the merged answer's status, algorithm, iterations, objective and point."""
+    returns the merged answer's status, algorithm, iterations, objective, message (the first
+    answer's `message` with the polish's note appended) and point."""
     lib = _ref()
     pin = _Pinned(lp)
     x = np.ascontiguousarray(col_value, dtype=np.float64)
@@ -372,7 +373,7 @@ def ref_polish_ipm(lp, col_value, row_dual, col_dual, status, iterations, algori
     rc = lib.ref_polish_ipm(C.byref(pin.s), _p(x, _f64p), _p(rd, _f64p), _p(cd, _f64p),
                             STATUS_VALUES[status], int(iterations), algorithm.encode(),
                             float(scaled_worst), _p(xo, _f64p), _p(rdo, _f64p), _p(cdo, _f64p),
-                            C.byref(out))
+                            C.byref(out), message.encode())
     if rc != 0:
         raise RuntimeError(out.message.decode())
     return {"status": STATUS_NAMES[out.status], "polished": bool(out.polished),

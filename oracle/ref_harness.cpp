@@ -357,12 +357,14 @@ struct ref_polish_out {
 
 /// first_status is the first answer's sankhya::SolveStatus value; first_algorithm its
 /// Solution::algorithm (e.g. "pdhg-gpu"); first_scaled_worst its max(primal, dual)
-/// infeasibility over the recompute_quality scales. col_value / row_dual / col_dual are the
-/// first answer in the reference's units and signs; polished outputs may be NULL.
+/// infeasibility over the recompute_quality scales; first_message its Solution::message (may
+/// be NULL). col_value / row_dual / col_dual are the first answer in the reference's units and
+/// signs; polished outputs may be NULL.
 int ref_polish_ipm(const ref_lp* lp, const double* col_value, const double* row_dual,
                    const double* col_dual, std::int32_t first_status, std::int64_t first_iterations,
                    const char* first_algorithm, double first_scaled_worst, double* x_out,
-                   double* rd_out, double* cd_out, ref_polish_out* out) {
+                   double* rd_out, double* cd_out, ref_polish_out* out,
+                   const char* first_message) {
   using namespace sankhya;
   try {
     const Model model = to_model(*lp);
@@ -386,6 +388,17 @@ int ref_polish_ipm(const ref_lp* lp, const double* col_value, const double* row_
     out->polished = better ? 1 : 0;
     out->polish_iterations = polished.iterations;
     std::string algorithm = first_algorithm ? first_algorithm : "";
+    // solve.cpp:225-241: the merged message of the answer that stands
+    std::string message = first_message ? first_message : "";
+    if (better) {
+      message += "; polished by the interior point in " + std::to_string(polished.iterations) +
+                 " iterations" + (polished.message.empty() ? std::string()
+                                                           : " (" + polished.message + ")");
+    } else {
+      message += "; the interior-point polish did not improve it (" +
+                 std::string(to_string(polished.status)) + " after " +
+                 std::to_string(polished.iterations) + " iterations: " + polished.message + ")";
+    }
     if (better) {
       algorithm += "+ipm";  // solve.cpp:237
       out->status = static_cast<std::int32_t>(polished.status);
@@ -401,7 +414,7 @@ int ref_polish_ipm(const ref_lp* lp, const double* col_value, const double* row_
       out->iterations = first_iterations;
     }
     std::snprintf(out->algorithm, sizeof out->algorithm, "%s", algorithm.c_str());
-    std::snprintf(out->message, sizeof out->message, "%s", polished.message.c_str());
+    std::snprintf(out->message, sizeof out->message, "%s", message.c_str());
     return 0;
   } catch (const std::exception& e) {
     std::snprintf(out->message, sizeof out->message, "%s", e.what());

@@ -142,3 +142,32 @@ def test_oracle_steps_meet_the_reference_gpu_slot_known_answers():
     x_next, _ = oracle.oracle_primal_step(1.0, x=[0.0, 0.0], cost=[1e3, -1e3], at_y=[0.0, 0.0],
                                           lower=[-1e30, -1e31], upper=[1e30, 2e30])
     assert x_next.tolist() == [-1e3, 1e3]
+
+
+def test_stop_at_request_on_adlittle_as_the_reference_test_pins_it():
+    """tests/unit/test_pdhg.cpp:339-381 on the oracle: adlittle (data/netlib, read by the
+    reference's reader) at a 1e-4 request. The honest run is optimal; with pdhg_stop_at_request
+    the loop stops earlier, on a point reported feasible (it does not meet the absolute
+    standard), primal-feasible to 1e-7 and at the honest objective to 1e-3 relative. The
+    reference test runs the whole solve(), presolve included, and its recorded counts (132,520
+    and 192,080, bench/results/pdhg-stop-at-request-f18d4b0.csv, pdhg-79ec7f7.csv) are of the
+    presolved model; on the model as read, solve_pdhg itself takes 72,400 and 209,160, and the
+    oracle must equal the reference build there iteration for iteration."""
+    from cases import netlib_cases
+
+    lp = next(c[0] for c in netlib_cases() if c[0].name == "adlittle")
+    honest = oracle.oracle_solve(lp, tolerance=1e-4, iteration_limit=1000000)
+    cheap = oracle.oracle_solve(lp, tolerance=1e-4, iteration_limit=1000000,
+                                stop_at_request=True)
+    assert honest.status == "optimal" and cheap.status == "feasible"
+    assert cheap.iterations < honest.iterations
+    assert (cheap.iterations, honest.iterations) == (72400, 209160)
+    assert cheap.residuals["absolute_primal"] <= 1e-7
+    assert abs(cheap.objective - honest.objective) <= 1e-3 * max(1.0, abs(honest.objective))
+    if oracle.ref_available():
+        for mine, sar in ((honest, False), (cheap, True)):
+            ref = oracle.ref_solve(lp, tolerance=1e-4, iteration_limit=1000000,
+                                   stop_at_request=sar)
+            assert (ref.status, ref.iterations, ref.objective) == (mine.status, mine.iterations,
+                                                                   mine.objective)
+            assert np.array_equal(ref.col_value, mine.col_value)
