@@ -1,6 +1,11 @@
 """The certificate checkers the GPU tests use, pinned to the reference's own
 (src/core/certificate.cpp:29-218, through the reference build when it is present), on
-certificates that exist by construction and on near-misses that must be turned down."""
+certificates that exist by construction and on near-misses that must be turned down; and the
+known answers of the reference's certificate tests (tests/unit/test_certificate.cpp:73-182) on
+all three checkers: the numpy restatement, the reference's own, and the library's
+farkas_holds / ray_holds that every certificate passes before the library reports it."""
+import os
+
 import numpy as np
 import pytest
 
@@ -56,3 +61,84 @@ def test_generators_keep_the_planted_structure():
     a = lp.to_scipy_csc()
     assert np.allclose(a @ lp.ray_star, 0.0)
     assert float(lp.cost @ lp.ray_star) < 0.0
+
+
+# The known answers of the reference's certificate tests (tests/unit/test_certificate.cpp:
+# 73-182): (name, kind, A rows, row_lower, row_upper, cost, col_lower, col_upper, vector,
+# verdict, a phrase of the reference checker's reason).
+_INF = float("inf")
+_PAIR = ([[1.0], [1.0]], [5.0, -_INF], [_INF, 2.0], [1.0], [0.0], [_INF])  # x >= 5, x <= 2
+_OPEN = ([[1.0]], [1.0], [_INF], [-1.0], [-_INF], [_INF])  # min -x, x >= 1
+KNOWN_ANSWERS = [
+    ("aggregate_rows", "F", *_PAIR, [1.0, -1.0], True, "at least 3"),
+    ("scaled_up", "F", *_PAIR, [1e6, -1e6], True, None),
+    ("scaled_down", "F", *_PAIR, [1e-6, -1e-6], True, None),
+    ("opposite_sign", "F", *_PAIR, [-1.0, 1.0], False, None),
+    ("missing_row_bound", "F", *_PAIR, [-1.0, -1.0], False, "does not have"),
+    ("free_column", "F", [[1.0]], [5.0], [_INF], [1.0], [-_INF], [_INF], [1.0], False,
+     "free upward"),
+    ("all_zero", "F", *_PAIR, [0.0, 0.0], False, "every multiplier is zero"),
+    ("marginal", "F", [[1.0], [1.0]], [5.0, -_INF], [_INF, 5.0 - 1e-12], [1.0], [0.0], [_INF],
+     [1.0, -1.0], False, "not a contradiction beyond rounding"),
+    ("unblocked_ray", "R", *_OPEN, [1.0], True, "improves"),
+    ("worsening_ray", "R", *_OPEN, [-1.0], False, None),
+    ("bound_blocks", "R", [[1.0]], [1.0], [_INF], [-1.0], [-_INF], [10.0], [1.0], False,
+     "upper bound"),
+    ("row_blocks", "R", [[1.0, 1.0]], [-_INF], [10.0], [-1.0, -1.0], [-_INF, -_INF],
+     [_INF, _INF], [1.0, 1.0], False, "row"),
+    ("zero_direction", "R", *_OPEN, [0.0], False, "not a direction"),
+]
+
+
+def _known_lp(case):
+    _, _, rows, rl, ru, cost, cl, cu, *_ = case
+    return lpgen.from_dense(rows, rl, ru, cost, cl, cu)
+
+
+@pytest.mark.parametrize("case", KNOWN_ANSWERS, ids=[c[0] for c in KNOWN_ANSWERS])
+def test_numpy_and_reference_checkers_give_the_reference_known_answers(case):
+    name, kind, *_, vec, want, phrase = case
+    lp = _known_lp(case)
+    got, why = (farkas_numpy if kind == "F" else ray_numpy)(lp, vec)
+    assert got == want, (name, why)
+    if oracle.ref_available():
+        got, why = (oracle.ref_farkas_check if kind == "F" else oracle.ref_ray_check)(lp, vec)
+        assert got == want, (name, why)
+        if phrase:
+            assert phrase in why, (name, why)
+
+
+def test_library_checkers_give_the_reference_known_answers(tmp_path):
+    """The library's own farkas_holds / ray_holds (pdhg_host.cpp), through
+    tests/certificate_check.cpp compiled against the library's host source."""
+    import shutil
+    import subprocess
+
+    cuda_inc = "/usr/local/cuda/include"
+    if shutil.which("g++") is None or not os.path.isdir(cuda_inc):
+        pytest.skip("no C++ compiler or CUDA headers")
+    here = os.path.dirname(os.path.abspath(__file__))
+    root = os.path.dirname(here)
+    exe = tmp_path / "certificate_check"
+    cmd = ["g++", "-O1", "-std=c++17", "-pthread", "-I", cuda_inc, "-I",
+           os.path.join(root, "include"), "-I", os.path.join(root, "sih26_b200", "csrc"),
+           os.path.join(here, "certificate_check.cpp"),
+           os.path.join(root, "sih26_b200", "csrc", "pdhg_host.cpp"), "-o", str(exe)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:  # the host source may want the CUDA runtime's symbols at link time
+        r = subprocess.run(cmd + ["-L/usr/local/cuda/lib64", "-lcudart"], capture_output=True,
+                           text=True)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = []
+    for case in KNOWN_ANSWERS:
+        name, kind, rows, rl, ru, cost, cl, cu, vec, _, _ = case
+        toks = [name, kind, str(len(rl)), str(len(cost))]
+        toks += [repr(float(v)) for row in rows for v in row]
+        toks += [repr(float(v)) for v in (*rl, *ru, *cost, *cl, *cu, *vec)]
+        lines.append(" ".join(toks))
+    cases = tmp_path / "cases.txt"
+    cases.write_text("\n".join(lines) + "\n")
+    out = subprocess.run([str(exe), str(cases)], capture_output=True, text=True, timeout=60)
+    assert out.returncode == 0, out.stdout + out.stderr
+    got = dict(line.split() for line in out.stdout.splitlines())
+    assert got == {c[0]: "1" if c[9] else "0" for c in KNOWN_ANSWERS}
