@@ -1,9 +1,10 @@
 // Runs the reference-side adapter (integration/pdhg_gpu_adapter.cpp) as the reference solver
-// would: a Model built with the reference's own API (the way tests/unit/test_pdhg.cpp builds
+// would: Models built with the reference's own API (the way tests/unit/test_pdhg.cpp builds
 // its LPs), the reference's default Options, its Logger. Linked against the reference's
-// objects and this library; prints one line for tests/test_integration_adapter.py:
-//   status=<sankhya::to_string(status)> algorithm=<...> iterations=<...> objective=<...>
-//   message=<...>
+// objects and this library; prints one line per adapter call for
+// tests/test_integration_adapter.py:
+//   call=<lp|batch0|batch1|qp> status=<sankhya::to_string(status)> algorithm=<...>
+//   iterations=<...> objective=<...> message=<...>
 #include <cstdio>
 #include <string>
 #include <vector>
@@ -14,6 +15,15 @@
 
 namespace sankhya::pdhg {
 Solution solve_pdhg_gpu(const Model& model, const Options& options, Logger& logger);
+std::vector<Solution> solve_pdhg_gpu_batch(const std::vector<const Model*>& models,
+                                           const Options& options, Logger& logger);
+Solution solve_convex_qp_gpu(const Model& model, const Options& options, Logger& logger);
+}
+
+static void report(const char* call, const sankhya::Solution& s) {
+  std::printf("call=%s status=%s algorithm=%s iterations=%lld objective=%.17g message=%s\n",
+              call, sankhya::to_string(s.status), s.algorithm.c_str(),
+              static_cast<long long>(s.iterations), s.objective, s.message.c_str());
 }
 
 int main() {
@@ -41,10 +51,20 @@ int main() {
   Options options;
   options.set_bool("log_to_console", false);
   options.set_double("pdhg_tolerance", 1e-8);
+  options.set_double("qp_tolerance", 1e-8);
   Logger logger(stdout, LogLevel::kWarning);
-  const Solution s = pdhg::solve_pdhg_gpu(model, options, logger);
-  std::printf("status=%s algorithm=%s iterations=%lld objective=%.17g message=%s\n",
-              to_string(s.status), s.algorithm.c_str(), static_cast<long long>(s.iterations),
-              s.objective, s.message.c_str());
+  report("lp", pdhg::solve_pdhg_gpu(model, options, logger));
+  const std::vector<Solution> batch = pdhg::solve_pdhg_gpu_batch({&model, &model}, options,
+                                                                  logger);
+  report("batch0", batch.at(0));
+  report("batch1", batch.at(1));
+  // the same rows with 1/2 (x^2 + y^2) added: (3, 5) projected onto 3x + 2y <= 18, optimum
+  // (36/13, 63/13) at 1/26 - 17
+  Model qp = model;
+  qp.hessian.reset(2, 2);
+  qp.hessian.add_entry(0, 0, 1.0);
+  qp.hessian.add_entry(1, 1, 1.0);
+  qp.hessian.finalize();
+  report("qp", pdhg::solve_convex_qp_gpu(qp, options, logger));
   return 0;
 }

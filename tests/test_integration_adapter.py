@@ -2,9 +2,11 @@
 reference's own headers and linked against the reference's own objects (oracle/_ref) and this
 library, then run through tests/adapter_check.cpp on a Model built with the reference's API.
 
-Without a GPU the adapter must hand back kNumericalError with the library's reason, never a
-CPU answer (the boundary has no fallback); with one, the known optimum of
-tests/unit/test_pdhg.cpp:642-648 (-36 at (2, 6)) under the name "pdhg-gpu". The adapter reads
+Three adapter calls run: the single LP, a batch of two LPs (answers carrying the quality block
+the device measured) and a convex QP. Without a GPU each must hand back kNumericalError with
+the library's reason, never a CPU answer (the boundary has no fallback); with one, the known
+optima: -36 at (2, 6) for the LP of tests/unit/test_pdhg.cpp:642-648 under the name
+"pdhg-gpu", and 1/26 - 17 at (36/13, 63/13) for the QP under "qp-gpu". The adapter reads
 the GPU option rows only where the registry has them, so it runs against the reference's
 registry as it stands (whose typed accessors abort on an unknown name).
 """
@@ -36,19 +38,31 @@ def test_adapter_builds_against_the_reference_and_reports_without_fallback(tmp_p
            "-I", os.path.join(ROOT, "include"), "-I", fmt_inc,
            os.path.join(ROOT, "integration", "pdhg_gpu_adapter.cpp"),
            os.path.join(HERE, "adapter_check.cpp"), REF_SO, pdhg.LIBPATH,
-           "-Wl,-rpath," + os.path.dirname(REF_SO), "-Wl,-rpath," + os.path.dirname(pdhg.LIBPATH),
+           "-Wl,-rpath," + os.path.dirname(REF_SO),
+           "-Wl,-rpath," + os.path.dirname(pdhg.LIBPATH),
            "-fopenmp", "-o", str(exe)]
     r = subprocess.run(cmd, capture_output=True, text=True)
     assert r.returncode == 0, r.stderr[-3000:]
     out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
     assert out.returncode == 0, out.stdout + out.stderr
-    line = out.stdout.strip().splitlines()[-1]
-    fields = dict(tok.split("=", 1) for tok in line.split(" message=")[0].split())
-    message = line.split(" message=", 1)[1]
-    assert fields["algorithm"] == "pdhg-gpu", line
-    if fields["status"] == "numerical_error":
-        assert message.startswith("GPU PDHG: ") and "device" in message, line
-        assert int(fields["iterations"]) == 0, line
-    else:
-        assert fields["status"] == "optimal", line
-        assert abs(float(fields["objective"]) + 36.0) <= 1e-6, line
+    calls = {}
+    for line in out.stdout.strip().splitlines():
+        if not line.startswith("call="):
+            continue
+        head, message = line.split(" message=", 1)
+        fields = dict(tok.split("=", 1) for tok in head.split())
+        fields["message"] = message
+        calls[fields["call"]] = fields
+    assert set(calls) == {"lp", "batch0", "batch1", "qp"}, out.stdout
+    for name, f in calls.items():
+        engine = "qp" if name == "qp" else "pdhg"
+        assert f["algorithm"] == f"{engine}-gpu", f
+        if f["status"] == "numerical_error":
+            assert f["message"].startswith(f"GPU {engine.upper()}: "), f
+            assert "device" in f["message"] and int(f["iterations"]) == 0, f
+        elif name == "qp":
+            assert f["status"] == "optimal", f
+            assert abs(float(f["objective"]) - (1 / 26 - 17)) <= 1e-6 * 17, f
+        else:
+            assert f["status"] == "optimal", f
+            assert abs(float(f["objective"]) + 36.0) <= 1e-6 * 36, f
