@@ -112,6 +112,7 @@ Solution finish(Pending& p, const Model& model, bool measured_here) {
     s.primal_ray = p.ray;                        // ... and of ray_proves_unbounded
   }
   s.iterations = p.r.iterations;
+  s.objective = p.r.objective;                   // original sense, offset included
   s.solve_seconds = p.r.total_seconds;
   s.dual_bound = p.r.dual_bound;
   s.message = p.r.message;
