@@ -32,5 +32,6 @@ from .loader import (  # noqa: F401
     ref_scaling,
     ref_solve,
     ref_spectral_norm,
+    ref_validate,
 )
 from .quality import recompute_quality  # noqa: F401,E402

@@ -144,6 +144,7 @@ def _ref():
                                               _f64p]
         lib.ref_kkt_instance.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_int, C.POINTER(_LP),
                                          C.POINTER(C.c_double)]
+        lib.ref_validate.argtypes = [C.POINTER(_LP), C.c_char_p, C.c_int]
         lib.ref_polish_ipm.argtypes = [C.POINTER(_LP), _f64p, _f64p, _f64p, C.c_int32, C.c_int64,
                                        C.c_char_p, C.c_double, _f64p, _f64p, _f64p,
                                        C.POINTER(_PolishOut), C.c_char_p]
@@ -289,6 +290,15 @@ def ref_solve(lp, tolerance=1e-4, iteration_limit=-1, time_limit=float("inf"), r
     return OracleResult(STATUS_NAMES[out.status], out.iterations, out.objective,
                         out.dual_bound, x, rd, cd, message=out.message.decode(),
                         solve_seconds=out.solve_seconds)
+
+
+def ref_validate(lp) -> str:
+    """The reference's Model::validate text for the LP ("" when it passes)."""
+    lib = _ref()
+    pin = _Pinned(lp)
+    why = C.create_string_buffer(512)
+    lib.ref_validate(C.byref(pin.s), why, len(why))
+    return why.value.decode()
 
 
 def ref_farkas_check(lp, y) -> tuple[bool, str]:

@@ -185,6 +185,15 @@ double ref_spectral_norm(const ref_lp* lp, int iterations, unsigned seed) {
 
 /// sankhya::farkas_proves_infeasible / ray_proves_unbounded. Returns 1 when the certificate
 /// proves its verdict, 0 when it does not (with the reason), -1 on an internal error.
+/// The reference's Model::validate (src/core/model.cpp:125-210) of the LP: returns 1 when it
+/// passes, else 0 with validate()'s text in `why` -- the text solve_pdhg reports as its
+/// kModelError message (src/pdhg/pdhg.cpp:273-278).
+int ref_validate(const ref_lp* lp, char* why, int why_len) {
+  const std::string text = to_model(*lp).validate();
+  copy_text(why, static_cast<std::size_t>(why_len), text);
+  return text.empty() ? 1 : 0;
+}
+
 int ref_farkas_check(const ref_lp* lp, const double* y, char* why, int why_len) {
   try {
     const sankhya::Model model = to_model(*lp);

@@ -184,3 +184,60 @@ def test_server_defaults_and_stats_arguments(lib):
     st = P._ServerStats()
     assert lib.sankhya_pdhg_server_get_stats(None, C.byref(st)) == 10
     assert "must not be NULL" in lib.sankhya_pdhg_gpu_last_error().decode()
+
+
+def _malformed():
+    """LPs that break one rule of Model::validate each (src/core/model.cpp:125-210), with the
+    formatting edge cases of its messages, and two that break several (the first rule wins)."""
+    def base():
+        return lpgen.uniform_planted(6, 10, 3, seed=1)
+
+    def edit(**arrays):
+        lp = base()
+        for name, (index, value) in arrays.items():
+            a = np.array(getattr(lp, name), dtype=np.float64)
+            a[index] = value
+            setattr(lp, name, a)
+        return lp
+
+    cases = [
+        ("nan_entry", edit(values=(4, math.nan))),
+        ("neg_nan_entry", edit(values=(4, -math.nan))),
+        ("inf_entry", edit(values=(0, math.inf))),
+        ("neg_inf_entry", edit(values=(7, -math.inf))),
+        ("nan_col_lower", edit(col_lower=(3, math.nan))),
+        ("nan_col_upper", edit(col_upper=(9, math.nan))),
+        ("crossed_col", edit(col_lower=(2, 3.0), col_upper=(2, 1.0))),
+        ("crossed_col_wide", edit(col_lower=(5, 1e300), col_upper=(5, 2.5e-7))),
+        ("crossed_col_inf", edit(col_lower=(1, math.inf), col_upper=(1, -math.inf))),
+        ("nan_cost", edit(cost=(8, math.nan))),
+        ("nan_row_bound", edit(row_upper=(2, math.nan))),
+        ("crossed_row", edit(row_lower=(4, 0.1), row_upper=(4, -1234567.0))),
+        ("nan_offset", base()),
+        ("entry_before_bounds", edit(values=(12, math.nan), col_lower=(0, math.nan))),
+        ("col_before_row", edit(cost=(9, math.nan), row_lower=(0, math.nan))),
+    ]
+    cases[12][1].objective_offset = math.nan
+    big = lpgen.uniform_planted(20000, 100000, 10, seed=2)  # ~1M nonzeros: parallel scan
+    v = np.array(big.values)
+    v[len(v) - 5] = math.inf
+    v[len(v) // 2] = math.nan
+    big.values = v
+    cases.append(("first_of_two_entries", big))
+    return cases
+
+
+@pytest.mark.parametrize("name,lp", _malformed(), ids=[c[0] for c in _malformed()])
+def test_model_error_text_is_the_reference_validate_text(lib, name, lp):
+    """The MODEL_ERROR message is Model::validate's text, as solve_pdhg reports it
+    (src/pdhg/pdhg.cpp:273-278), character for character, checked on the host before any GPU
+    work (so it runs here)."""
+    import oracle
+
+    if not oracle.ref_available():
+        pytest.skip("reference build (oracle/_ref) not present")
+    want = oracle.ref_validate(lp)
+    assert want, name
+    s = P.solve_pdhg(lp)
+    assert s.status == "model_error", (name, s.status, s.message)
+    assert s.message == want, (name, s.message, want)
