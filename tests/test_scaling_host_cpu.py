@@ -7,7 +7,8 @@ the device-preparation threshold, and the device version is tested against it on
 tests/scaling_check.cpp, compiled here against the library's host source, on LPs with every
 bound and row kind, both senses (the min-space cost of a maximised LP is the negated cost, as
 pdhg.cpp:287-291 forms it), block-angular long rows, and a 2M-nonzero power-law LP whose row
-and column passes are split over several host threads.
+and column passes are split over several host threads. The norm estimate's random start
+(uniform_draws) is pinned to the standard library's draws the same way.
 """
 import os
 import shutil
@@ -83,3 +84,23 @@ def test_host_scaling_is_the_reference_scaling_bit_for_bit(checker, tmp_path, na
         for k in KEYS:
             # equal bits: the same values, with infinities and their signs in the same places
             assert np.array_equal(mine[k].view(np.int64), ref[k].view(np.int64)), (name, ruiz, k)
+
+
+def test_host_draws_are_the_standard_library_draws(tmp_path):
+    """The library's uniform_draws, the norm estimate's random start (and the QP engine's), is
+    std::mt19937 with std::uniform_real_distribution<double> bit for bit, across the
+    generator's 624-word twist boundaries (tests/draws_check.cpp)."""
+    if shutil.which("g++") is None or not os.path.isdir(CUDA_INC):
+        pytest.skip("no C++ compiler or CUDA headers")
+    exe = tmp_path / "draws_check"
+    cmd = ["g++", "-O2", "-std=c++17", "-pthread", "-I", CUDA_INC, "-I",
+           os.path.join(ROOT, "include"), "-I", os.path.join(ROOT, "sih26_b200", "csrc"),
+           os.path.join(HERE, "draws_check.cpp"),
+           os.path.join(ROOT, "sih26_b200", "csrc", "pdhg_host.cpp"), "-o", str(exe)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        r = subprocess.run(cmd + ["-L/usr/local/cuda/lib64", "-lcudart"], capture_output=True,
+                           text=True)
+    assert r.returncode == 0, r.stderr[-2000:]
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0 and out.stdout.strip() == "ok", out.stdout
