@@ -1,10 +1,12 @@
 // The library's own certificate checks (pdhg_host.cpp: farkas_holds, ray_holds), the ones every
 // certificate passes before the library reports it, run on small LPs read from a text file.
 // Each case is whitespace-separated tokens:
-//   name kind(F|R) m n  a[m*n] (row-major, zeros not stored)  row_lower[m] row_upper[m]
-//   cost[n] col_lower[n] col_upper[n]  vector (m multipliers for F, n directions for R)
-// with "inf" / "-inf" for absent bounds. Prints "name 1" or "name 0" per case, for
-// tests/test_certificates_cpu.py.
+//   name kind(F|R|P) m n  a[m*n] (row-major, zeros not stored)  row_lower[m] row_upper[m]
+//   cost[n] col_lower[n] col_upper[n]  vector (m multipliers for F, n directions for R, P)
+// with "inf" / "-inf" for absent bounds. Prints "name 1" or "name 0" per case (F: farkas_holds,
+// R: ray_holds), and for P, the repair of a primal-ray candidate, "name B A": B whether the
+// candidate passes ray_holds as it is, A whether repair_ray succeeds and its output passes
+// ray_holds. For tests/test_certificates_cpu.py.
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
@@ -65,6 +67,13 @@ int main(int argc, char** argv) {
     p.col_upper = cu.data();
     p.row_lower = rl.data();
     p.row_upper = ru.data();
+    if (kind == "P") {
+      const bool before = ray_holds(p, vec);
+      std::vector<double> d = vec;
+      const bool after = repair_ray(p, d) && ray_holds(p, d);
+      std::printf("%s %d %d\n", name.c_str(), before ? 1 : 0, after ? 1 : 0);
+      continue;
+    }
     const bool holds = kind == "F" ? farkas_holds(p, vec) : ray_holds(p, vec);
     std::printf("%s %d\n", name.c_str(), holds ? 1 : 0);
   }

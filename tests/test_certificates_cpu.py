@@ -108,9 +108,9 @@ def test_numpy_and_reference_checkers_give_the_reference_known_answers(case):
             assert phrase in why, (name, why)
 
 
-def test_library_checkers_give_the_reference_known_answers(tmp_path):
-    """The library's own farkas_holds / ray_holds (pdhg_host.cpp), through
-    tests/certificate_check.cpp compiled against the library's host source."""
+@pytest.fixture(scope="module")
+def cert_checker(tmp_path_factory):
+    """tests/certificate_check.cpp compiled against the library's host source."""
     import shutil
     import subprocess
 
@@ -119,7 +119,7 @@ def test_library_checkers_give_the_reference_known_answers(tmp_path):
         pytest.skip("no C++ compiler or CUDA headers")
     here = os.path.dirname(os.path.abspath(__file__))
     root = os.path.dirname(here)
-    exe = tmp_path / "certificate_check"
+    exe = tmp_path_factory.mktemp("certs") / "certificate_check"
     cmd = ["g++", "-O1", "-std=c++17", "-pthread", "-I", cuda_inc, "-I",
            os.path.join(root, "include"), "-I", os.path.join(root, "sih26_b200", "csrc"),
            os.path.join(here, "certificate_check.cpp"),
@@ -129,16 +129,65 @@ def test_library_checkers_give_the_reference_known_answers(tmp_path):
         r = subprocess.run(cmd + ["-L/usr/local/cuda/lib64", "-lcudart"], capture_output=True,
                            text=True)
     assert r.returncode == 0, r.stderr[-2000:]
+    return exe
+
+
+def _run_checker(exe, tmp_path, cases):
+    """cases: (name, kind, dense rows, row_lower, row_upper, cost, col_lower, col_upper,
+    vector); returns {name: [verdicts]}."""
+    import subprocess
+
     lines = []
-    for case in KNOWN_ANSWERS:
-        name, kind, rows, rl, ru, cost, cl, cu, vec, _, _ = case
+    for name, kind, rows, rl, ru, cost, cl, cu, vec in cases:
         toks = [name, kind, str(len(rl)), str(len(cost))]
         toks += [repr(float(v)) for row in rows for v in row]
         toks += [repr(float(v)) for v in (*rl, *ru, *cost, *cl, *cu, *vec)]
         lines.append(" ".join(toks))
-    cases = tmp_path / "cases.txt"
-    cases.write_text("\n".join(lines) + "\n")
-    out = subprocess.run([str(exe), str(cases)], capture_output=True, text=True, timeout=60)
+    path = tmp_path / "cases.txt"
+    path.write_text("\n".join(lines) + "\n")
+    out = subprocess.run([str(exe), str(path)], capture_output=True, text=True, timeout=120)
     assert out.returncode == 0, out.stdout + out.stderr
-    got = dict(line.split() for line in out.stdout.splitlines())
-    assert got == {c[0]: "1" if c[9] else "0" for c in KNOWN_ANSWERS}
+    return {line.split()[0]: line.split()[1:] for line in out.stdout.splitlines()}
+
+
+def test_library_checkers_give_the_reference_known_answers(cert_checker, tmp_path):
+    """The library's own farkas_holds / ray_holds (pdhg_host.cpp), through
+    tests/certificate_check.cpp compiled against the library's host source."""
+    got = _run_checker(cert_checker, tmp_path, [c[:9] for c in KNOWN_ANSWERS])
+    assert got == {c[0]: ["1" if c[9] else "0"] for c in KNOWN_ANSWERS}
+
+
+def _dense(lp):
+    a = np.zeros((lp.num_rows, lp.num_cols))
+    for j in range(lp.num_cols):
+        for k in range(lp.col_starts[j], lp.col_starts[j + 1]):
+            a[lp.row_indices[k], j] = lp.values[k]
+    return a.tolist()
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_ray_repair_recovers_a_planted_ray_and_never_makes_a_proof(cert_checker, tmp_path,
+                                                                   seed):
+    """repair_ray (pdhg_host.cpp) on primal-ray candidates like the ones PDHG iterates leave
+    behind: the planted ray of an unbounded LP (lpgen.make_unbounded) passes as it is and after
+    the repair; with the two ray columns moving 2e-6 apart and 1e-7 noise on every bounded
+    column it fails as it is (rows and bounds move) and passes once repaired; a negated
+    candidate and a random direction stay rejected, since the repaired vector must still pass
+    the reference's rules (certificate.cpp:121-218)."""
+    rng = np.random.default_rng(seed)
+    lp = _unbounded(seed)
+    n = lp.num_cols
+    noisy = lp.ray_star.copy()
+    noisy[-1] += 2e-6
+    noisy[:-2] += 1e-7 * rng.standard_normal(n - 2)
+    vectors = {"exact": lp.ray_star, "noisy": noisy, "negated": -noisy,
+               "random": rng.standard_normal(n)}
+    rows = _dense(lp)
+    cases = [(name, "P", rows, lp.row_lower, lp.row_upper, lp.cost, lp.col_lower, lp.col_upper,
+              vec) for name, vec in vectors.items()]
+    got = _run_checker(cert_checker, tmp_path, cases)
+    assert got == {"exact": ["1", "1"], "noisy": ["0", "1"], "negated": ["0", "0"],
+                   "random": ["0", "0"]}, got
+    # the numpy restatement agrees on the candidates as they are
+    for name, vec in vectors.items():
+        assert ray_numpy(lp, vec)[0] == (got[name][0] == "1"), name
