@@ -8,7 +8,8 @@ tests/scaling_check.cpp, compiled here against the library's host source, on LPs
 bound and row kind, both senses (the min-space cost of a maximised LP is the negated cost, as
 pdhg.cpp:287-291 forms it), block-angular long rows, and a 2M-nonzero power-law LP whose row
 and column passes are split over several host threads. The norm estimate's random start
-(uniform_draws) is pinned to the standard library's draws the same way.
+(uniform_draws) is pinned to the standard library's draws the same way, and the host layout
+(permute: length-sorted CSR copies of A and A') is checked against the CSC it came from.
 """
 import os
 import shutil
@@ -104,3 +105,74 @@ def test_host_draws_are_the_standard_library_draws(tmp_path):
     assert r.returncode == 0, r.stderr[-2000:]
     out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
     assert out.returncode == 0 and out.stdout.strip() == "ok", out.stdout
+
+
+@pytest.fixture(scope="module")
+def permuter(tmp_path_factory):
+    if shutil.which("g++") is None or not os.path.isdir(CUDA_INC):
+        pytest.skip("no C++ compiler or CUDA headers")
+    exe = tmp_path_factory.mktemp("permute") / "permute_check"
+    cmd = ["g++", "-O2", "-std=c++17", "-pthread", "-I", CUDA_INC, "-I",
+           os.path.join(ROOT, "include"), "-I", os.path.join(ROOT, "sih26_b200", "csrc"),
+           os.path.join(HERE, "permute_check.cpp"),
+           os.path.join(ROOT, "sih26_b200", "csrc", "pdhg_host.cpp"), "-o", str(exe)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        r = subprocess.run(cmd + ["-L/usr/local/cuda/lib64", "-lcudart"], capture_output=True,
+                           text=True)
+    assert r.returncode == 0, r.stderr[-2000:]
+    return exe
+
+
+def _sorted_by_count_stable(perm, counts):
+    """perm lists every index once, by count descending, ties in index order."""
+    assert np.array_equal(np.sort(perm), np.arange(len(counts)))
+    want = np.lexsort((np.arange(len(counts)), -counts))
+    return np.array_equal(perm, want)
+
+
+@pytest.mark.parametrize("name,lp", _lps(), ids=[c[0] for c in _lps()])
+def test_host_permutation_holds_the_matrix_in_both_orders(permuter, tmp_path, name, lp):
+    """The library's permute (pdhg_host.cpp), which lays out every LP the batched engine and
+    the host preparation run: rows of A and of A' in nonzero order, longest first and stable,
+    and both CSR copies hold exactly the CSC's entries, their column indices pointing into the
+    other permuted space."""
+    m, n, nnz = lp.num_rows, lp.num_cols, lp.num_nonzeros
+    src, dst = tmp_path / "in.bin", tmp_path / "out.bin"
+    with open(src, "wb") as f:
+        np.array([m, n, nnz, 0], dtype=np.int32).tofile(f)
+        np.asarray(lp.col_starts, dtype=np.int32).tofile(f)
+        np.asarray(lp.row_indices, dtype=np.int32).tofile(f)
+        for a in (lp.values, lp.cost, lp.col_lower, lp.col_upper, lp.row_lower, lp.row_upper):
+            np.asarray(a, dtype=np.float64).tofile(f)
+    r = subprocess.run([str(permuter), str(src), str(dst)], capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr
+    raw = open(dst, "rb").read()
+    ints = np.frombuffer(raw, dtype=np.int32, count=m + n + (m + 1) + nnz + (n + 1) + nnz)
+    rest = np.frombuffer(raw, dtype=np.float64, offset=ints.nbytes)
+    row_perm, col_perm, a_ptr, a_idx, at_ptr, at_idx = np.split(
+        ints, np.cumsum([m, n, m + 1, nnz, n + 1]))
+    a_val, at_val = rest[:nnz], rest[nnz:]
+    assert rest.size == 2 * nnz
+    cs = np.asarray(lp.col_starts, dtype=np.int64)
+    ri = np.asarray(lp.row_indices, dtype=np.int64)
+    cols = np.repeat(np.arange(n), np.diff(cs))
+    assert _sorted_by_count_stable(row_perm, np.bincount(ri, minlength=m))
+    assert _sorted_by_count_stable(col_perm, np.diff(cs))
+    ref = np.lexsort((cols, ri))
+    want = (ri[ref], cols[ref], np.asarray(lp.values)[ref])
+    # A in permuted row order, indices into the permuted columns
+    assert a_ptr[0] == 0 and a_ptr[-1] == nnz and np.all(np.diff(a_ptr) >= 0)
+    ra = row_perm[np.repeat(np.arange(m), np.diff(a_ptr))]
+    ca = col_perm[a_idx]
+    o = np.lexsort((ca, ra))
+    assert np.array_equal(ra[o], want[0]) and np.array_equal(ca[o], want[1])
+    assert np.array_equal(a_val[o], want[2])
+    # A' in permuted column order, indices into the permuted rows
+    assert at_ptr[0] == 0 and at_ptr[-1] == nnz and np.all(np.diff(at_ptr) >= 0)
+    ct = col_perm[np.repeat(np.arange(n), np.diff(at_ptr))]
+    rt = row_perm[at_idx]
+    o = np.lexsort((ct, rt))
+    assert np.array_equal(rt[o], want[0]) and np.array_equal(ct[o], want[1])
+    assert np.array_equal(at_val[o], want[2])
